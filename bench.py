@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: photon-map kd-tree build + exact-kNN radiance estimate on B200.
+
+One step = one pass of the hot path over one synthetic photon map: build the
+point kd-tree over N photons, then the k-nearest radiance estimate at Q query
+points (Morton sort included).  Default workload ("plain"): 1,048,576 photons
+(80% uniform on the five room walls, 20% in a sigma=0.01 caustic on the
+floor), 2,073,600 uniform wall queries (one per 1920x1080 pixel), k = 100,
+R = 0.05, cone filter, FP32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica (its own seeded map and
+query set): the path has no data exchange, so scaling is weak and value is
+the total queries/s of all ranks.  --impl reference times the CPU port of the
+reference algorithm (oracle/, multithreaded kd-tree) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "kNN radiance estimates/s (kd-tree build + k-nearest query per step)"
+UNIT = "queries/s"
+
+
+def workload_config(name: str) -> dict:
+    from mnrt_b200 import gen
+    c = dict(gen.CONFIGS[name])
+    desc = (f"{name}: {c['n']:,} photons ({int(100 * (1 - c.get('caustic_frac', 0)))}% walls / "
+            f"{int(100 * c.get('caustic_frac', 0))}% caustic), {c['nq']:,} wall queries"
+            f"{' (50% clustered)' if c.get('cluster_frac') else ''}, k={c['k']}, R={c['r_max']}, "
+            f"{c['filter']} filter, FP32")
+    c["workload"] = desc
+    return c
+
+
+def make_inputs(cfg: dict, rank: int):
+    from mnrt_b200 import gen
+    ph = gen.photons(cfg["n"], seed=1000 + rank, caustic_frac=cfg.get("caustic_frac", 0.2),
+                     power_mean=cfg.get("power_mean"))
+    q = gen.queries(cfg["nq"], seed=2000 + rank, cluster_frac=cfg.get("cluster_frac", 0.0))
+    return ph, q
+
+
+# ------------------------------------------------------------- CPU legs --
+
+def cpu_reference_step(ph, q, cfg, sample: int, threads: int, rng: np.random.Generator):
+    """One CPU step: full kd-tree build + a bounded query sample, scaled to Q."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+    tree = oracle.KdTree(ph.pos)
+    t1 = time.perf_counter()
+    sel = rng.choice(q.n, size=min(sample, q.n), replace=False)
+    qp, qn = q.pos[sel], q.nrm[sel]
+    idx, _d2, cnt, _r2 = tree.knn(qp, cfg["k"], cfg["r_max"], threads=threads)
+    oracle.radiance_fp64(ph.pos, ph.pow, qp, qn, idx, cnt, cfg["k"], cfg["r_max"], cfg["filter"], 1.0, 0,
+                         threads=threads)
+    t2 = time.perf_counter()
+    step_s = (t1 - t0) + (t2 - t1) * q.n / len(sel)
+    return q.n / step_s, t1 - t0, (t2 - t1) / len(sel)
+
+
+def calibrate_sample(ph, q, cfg, threads: int, target_s: float) -> int:
+    from oracle import oracle
+    tree = oracle.KdTree(ph.pos)
+    probe = min(20000, q.n)
+    t0 = time.perf_counter()
+    tree.knn(q.pos[:probe], cfg["k"], cfg["r_max"], threads=threads)
+    per = (time.perf_counter() - t0) / probe
+    return int(max(1000, min(q.n, target_s / max(per, 1e-9))))
+
+
+def run_reference(args, cfg) -> dict:
+    from oracle import oracle
+    ph, q = make_inputs(cfg, 0)
+    threads = oracle.threads_available()
+    sample = calibrate_sample(ph, q, cfg, threads, target_s=1.5)
+    rng = np.random.default_rng(7)
+    for _ in range(args.warmup):
+        cpu_reference_step(ph, q, cfg, sample, threads, rng)
+    vals, builds = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, b, _per = cpu_reference_step(ph, q, cfg, sample, threads, rng)
+        vals.append(v)
+        builds.append(b)
+    wall = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    sample_desc = (f"kd-tree build over all {cfg['n']:,} photons + {sample:,} of {cfg['nq']:,} queries per step "
+                   f"(random subset), query time scaled to all queries")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * cfg["nq"] / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "photons": cfg["n"], "queries": cfg["nq"], "k": cfg["k"],
+                   "r_max": cfg["r_max"], "filter": cfg["filter"], "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample_desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "build_ms_cpu": 1000.0 * float(np.mean(builds)), "wall_s": wall,
+        "note": "the reference ships no CPU path and cannot be built here; this is the oracle's port of its "
+                "algorithm (exact kNN, multithreaded kd-tree)",
+    }
+
+
+# ------------------------------------------------------------------ GPU --
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    f = ROOT / "profiles" / f"{kernel}_{workload}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, cfg) -> dict | None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from mnrt_b200.photon_map import PhotonMap
+
+    ph, q = make_inputs(cfg, rank)
+    N, Q, k, R = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h_pos, h_pow, h_qpos, h_qnrm = pin(ph.pos), pin(ph.pow), pin(q.pos), pin(q.nrm)
+    h_rad = torch.empty((Q, 4), dtype=torch.float32).pin_memory()
+    d_pos, d_pow = h_pos.to(dev), h_pow.to(dev)
+    d_qpos, d_qnrm = h_qpos.to(dev), h_qnrm.to(dev)
+    d_rad = torch.empty((Q, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
+
+    pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
+    if args.leaf or args.wpb or args.rounds:
+        pm.set_tuning(leaf_size=args.leaf or 16, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 8)
+    pm.reserve(N, Q)
+    pm.set_profiling(True)
+    out = {"rad": d_rad}
+    qkw = dict(k=k, r_max=R, filter=cfg["filter"], cone_k=1.0, sorted_queries=not args.unsorted)
+
+    def step():
+        pm.build(d_pos, d_pow)
+        pm.query(d_qpos, d_qnrm, out=out, **qkw)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = pm.info().launches
+    builds, queries, kernels, sorts, steps_ms = [], [], [], [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()                       # evict L2 between timed steps (not timed)
+            e0.record()
+            step()
+            e1.record()
+            e1.synchronize()
+            steps_ms.append(e0.elapsed_time(e1))
+            t = pm.last_timings()
+            builds.append(t.build_ms)
+            queries.append(t.query_ms)
+            kernels.append(t.query_kernel_ms)
+            sorts.append(t.query_sort_ms)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clk.summary()
+    launches = pm.info().launches - launches0
+    info = pm.info()
+    total_ms = float(np.sum(steps_ms))
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = world * Q / (ms_per_step / 1000.0)
+
+    # end to end through the public API: pinned host in, host radiance out
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0.record()
+        d_pos.copy_(h_pos, non_blocking=True)
+        d_pow.copy_(h_pow, non_blocking=True)
+        d_qpos.copy_(h_qpos, non_blocking=True)
+        d_qnrm.copy_(h_qnrm, non_blocking=True)
+        step()
+        h_rad.copy_(d_rad, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = float(np.sum(e2e_ms))
+    if world > 1:
+        tt = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = world * Q / (e2e_total / args.steps / 1000.0)
+
+    kern_ms = float(np.mean(kernels))
+    nodes = info.num_nodes
+    alg_bytes = 48 * Q + 32 * N + 64 * (nodes + 1)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kern_ms / 1000.0) / 1e9
+    build_ms = float(np.mean(builds))
+    build_bytes = 68 * N + 64 * (nodes + 1)
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R,
+                   "filter": cfg["filter"], "query_order": "as given" if args.unsorted else "Morton-sorted",
+                   "l2": "flushed between steps (256 MiB write, untimed)",
+                   "parallelism": f"{world} independent replica(s), one per GPU"},
+        "build_ms": build_ms, "query_ms": float(np.mean(queries)), "query_sort_ms": float(np.mean(sorts)),
+        "query_kernel_ms": kern_ms, "query_only_mqueries_per_s": Q / (float(np.mean(queries)) / 1000.0) / 1e6,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profiled_traffic("k_knn_tree", args.config), "kernel": "k_knn_tree",
+                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
+        "roofline_build": {"bound": "hbm", "achieved": build_bytes / (build_ms / 1000.0) / 1e9, "peak": peak,
+                           "unit": "GB/s", "frac": build_bytes / (build_ms / 1000.0) / 1e9 / peak,
+                           "algorithmic_bytes": build_bytes},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * N + 32 * Q,
+                "d2h_bytes_per_step": 16 * Q},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "tree_nodes": nodes,
+        "device_errors": info.device_errors,
+    }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        threads = oracle.threads_available()
+        sample = calibrate_sample(ph, q, cfg, threads, target_s=8.0)
+        v, b, per = cpu_reference_step(ph, q, cfg, sample, threads, np.random.default_rng(11))
+        result["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"kd-tree build over all {N:,} photons ({1000 * b:.0f} ms) + {sample:,} random queries of "
+                      f"{Q:,}, query time scaled to all queries"}
+    return result
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff"])
+    ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--leaf", type=int, default=0)
+    ap.add_argument("--wpb", type=int, default=0)
+    ap.add_argument("--rounds", type=int, default=0)
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg = workload_config(args.config)
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        print(json.dumps(run_reference(args, cfg)), flush=True)
+        return 0
+    res = run_ours(args, cfg)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

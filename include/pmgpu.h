@@ -1,0 +1,216 @@
+/*
+ * pmgpu.h -- C ABI of the B200 photon-map density-estimation engine.
+ *
+ * One engine object (pm_map) replaces the reference's PhotonMap + KDTreePoint
+ * pair (paths inside jonike/mnrt):
+ *   PhotonMap::PhotonMap(maxPhotons, aabbMin, aabbMax, rMax, settings)  PhotonMap.h:89
+ *   PhotonMap::Merge / ScaleFlux / BuildMap                             PhotonMap.h:122-158
+ *   KDTreePoint(d_points, n, aabbMin, aabbMax, rMax) + BuildTree()       KDTreePoint.h:83, KDTreeGPU.h:207
+ *   PhotonMap::Gather / GatherFor / Visualize                           PhotonMap.h:195-232
+ *   PhotonMap::SetKNNTargetCount                                         PhotonMap.h:257
+ *   KDTreePoint::ComputeQueryRadii                                       KDTreePoint.h:122
+ *
+ * Conventions
+ *   - Every entry point returns pm_status: 0 on success, a negative code on
+ *     error.  Nothing aborts the process.  pm_last_error() describes the last
+ *     failure of a handle.
+ *   - "float4 arrays" are plain float pointers to 4*n contiguous floats,
+ *     16-byte aligned, in device memory unless the name says host.
+ *   - stream is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls are asynchronous on that stream unless documented otherwise.
+ *   - Handles are independent; there is no global mutable state.  One handle
+ *     must not be used from two host threads at once.
+ *
+ * Photon formats accepted by pm_build (PM_PHOTONS_*):
+ *   REFERENCE: the reference's PhotonData (KernelDefs.h:537-629):
+ *              pos.xyz = position, pos.w = azimuth phi in [0, 2pi),
+ *              pow.xyz = RGB flux, pow.w = polar theta in [0, pi];
+ *              incident direction = (sin t cos p, sin t sin p, cos t)
+ *              (GPU/mncudautil_dev.h:345-352).
+ *   PACKED:    pos.xyz = position, pos.w ignored,
+ *              pow.xyz = RGB flux, pow.w = octahedral direction code
+ *              (uint32 bits: 16-bit snorm u | 16-bit snorm v << 16).
+ */
+#ifndef PMGPU_H
+#define PMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PM_API __attribute__((visibility("default")))
+#else
+#define PM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pm_status;
+
+enum {
+    PM_OK = 0,
+    PM_ERR_INVALID = -1,     /* bad argument (null pointer, k == 0, r_max <= 0, ...) */
+    PM_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+    PM_ERR_OOM = -3,         /* device allocation failed */
+    PM_ERR_STATE = -4,       /* call not valid in this state (no map built, capture growth) */
+    PM_ERR_DEVICE = -5,      /* a kernel reported an error (stack overflow, NaN input, ...) */
+    PM_ERR_UNSUPPORTED = -6  /* parameter outside what this build supports (k > PM_MAX_K) */
+};
+
+enum { PM_PHOTONS_REFERENCE = 0, PM_PHOTONS_PACKED = 1 };
+enum { PM_FILTER_BOX = 0, PM_FILTER_CONE = 1, PM_FILTER_EPANECHNIKOV = 2 };
+enum { PM_MODE_EXACT = 0, PM_MODE_ZHOU_COMPAT = 1 };
+enum { PM_ORDER_SORTED = 0, PM_ORDER_AS_GIVEN = 1 };
+
+/* Largest k the query kernels support. */
+#define PM_MAX_K 128u
+
+/* Device-side error bits, returned in pm_map_info.device_errors. */
+#define PM_DEVERR_STACK 0x1u     /* traversal stack overflow (query result invalid) */
+#define PM_DEVERR_NONFINITE 0x2u /* non-finite photon position at build */
+#define PM_DEVERR_QNONFINITE 0x4u/* non-finite query position */
+
+typedef struct pm_map pm_map;
+
+typedef struct pm_query_desc {
+    uint32_t k;          /* neighbours per query, 1..PM_MAX_K (reference: SetKNNTargetCount, default 100) */
+    float r_max;         /* maximum query radius R (reference: globalQRadiusMax) */
+    int filter;          /* PM_FILTER_* */
+    float cone_k;        /* cone filter constant k_c >= 1 (Jensen 2001), used by PM_FILTER_CONE */
+    int mode;            /* PM_MODE_EXACT or PM_MODE_ZHOU_COMPAT */
+    uint32_t min_found;  /* estimates from fewer photons are zeroed (reference uses 8) */
+    int order;           /* PM_ORDER_SORTED: Morton-sort the queries first; AS_GIVEN: keep order */
+    uint32_t refine_iters; /* ZHOU_COMPAT only: histogram refinement rounds (reference default 2) */
+} pm_query_desc;
+
+typedef struct pm_map_info {
+    uint32_t num_photons;
+    uint32_t num_nodes;       /* internal nodes of the tree (valid after a synchronising call) */
+    uint32_t leaf_size;       /* maximum photons per leaf */
+    uint32_t device_errors;   /* PM_DEVERR_* bits seen since the last pm_clear_errors */
+    float bounds_min[3];
+    float bounds_max[3];
+    float max_power;
+    uint64_t launches;        /* kernels launched through this handle so far */
+} pm_map_info;
+
+/* Allocation hook: lets a caller route engine allocations through its own
+ * allocator (and lets tests inject failures).  alloc returns 0 on success. */
+typedef int (*pm_alloc_fn)(void** ptr, size_t bytes, void* user);
+typedef void (*pm_free_fn)(void* ptr, void* user);
+
+/* PhotonMap::PhotonMap(maxPhotons, sceneAABBMin, sceneAABBMax, globalQRadiusMax)
+ * (PhotonMap.h:89).  Makes no CUDA call; storage is reserved on first build.
+ * aabb_min/aabb_max (host, 3 floats each, may be NULL) are the scene bounds;
+ * the build uses the photons' own bounds, clipped to nothing. */
+PM_API pm_status pm_create(pm_map** out, uint32_t max_photons, const float* aabb_min, const float* aabb_max,
+                    float r_max);
+PM_API pm_status pm_destroy(pm_map* map);
+
+/* Routes this handle's device allocations through alloc/free (NULL, NULL
+ * restores cudaMalloc/cudaFree).  Must be set before the first build. */
+PM_API pm_status pm_set_allocator(pm_map* map, pm_alloc_fn alloc, pm_free_fn free_fn, void* user);
+
+/* Tuning knobs (chosen by the autotuner): photons per leaf (1..32), warps per
+ * query block (1..8) and query rounds of 32 per work chunk (1..4096). */
+PM_API pm_status pm_set_tuning(pm_map* map, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk);
+
+/* Reserves storage for up to max_photons photons and max_queries queries so
+ * that later builds and queries allocate nothing (needed for stream capture). */
+PM_API pm_status pm_reserve(pm_map* map, uint32_t max_photons, uint32_t max_queries);
+
+/* KDTreePoint(d_points, n, ...) + KDTreeGPU::BuildTree() (KDTreeGPU.cpp:175),
+ * fused with PhotonMap::BuildMap (PhotonMap.cpp:157).  The engine copies and
+ * reorders the photons; the caller's buffers may be reused after the call
+ * completes on the stream.  n == 0 builds an empty map. */
+PM_API pm_status pm_build(pm_map* map, const float* d_pos4, const float* d_pow4, uint32_t n, int format,
+                   void* stream);
+
+/* Exact-kNN radiance estimate (the kernel_PhotonGather / dev_RangeSearch path,
+ * GPU/photon_knn.cu:113-235,487-552, with exact k-nearest semantics).
+ *   d_qpos4, d_qnrm4: query positions and normals (float4, w ignored), nq each.
+ *   d_rad4 (required): per-query irradiance estimate (rgb; w = count as float).
+ *   d_nbr (optional, nq*k uint32): neighbour photon indices (caller order),
+ *          sorted by (d^2, index); unused slots hold 0xFFFFFFFF.
+ *   d_r2 (optional, nq floats): r^2 used by the filter.
+ *   d_count (optional, nq uint32): neighbours found (<= k).
+ * In PM_MODE_ZHOU_COMPAT the estimate follows the reference's own answer: a
+ * histogram-refined radius, then every photon inside it (d_nbr must be NULL). */
+PM_API pm_status pm_query(pm_map* map, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                   uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, void* stream);
+
+/* Brute-force exact kNN over every photon (test and validation path). */
+PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
+                              const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,
+                              uint32_t* d_count, void* stream);
+
+/* Reverse-mode adjoint of pm_query (exact mode).  Given dL/dE per query
+ * (d_grad_rad4, rgb), writes dL/dpower (d_grad_pow4, rgb, w = 0) and
+ * dL/dposition (d_grad_pos4, xyz, w = 0) for every photon in caller order.
+ * d_nbr / d_r2 / d_count: the forward outputs (NULL = recompute the kNN).
+ * Scatter is a deterministic sort-by-photon segmented reduction: the result
+ * is bitwise reproducible. */
+PM_API pm_status pm_query_backward(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
+                            const float* d_qnrm4, uint32_t nq, const float* d_grad_rad4, const uint32_t* d_nbr,
+                            const float* d_r2, const uint32_t* d_count, float* d_grad_pow4, float* d_grad_pos4,
+                            void* stream);
+
+/* PhotonMap::GatherFor (PhotonMap.cpp:234-270, kernel_PhotonGather
+ * GPU/photon_knn.cu:493-551): estimate at gather-ray hits and accumulate
+ *   d_io_radiance4[idx] += clr.w * clr.rgb / pi * E * influence.rgb
+ *   d_io_recip_dist[idx] += rsqrt(|hit - origin|^2)   (if non-NULL)
+ * with idx = d_idx_shading[i] (NULL = i), the normal flipped to face the
+ * incoming ray, and estimates from fewer than desc->min_found photons zeroed
+ * when d_clr_diffuse4 is non-NULL.  NULL d_clr_diffuse4 means white and no
+ * min_found rule (the reference's photon visualisation).  Indices must be
+ * distinct within one call (the reference accumulates without atomics). */
+PM_API pm_status pm_gather_for(pm_map* map, const pm_query_desc* desc, const float* d_hit_pos4,
+                        const float* d_hit_nrm4, const float* d_ray_dir4, const float* d_ray_origin4,
+                        const float* d_ray_influence4, const float* d_clr_diffuse4, const uint32_t* d_idx_shading,
+                        uint32_t n, float* d_io_radiance4, float* d_io_recip_dist, void* stream);
+
+/* PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): scales the RGB flux of the
+ * built map in place (direction bits untouched). */
+PM_API pm_status pm_scale_flux(pm_map* map, float scale, void* stream);
+
+/* KDTreePoint::ComputeQueryRadii (KDTreePoint.cpp:229-248) in ZHOU_COMPAT
+ * semantics: the reference's histogram-refined query radius per point. */
+PM_API pm_status pm_compute_query_radii(pm_map* map, const pm_query_desc* desc, const float* d_qpos4, uint32_t nq,
+                                 float* d_radii, void* stream);
+
+/* Phase timing with CUDA events recorded on the call's stream (off by
+ * default).  pm_last_timings waits for the last recorded events. */
+typedef struct pm_timings {
+    float build_ms;          /* whole pm_build */
+    float build_sort_ms;     /* Morton codes + radix sort inside pm_build */
+    float query_ms;          /* whole pm_query */
+    float query_sort_ms;     /* query Morton sort inside pm_query (0 when AS_GIVEN) */
+    float query_kernel_ms;   /* the kNN kernel alone */
+    uint32_t build_launches; /* kernels launched by the last pm_build */
+    uint32_t query_launches; /* kernels launched by the last pm_query */
+} pm_timings;
+PM_API pm_status pm_set_profiling(pm_map* map, int enable);
+PM_API pm_status pm_last_timings(pm_map* map, pm_timings* out);
+
+/* Blocks until the stream is idle, then fills info (including device error bits). */
+PM_API pm_status pm_get_info(pm_map* map, pm_map_info* info, void* stream);
+PM_API pm_status pm_clear_errors(pm_map* map, void* stream);
+
+/* Copies the tree for structural validation: nodes as 16 uint32 each
+ * (child 0: lo xyz, hi xyz, ref, count; child 1: same), and the photons in
+ * tree order (pos4 with w = caller index bits, pow4 with w = direction bits).
+ * Synchronous.  Any output pointer may be NULL. */
+PM_API pm_status pm_export_tree(pm_map* map, uint32_t* host_nodes, uint32_t max_nodes, float* host_pos4,
+                         float* host_pow4, uint32_t max_photons);
+
+PM_API const char* pm_last_error(const pm_map* map);
+PM_API const char* pm_status_string(pm_status s);
+PM_API int pm_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PMGPU_H */

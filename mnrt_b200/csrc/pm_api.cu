@@ -1,0 +1,489 @@
+// pm_api.cu -- C ABI of the engine (include/pmgpu.h).
+//
+// A pm_map owns every device buffer it uses (photons in tree order, nodes,
+// build and query scratch).  Arguments are validated before any CUDA call, so
+// invalid calls fail the same way with or without a GPU.  Storage grows on
+// demand outside stream capture; pm_reserve pre-sizes it for capture.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "pm_internal.h"
+#include "../../include/pmgpu.h"
+
+using namespace pm;
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct pm_map {
+    // configuration
+    uint32_t max_photons = 0;
+    float scene_min[3] = {0, 0, 0}, scene_max[3] = {0, 0, 0};
+    float r_max = 0.0f;
+    uint32_t leaf_size = 16;
+    int warps_per_block = 4;
+    int rounds_per_chunk = 8;
+    pm_alloc_fn alloc = nullptr;
+    pm_free_fn free_fn = nullptr;
+    void* alloc_user = nullptr;
+    // state
+    uint32_t n = 0;
+    bool built = false;
+    uint32_t cap_photons = 0;   // capacity of photon-sized buffers
+    uint32_t cap_queries = 0;   // capacity of query-sized buffers
+    // photon-sized
+    DevBuf pos, pow, nodes, hdr;
+    DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
+    // query-sized
+    DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter;
+    // profiling: events recorded on the call's stream when enabled
+    bool profiling = false;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // b0 b1 b2 q0 q1 q2
+    bool have_build_ev = false, have_query_ev = false;
+    uint32_t build_launches = 0, query_launches = 0;
+    uint64_t launches = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+pm_status fail(pm_map* m, pm_status s, const char* fmt, ...) {
+    if (m) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(m->err, sizeof(m->err), fmt, ap);
+        va_end(ap);
+    }
+    return s;
+}
+
+pm_status check_cuda(pm_map* m, const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(m, PM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return PM_OK;
+}
+
+bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) { cudaGetLastError(); return false; }
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+void buf_free(pm_map* m, DevBuf& b) {
+    if (b.ptr) {
+        if (m->free_fn) m->free_fn(b.ptr, m->alloc_user);
+        else cudaFree(b.ptr);
+    }
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+pm_status buf_ensure(pm_map* m, DevBuf& b, size_t bytes, const char* name) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return PM_OK;
+    buf_free(m, b);
+    void* p = nullptr;
+    if (m->alloc) {
+        if (m->alloc(&p, bytes, m->alloc_user) != 0 || !p)
+            return fail(m, PM_ERR_OOM, "allocation of %zu bytes for %s failed (caller allocator)", bytes, name);
+    } else {
+        const cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(m, e == cudaErrorMemoryAllocation ? PM_ERR_OOM : PM_ERR_CUDA,
+                        "cudaMalloc of %zu bytes for %s failed: %s", bytes, name, cudaGetErrorString(e));
+        }
+    }
+    b.ptr = p;
+    b.bytes = bytes;
+    return PM_OK;
+}
+
+template <class T> T* P(const DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+size_t sort_words(uint32_t n) { return sort_scratch_words(n) + 1 + scan_scratch_words(n) + 64; }
+
+pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
+    if (n <= m->cap_photons && m->hdr.ptr) return PM_OK;
+    if (capturing(st))
+        return fail(m, PM_ERR_STATE, "map storage must grow to %u photons during stream capture; call pm_reserve first", n);
+    const size_t cap = n ? n : 1;
+    pm_status s;
+#define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
+    ENSURE(pos, cap * sizeof(float4));
+    ENSURE(pow, cap * sizeof(float4));
+    ENSURE(nodes, (cap + 1) * sizeof(Node));
+    ENSURE(hdr, sizeof(MapHeader));
+    ENSURE(keys0, cap * sizeof(uint64_t));
+    ENSURE(keys1, cap * sizeof(uint64_t));
+    ENSURE(vals0, cap * sizeof(uint32_t));
+    ENSURE(vals1, cap * sizeof(uint32_t));
+    ENSURE(scratch, sort_words((uint32_t)cap) * sizeof(uint32_t));
+    ENSURE(kfirst, cap * sizeof(uint32_t));
+    ENSURE(klast, cap * sizeof(uint32_t));
+    ENSURE(ksplit, cap * sizeof(uint32_t));
+    ENSURE(kkeep, cap * sizeof(uint32_t));
+    ENSURE(krank, cap * sizeof(uint32_t));
+    ENSURE(parent, (cap + 1) * sizeof(uint32_t));
+    ENSURE(arrive, (cap + 1) * sizeof(uint32_t));
+    ENSURE(nleaf, (cap + 1) * sizeof(uint32_t));
+    ENSURE(partials, (8 * 1184 + 16) * sizeof(uint32_t));
+#undef ENSURE
+    m->cap_photons = (uint32_t)cap;
+    return PM_OK;
+}
+
+pm_status ensure_query_capacity(pm_map* m, uint32_t nq, cudaStream_t st) {
+    if (nq <= m->cap_queries && m->counter.ptr) return PM_OK;
+    if (capturing(st))
+        return fail(m, PM_ERR_STATE, "query storage must grow to %u queries during stream capture; call pm_reserve first", nq);
+    const size_t cap = nq ? nq : 1;
+    pm_status s;
+#define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
+    ENSURE(qkeys0, cap * sizeof(uint64_t));
+    ENSURE(qkeys1, cap * sizeof(uint64_t));
+    ENSURE(qvals0, cap * sizeof(uint32_t));
+    ENSURE(qvals1, cap * sizeof(uint32_t));
+    ENSURE(qscratch, sort_words((uint32_t)cap) * sizeof(uint32_t));
+    ENSURE(counter, 64 * sizeof(uint32_t));
+#undef ENSURE
+    m->cap_queries = (uint32_t)cap;
+    return PM_OK;
+}
+
+pm_status validate_desc(pm_map* m, const pm_query_desc* d, bool exact_only) {
+    if (!d) return fail(m, PM_ERR_INVALID, "query descriptor is NULL");
+    if (d->k == 0) return fail(m, PM_ERR_INVALID, "k must be >= 1");
+    if (d->k > PM_MAX_K) return fail(m, PM_ERR_UNSUPPORTED, "k = %u exceeds PM_MAX_K = %u", d->k, PM_MAX_K);
+    if (!(d->r_max > 0.0f) || !std::isfinite(d->r_max))
+        return fail(m, PM_ERR_INVALID, "r_max must be finite and > 0 (got %g)", (double)d->r_max);
+    if (d->filter < PM_FILTER_BOX || d->filter > PM_FILTER_EPANECHNIKOV)
+        return fail(m, PM_ERR_INVALID, "unknown filter %d", d->filter);
+    if (d->filter == PM_FILTER_CONE && !(d->cone_k >= 1.0f && std::isfinite(d->cone_k)))
+        return fail(m, PM_ERR_INVALID, "cone_k must be finite and >= 1 (got %g)", (double)d->cone_k);
+    if (d->mode != PM_MODE_EXACT && d->mode != PM_MODE_ZHOU_COMPAT)
+        return fail(m, PM_ERR_INVALID, "unknown mode %d", d->mode);
+    if (exact_only && d->mode != PM_MODE_EXACT)
+        return fail(m, PM_ERR_INVALID, "this entry point supports PM_MODE_EXACT only");
+    if (d->order != PM_ORDER_SORTED && d->order != PM_ORDER_AS_GIVEN)
+        return fail(m, PM_ERR_INVALID, "unknown query order %d", d->order);
+    return PM_OK;
+}
+
+MapView view_of(pm_map* m) {
+    MapView v;
+    v.pos = P<float4>(m->pos);
+    v.pow = P<float4>(m->pow);
+    v.nodes = P<Node>(m->nodes);
+    v.hdr = P<MapHeader>(m->hdr);
+    v.n = m->n;
+    return v;
+}
+
+QueryParams params_of(const pm_query_desc* d) {
+    QueryParams p;
+    p.k = d->k;
+    p.r2 = d->r_max * d->r_max;
+    p.filter = d->filter;
+    p.cone_k = d->filter == PM_FILTER_CONE ? d->cone_k : 1.0f;
+    p.min_found = d->min_found;
+    return p;
+}
+
+// Morton order of the queries (returns the permutation or nullptr).
+const uint32_t* sort_queries(pm_map* m, const float4* qpos, uint32_t nq, cudaStream_t st, int* launches) {
+    *launches += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint64_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
+    uint64_t* keys[2] = {P<uint64_t>(m->qkeys0), P<uint64_t>(m->qkeys1)};
+    uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
+    const int cur = radix_sort_pairs(keys, vals, nq, 48, P<uint32_t>(m->qscratch), st, launches);
+    return vals[cur];
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_abi_version(void) { return 1; }
+
+const char* pm_status_string(pm_status s) {
+    switch (s) {
+        case PM_OK: return "ok";
+        case PM_ERR_INVALID: return "invalid argument";
+        case PM_ERR_CUDA: return "CUDA error";
+        case PM_ERR_OOM: return "out of device memory";
+        case PM_ERR_STATE: return "invalid state";
+        case PM_ERR_DEVICE: return "device-side error";
+        case PM_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+const char* pm_last_error(const pm_map* m) { return m ? m->err : "null handle"; }
+
+pm_status pm_create(pm_map** out, uint32_t max_photons, const float* aabb_min, const float* aabb_max, float r_max) {
+    if (!out) return PM_ERR_INVALID;
+    *out = nullptr;
+    if (!(r_max > 0.0f) || !std::isfinite(r_max)) return PM_ERR_INVALID;
+    pm_map* m = new (std::nothrow) pm_map();
+    if (!m) return PM_ERR_OOM;
+    m->max_photons = max_photons;
+    for (int a = 0; a < 3; ++a) {
+        m->scene_min[a] = aabb_min ? aabb_min[a] : 0.0f;
+        m->scene_max[a] = aabb_max ? aabb_max[a] : 0.0f;
+    }
+    m->r_max = r_max;
+    *out = m;
+    return PM_OK;
+}
+
+pm_status pm_destroy(pm_map* m) {
+    if (!m) return PM_ERR_INVALID;
+    DevBuf* all[] = {&m->pos, &m->pow, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
+                     &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
+                     &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
+                     &m->qscratch, &m->counter};
+    for (DevBuf* b : all) buf_free(m, *b);
+    for (cudaEvent_t& e : m->ev)
+        if (e) cudaEventDestroy(e);
+    delete m;
+    return PM_OK;
+}
+
+pm_status pm_set_allocator(pm_map* m, pm_alloc_fn alloc, pm_free_fn free_fn, void* user) {
+    if (!m) return PM_ERR_INVALID;
+    if ((alloc == nullptr) != (free_fn == nullptr))
+        return fail(m, PM_ERR_INVALID, "alloc and free must both be set or both be NULL");
+    if (m->hdr.ptr || m->counter.ptr) return fail(m, PM_ERR_STATE, "allocator must be set before the first build or query");
+    m->alloc = alloc;
+    m->free_fn = free_fn;
+    m->alloc_user = user;
+    return PM_OK;
+}
+
+pm_status pm_set_tuning(pm_map* m, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk) {
+    if (!m) return PM_ERR_INVALID;
+    if (leaf_size < 1 || leaf_size > kLeafMax) return fail(m, PM_ERR_INVALID, "leaf_size must be in [1, %u]", kLeafMax);
+    if (warps_per_block < 1 || warps_per_block > 8) return fail(m, PM_ERR_INVALID, "warps_per_block must be in [1, 8]");
+    if (rounds_per_chunk < 1 || rounds_per_chunk > 4096) return fail(m, PM_ERR_INVALID, "rounds_per_chunk must be in [1, 4096]");
+    m->leaf_size = leaf_size;
+    m->warps_per_block = warps_per_block;
+    m->rounds_per_chunk = rounds_per_chunk;
+    return PM_OK;
+}
+
+pm_status pm_reserve(pm_map* m, uint32_t max_photons, uint32_t max_queries) {
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = ensure_photon_capacity(m, max_photons, nullptr);
+    if (s != PM_OK) return s;
+    return ensure_query_capacity(m, max_queries, nullptr);
+}
+
+pm_status pm_build(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t n, int format, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (format != PM_PHOTONS_REFERENCE && format != PM_PHOTONS_PACKED)
+        return fail(m, PM_ERR_INVALID, "unknown photon format %d", format);
+    if (n > 0 && (!d_pos4 || !d_pow4)) return fail(m, PM_ERR_INVALID, "photon arrays must be non-NULL when n > 0");
+    if (n > 0 && (!aligned16(d_pos4) || !aligned16(d_pow4)))
+        return fail(m, PM_ERR_INVALID, "photon arrays must be 16-byte aligned");
+    if (m->max_photons && n > m->max_photons)
+        return fail(m, PM_ERR_INVALID, "n = %u exceeds the map's max_photons = %u", n, m->max_photons);
+    if (n > 0x7fffffffu) return fail(m, PM_ERR_UNSUPPORTED, "n = %u exceeds 2^31 - 1 photons", n);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    pm_status s = ensure_photon_capacity(m, n, st);
+    if (s != PM_OK) return s;
+    BuildBuffers bb;
+    bb.keys[0] = P<uint64_t>(m->keys0); bb.keys[1] = P<uint64_t>(m->keys1);
+    bb.vals[0] = P<uint32_t>(m->vals0); bb.vals[1] = P<uint32_t>(m->vals1);
+    bb.scratch = P<uint32_t>(m->scratch);
+    bb.kfirst = P<uint32_t>(m->kfirst); bb.klast = P<uint32_t>(m->klast); bb.ksplit = P<uint32_t>(m->ksplit);
+    bb.kkeep = P<uint32_t>(m->kkeep); bb.krank = P<uint32_t>(m->krank);
+    bb.parent = P<uint32_t>(m->parent); bb.arrive = P<uint32_t>(m->arrive); bb.nleaf = P<uint32_t>(m->nleaf);
+    bb.partials = P<uint32_t>(m->partials); bb.num_partials = 1184;
+    const bool prof = m->profiling && !capturing(st);
+    if (prof) cudaEventRecord(m->ev[0], st);
+    const int nl = build_map(reinterpret_cast<const float4*>(d_pos4), reinterpret_cast<const float4*>(d_pow4), n,
+                             format, m->leaf_size, P<float4>(m->pos), P<float4>(m->pow), P<Node>(m->nodes),
+                             P<MapHeader>(m->hdr), bb, st, prof ? m->ev[1] : nullptr);
+    if (prof) cudaEventRecord(m->ev[2], st);
+    m->have_build_ev = prof;
+    m->build_launches = (uint32_t)nl;
+    m->launches += (uint64_t)nl;
+    s = check_cuda(m, "pm_build");
+    if (s != PM_OK) return s;
+    m->n = n;
+    m->built = true;
+    return PM_OK;
+}
+
+static pm_status query_common(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                              uint32_t nq, float* d_rad4, bool exact_only) {
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = validate_desc(m, desc, exact_only);
+    if (s != PM_OK) return s;
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_rad4))
+        return fail(m, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
+    if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_rad4)))
+        return fail(m, PM_ERR_INVALID, "query and radiance arrays must be 16-byte aligned");
+    return PM_OK;
+}
+
+pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
+                   float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, void* stream) {
+    pm_status s = query_common(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, false);
+    if (s != PM_OK) return s;
+    if (desc->mode == PM_MODE_ZHOU_COMPAT)
+        return fail(m, PM_ERR_UNSUPPORTED, "PM_MODE_ZHOU_COMPAT is not available in this build");
+    if (nq == 0) return PM_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    s = ensure_query_capacity(m, nq, st);
+    if (s != PM_OK) return s;
+    const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
+    const bool prof = m->profiling && !capturing(st);
+    if (prof) cudaEventRecord(m->ev[3], st);
+    int nl = 0;
+    const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, qpos, nq, st, &nl) : nullptr;
+    if (prof) cudaEventRecord(m->ev[4], st);
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
+    nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
+                    P<uint32_t>(m->counter), m->warps_per_block, m->rounds_per_chunk, st);
+    if (prof) cudaEventRecord(m->ev[5], st);
+    m->have_query_ev = prof;
+    m->query_launches = (uint32_t)nl;
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_query");
+}
+
+pm_status pm_query_bruteforce(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                              uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count,
+                              void* stream) {
+    pm_status s = query_common(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, true);
+    if (s != PM_OK) return s;
+    if (nq == 0) return PM_OK;
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
+    m->launches += (uint64_t)query_bruteforce(view_of(m), params_of(desc), reinterpret_cast<const float4*>(d_qpos4),
+                                              reinterpret_cast<const float4*>(d_qnrm4), nq, out,
+                                              reinterpret_cast<cudaStream_t>(stream));
+    return check_cuda(m, "pm_query_bruteforce");
+}
+
+pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                            uint32_t nq, const float* d_grad_rad4, const uint32_t* d_nbr, const float* d_r2,
+                            const uint32_t* d_count, float* d_grad_pow4, float* d_grad_pos4, void* stream) {
+    (void)desc; (void)d_qpos4; (void)d_qnrm4; (void)nq; (void)d_grad_rad4; (void)d_nbr; (void)d_r2; (void)d_count;
+    (void)d_grad_pow4; (void)d_grad_pos4; (void)stream;
+    return fail(m, PM_ERR_UNSUPPORTED, "pm_query_backward is not available in this build");
+}
+
+pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit_pos4, const float* d_hit_nrm4,
+                        const float* d_ray_dir4, const float* d_ray_origin4, const float* d_ray_influence4,
+                        const float* d_clr_diffuse4, const uint32_t* d_idx_shading, uint32_t n, float* d_io_radiance4,
+                        float* d_io_recip_dist, void* stream) {
+    (void)desc; (void)d_hit_pos4; (void)d_hit_nrm4; (void)d_ray_dir4; (void)d_ray_origin4; (void)d_ray_influence4;
+    (void)d_clr_diffuse4; (void)d_idx_shading; (void)n; (void)d_io_radiance4; (void)d_io_recip_dist; (void)stream;
+    return fail(m, PM_ERR_UNSUPPORTED, "pm_gather_for is not available in this build");
+}
+
+pm_status pm_scale_flux(pm_map* m, float scale, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!std::isfinite(scale)) return fail(m, PM_ERR_INVALID, "scale must be finite");
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    scale_flux(P<float4>(m->pow), m->n, scale, P<MapHeader>(m->hdr), reinterpret_cast<cudaStream_t>(stream));
+    m->launches += 1;
+    return check_cuda(m, "pm_scale_flux");
+}
+
+pm_status pm_compute_query_radii(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, uint32_t nq,
+                                 float* d_radii, void* stream) {
+    (void)desc; (void)d_qpos4; (void)nq; (void)d_radii; (void)stream;
+    return fail(m, PM_ERR_UNSUPPORTED, "pm_compute_query_radii is not available in this build");
+}
+
+pm_status pm_get_info(pm_map* m, pm_map_info* info, void* stream) {
+    if (!m || !info) return fail(m, PM_ERR_INVALID, "info is NULL");
+    std::memset(info, 0, sizeof(*info));
+    info->leaf_size = m->leaf_size;
+    info->num_photons = m->n;
+    if (!m->built) return PM_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    MapHeader h;
+    if (cudaMemcpyAsync(&h, m->hdr.ptr, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return check_cuda(m, "pm_get_info");
+    info->num_nodes = h.num_nodes;
+    info->device_errors = h.errors;
+    for (int a = 0; a < 3; ++a) { info->bounds_min[a] = h.lo[a]; info->bounds_max[a] = h.hi[a]; }
+    info->max_power = h.max_power;
+    info->launches = m->launches;
+    return PM_OK;
+}
+
+pm_status pm_set_profiling(pm_map* m, int enable) {
+    if (!m) return PM_ERR_INVALID;
+    if (enable) {
+        for (cudaEvent_t& e : m->ev)
+            if (!e && cudaEventCreate(&e) != cudaSuccess) return check_cuda(m, "pm_set_profiling");
+    }
+    m->profiling = enable != 0;
+    return PM_OK;
+}
+
+pm_status pm_last_timings(pm_map* m, pm_timings* out) {
+    if (!m || !out) return fail(m, PM_ERR_INVALID, "timings output is NULL");
+    std::memset(out, 0, sizeof(*out));
+    out->build_launches = m->build_launches;
+    out->query_launches = m->query_launches;
+    if (m->have_build_ev) {
+        if (cudaEventSynchronize(m->ev[2]) != cudaSuccess) return check_cuda(m, "pm_last_timings");
+        cudaEventElapsedTime(&out->build_ms, m->ev[0], m->ev[2]);
+        cudaEventElapsedTime(&out->build_sort_ms, m->ev[0], m->ev[1]);
+    }
+    if (m->have_query_ev) {
+        if (cudaEventSynchronize(m->ev[5]) != cudaSuccess) return check_cuda(m, "pm_last_timings");
+        cudaEventElapsedTime(&out->query_ms, m->ev[3], m->ev[5]);
+        cudaEventElapsedTime(&out->query_sort_ms, m->ev[3], m->ev[4]);
+        cudaEventElapsedTime(&out->query_kernel_ms, m->ev[4], m->ev[5]);
+    }
+    return check_cuda(m, "pm_last_timings");
+}
+
+pm_status pm_clear_errors(pm_map* m, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!m->hdr.ptr) return PM_OK;
+    cudaMemsetAsync(&P<MapHeader>(m->hdr)->errors, 0, sizeof(uint32_t), reinterpret_cast<cudaStream_t>(stream));
+    return check_cuda(m, "pm_clear_errors");
+}
+
+pm_status pm_export_tree(pm_map* m, uint32_t* host_nodes, uint32_t max_nodes, float* host_pos4, float* host_pow4,
+                         uint32_t max_photons) {
+    if (!m) return PM_ERR_INVALID;
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (cudaDeviceSynchronize() != cudaSuccess) return check_cuda(m, "pm_export_tree");
+    MapHeader h;
+    if (cudaMemcpy(&h, m->hdr.ptr, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return check_cuda(m, "pm_export_tree");
+    const uint32_t total_nodes = h.num_nodes + 1;
+    if (host_nodes) {
+        if (max_nodes < total_nodes) return fail(m, PM_ERR_INVALID, "need room for %u nodes", total_nodes);
+        if (cudaMemcpy(host_nodes, m->nodes.ptr, (size_t)total_nodes * sizeof(Node), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda(m, "pm_export_tree");
+    }
+    if (host_pos4 || host_pow4) {
+        if (max_photons < m->n) return fail(m, PM_ERR_INVALID, "need room for %u photons", m->n);
+        if (host_pos4 && m->n &&
+            cudaMemcpy(host_pos4, m->pos.ptr, (size_t)m->n * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda(m, "pm_export_tree");
+        if (host_pow4 && m->n &&
+            cudaMemcpy(host_pow4, m->pow.ptr, (size_t)m->n * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda(m, "pm_export_tree");
+    }
+    return PM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,337 @@
+// pm_build.cu -- point kd-tree build over photons.
+//
+// Replaces KDTreeGPU::BuildTree (KDTreeGPU.cpp:175-209) with its large-node
+// stage (empty-space cuts, longest-axis spatial median, KDTreeGPU.cpp:444-664,
+// GPU/kdtree.cu:467-824), small-node stage (KDTreeGPU.cpp:945-1154) and
+// preorder layout pass (GPU/kdtree.cu:1658-1770).  The new build has no host
+// synchronisation and a fixed launch sequence (graph-capturable):
+//
+//   1. k_bounds       photon bounds + largest flux channel (one pass, last
+//                     block finalises the header)
+//   2. k_morton       48-bit Morton code per photon in the cubic root cell
+//   3. radix sort     (code, caller index): caller index breaks ties, so the
+//                     order -- and the whole tree -- is deterministic
+//                     (the reference picks sides of split-plane ties at
+//                     random, GPU/kdtree.cu:806-815)
+//   4. k_gather       photons into tree order as SoA float4 records
+//   5. k_radix_tree   binary radix tree over the sorted codes (Karras 2012):
+//                     each internal node splits at the highest Morton bit
+//                     that differs inside its range, i.e. at the spatial
+//                     median of its cell on the axis that bit encodes
+//                     (x, y, z in turn = the longest axis of a cube cell)
+//   6. scan           keep flags of nodes holding more than leaf_size photons
+//                     -> compacted node indices (stream compaction)
+//   7. k_emit         64-byte nodes: two child slots, each a leaf range or an
+//                     internal node, leaf boxes computed from their photons
+//   8. k_refit        bottom-up child boxes (atomic arrival counters; boxes
+//                     are min/max so the result is order independent)
+#include "pm_internal.h"
+
+namespace pm {
+
+constexpr int kBoundsThreads = 256;
+constexpr int kBoundsBlocksMax = 1184;   // 8 per SM on 148 SMs
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// partials: 8 words per block + one arrival counter at partials[8 * gridDim.x].
+__global__ void __launch_bounds__(kBoundsThreads) k_bounds(const float4* __restrict__ pos,
+                                                            const float4* __restrict__ pw, uint32_t n,
+                                                            float* __restrict__ partials, MapHeader* hdr) {
+    float v[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, 0.0f};
+    uint32_t bad = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 p = pos[i];
+        const float4 w = pw[i];
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) { bad = 1; continue; }
+        v[0] = fminf(v[0], p.x); v[1] = fminf(v[1], p.y); v[2] = fminf(v[2], p.z);
+        v[3] = fmaxf(v[3], p.x); v[4] = fmaxf(v[4], p.y); v[5] = fmaxf(v[5], p.z);
+        v[6] = fmaxf(v[6], fmaxf(fmaxf(fabsf(w.x), fabsf(w.y)), fabsf(w.z)));
+    }
+    __shared__ float s_v[kBoundsThreads / 32][8];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { v[a] = warp_min(v[a]); v[a + 3] = warp_max(v[a + 3]); }
+    v[6] = warp_max(v[6]);
+    bad = __any_sync(0xffffffffu, bad) ? 1u : 0u;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 7; ++a) s_v[warp][a] = v[a];
+        s_v[warp][7] = __uint_as_float(bad);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBoundsThreads / 32; ++w) {
+            for (int a = 0; a < 3; ++a) { s_v[0][a] = fminf(s_v[0][a], s_v[w][a]); s_v[0][a + 3] = fmaxf(s_v[0][a + 3], s_v[w][a + 3]); }
+            s_v[0][6] = fmaxf(s_v[0][6], s_v[w][6]);
+            s_v[0][7] = __uint_as_float(__float_as_uint(s_v[0][7]) | __float_as_uint(s_v[w][7]));
+        }
+        for (int a = 0; a < 8; ++a) partials[8 * blockIdx.x + a] = s_v[0][a];
+        __threadfence();
+        unsigned int* counter = reinterpret_cast<unsigned int*>(partials + 8 * gridDim.x);
+        s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    float r[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, 0.0f};
+    uint32_t rb = 0;
+    for (uint32_t b = 0; b < gridDim.x; ++b) {
+        const float* q = partials + 8 * b;
+        for (int a = 0; a < 3; ++a) { r[a] = fminf(r[a], __ldcg(q + a)); r[a + 3] = fmaxf(r[a + 3], __ldcg(q + a + 3)); }
+        r[6] = fmaxf(r[6], __ldcg(q + 6));
+        rb |= __float_as_uint(__ldcg(q + 7));
+    }
+    for (int a = 0; a < 3; ++a) { hdr->lo[a] = r[a]; hdr->hi[a] = r[a + 3]; }
+    hdr->max_power = r[6];
+    hdr->fix_scale = (r[6] > 0.0f) ? __fdiv_rn(1099511627776.0f, r[6]) : 0.0f;   // 2^40 / max
+    hdr->n = n;
+    if (rb) atomicOr(&hdr->errors, kErrNonFinite);
+    *reinterpret_cast<unsigned int*>(partials + 8 * gridDim.x) = 0u;   // ready for the next build
+}
+
+__device__ __forceinline__ float morton_scale(const MapHeader* hdr) {
+    const float ext = fmaxf(fmaxf(__fsub_rn(hdr->hi[0], hdr->lo[0]), __fsub_rn(hdr->hi[1], hdr->lo[1])),
+                            __fsub_rn(hdr->hi[2], hdr->lo[2]));
+    return (ext > 0.0f && isfinite(ext)) ? __fdiv_rn(65536.0f, ext) : 0.0f;
+}
+
+__global__ void k_morton(const float4* __restrict__ pos, uint32_t n, const MapHeader* __restrict__ hdr,
+                         uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float scale = morton_scale(hdr);
+    const float4 p = pos[i];
+    keys[i] = morton48(p.x, p.y, p.z, hdr->lo, scale);
+    vals[i] = i;
+}
+
+__global__ void k_gather(const float4* __restrict__ pos, const float4* __restrict__ pw,
+                         const uint32_t* __restrict__ order, uint32_t n, int format, float4* __restrict__ out_pos,
+                         float4* __restrict__ out_pow) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t src = order[i];
+    const float4 p = pos[src];
+    const float4 w = pw[src];
+    const uint32_t dir = (format == 0) ? spherical_to_oct(p.w, w.w) : __float_as_uint(w.w);
+    out_pos[i] = make_float4(p.x, p.y, p.z, __uint_as_float(src));
+    out_pow[i] = make_float4(w.x, w.y, w.z, __uint_as_float(dir));
+}
+
+// Common-prefix length of sorted codes i and j, caller index breaking ties.
+__device__ __forceinline__ int delta(const uint64_t* __restrict__ keys, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = keys[i], b = keys[j];
+    if (a != b) return __clzll(a ^ b);
+    return 64 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+__global__ void k_radix_tree(const uint64_t* __restrict__ keys, uint32_t n, uint32_t leaf_size,
+                             uint32_t* __restrict__ kfirst, uint32_t* __restrict__ klast,
+                             uint32_t* __restrict__ ksplit, uint32_t* __restrict__ kkeep) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nn = n;
+    if (i >= nn - 1) return;
+    const int d = (delta(keys, nn, i, i + 1) > delta(keys, nn, i, i - 1)) ? 1 : -1;
+    const int dmin = delta(keys, nn, i, i - d);
+    int64_t lmax = 2;
+    while (delta(keys, nn, i, i + lmax * d) > dmin) lmax <<= 1;
+    int64_t l = 0;
+    for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, nn, i, i + (l + t) * d) > dmin) l += t;
+    const int64_t j = i + l * d;
+    const int dnode = delta(keys, nn, i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(keys, nn, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int64_t gamma = i + s * d + (d < 0 ? -1 : 0);
+    const int64_t first = d > 0 ? i : j, last = d > 0 ? j : i;
+    kfirst[i] = (uint32_t)first;
+    klast[i] = (uint32_t)last;
+    ksplit[i] = (uint32_t)gamma;
+    kkeep[i] = (last - first + 1 > (int64_t)leaf_size) ? 1u : 0u;
+}
+
+__device__ __forceinline__ void leaf_box(const float4* __restrict__ pos, uint32_t first, uint32_t cnt, ChildSlot& s) {
+    float lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY, hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const float4 p = pos[first + k];
+        lo0 = fminf(lo0, p.x); lo1 = fminf(lo1, p.y); lo2 = fminf(lo2, p.z);
+        hi0 = fmaxf(hi0, p.x); hi1 = fmaxf(hi1, p.y); hi2 = fmaxf(hi2, p.z);
+    }
+    s.lo[0] = lo0; s.lo[1] = lo1; s.lo[2] = lo2;
+    s.hi[0] = hi0; s.hi[1] = hi1; s.hi[2] = hi2;
+}
+
+__device__ __forceinline__ ChildSlot empty_slot() {
+    ChildSlot s;
+    s.lo[0] = s.lo[1] = s.lo[2] = INFINITY;
+    s.hi[0] = s.hi[1] = s.hi[2] = -INFINITY;
+    s.ref = kInvalid;
+    s.cnt = 0;
+    return s;
+}
+
+// Thread per radix-tree node; kept nodes write their compacted node.
+__global__ void k_emit(const float4* __restrict__ pos, uint32_t n, uint32_t leaf_size,
+                       const uint32_t* __restrict__ kfirst, const uint32_t* __restrict__ klast,
+                       const uint32_t* __restrict__ ksplit, const uint32_t* __restrict__ kkeep,
+                       const uint32_t* __restrict__ krank, const uint32_t* __restrict__ total, Node* __restrict__ nodes,
+                       uint32_t* __restrict__ parent, uint32_t* __restrict__ arrive, uint32_t* __restrict__ nleaf,
+                       MapHeader* hdr) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        const uint32_t m = (n > 1) ? *total : 0u;
+        hdr->num_nodes = m;
+        Node sr;
+        sr.c[1] = empty_slot();
+        if (n == 0) {
+            sr.c[0] = empty_slot();
+        } else if (m == 0) {   // whole map is one leaf
+            ChildSlot s;
+            leaf_box(pos, 0, n, s);
+            s.ref = 0;
+            s.cnt = n;
+            sr.c[0] = s;
+        } else {               // root box is filled in by k_refit
+            sr.c[0] = empty_slot();
+            sr.c[0].ref = 1;
+            sr.c[0].cnt = 0;
+        }
+        nodes[0] = sr;
+    }
+    if (n < 2 || i >= (uint64_t)n - 1 || !kkeep[i]) return;
+    const uint32_t id = 1 + krank[i];
+    const uint32_t first = kfirst[i], last = klast[i], gamma = ksplit[i];
+    Node nd;
+    uint32_t leaves = 0;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const uint32_t cf = side ? gamma + 1 : first;
+        const uint32_t cl = side ? last : gamma;
+        const uint32_t size = cl - cf + 1;
+        ChildSlot s;
+        if (size <= leaf_size) {
+            leaf_box(pos, cf, size, s);
+            s.ref = cf;
+            s.cnt = size;
+            ++leaves;
+        } else {
+            const uint32_t c = side ? gamma + 1 : gamma;   // radix-tree index of the internal child
+            const uint32_t cid = 1 + krank[c];
+            s = empty_slot();
+            s.ref = cid;
+            s.cnt = 0;
+            parent[cid] = (id << 1) | (uint32_t)side;
+        }
+        nd.c[side] = s;
+    }
+    nodes[id] = nd;
+    arrive[id] = leaves;
+    nleaf[id] = leaves;
+}
+
+// Thread per compacted node: nodes whose two children are leaves start a
+// climb; each climber writes its box into the parent's slot and the second
+// arrival at a parent continues upwards.
+__global__ void k_refit(Node* nodes, const uint32_t* __restrict__ parent, uint32_t* arrive,
+                        const uint32_t* __restrict__ nleaf, const MapHeader* __restrict__ hdr, uint32_t max_nodes) {
+    const uint32_t m = hdr->num_nodes;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m || t >= max_nodes) return;
+    uint32_t id = 1 + t;
+    if (nleaf[id] != 2) return;
+    for (;;) {
+        const float* s0 = nodes[id].c[0].lo;
+        const float* s1 = nodes[id].c[1].lo;
+        float box[6];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            box[a] = fminf(__ldcg(s0 + a), __ldcg(s1 + a));
+            box[a + 3] = fmaxf(__ldcg(s0 + 3 + a), __ldcg(s1 + 3 + a));
+        }
+        uint32_t p, side;
+        if (id == 1) { p = 0; side = 0; }
+        else { const uint32_t ps = parent[id]; p = ps >> 1; side = ps & 1u; }
+        float* dst = nodes[p].c[side].lo;
+#pragma unroll
+        for (int a = 0; a < 6; ++a) __stcg(dst + a, box[a]);
+        if (p == 0) break;
+        __threadfence();
+        const uint32_t old = atomicAdd(&arrive[p], 1u);
+        if (old != 1u) break;     // the sibling subtree is still being refitted
+        __threadfence();
+        id = p;
+    }
+}
+
+__global__ void k_scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        hdr->max_power = __fmul_rn(hdr->max_power, fabsf(scale));
+        hdr->fix_scale = (hdr->max_power > 0.0f) ? __fdiv_rn(1099511627776.0f, hdr->max_power) : 0.0f;
+    }
+    if (i >= n) return;
+    float4 w = pw[i];
+    w.x = __fmul_rn(w.x, scale);
+    w.y = __fmul_rn(w.y, scale);
+    w.z = __fmul_rn(w.z, scale);
+    pw[i] = w;
+}
+
+void scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st) {
+    const uint32_t blocks = n ? (n + 255) / 256 : 1;
+    k_scale_flux<<<blocks, 256, 0, st>>>(pw, n, scale, hdr);
+}
+
+int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
+              float4* out_pos, float4* out_pow, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
+              cudaStream_t st, cudaEvent_t sort_done) {
+    int nl = 0;
+    const uint32_t nb = (uint32_t)((n + kBoundsThreads - 1) / kBoundsThreads);
+    const uint32_t bblocks = nb < 1 ? 1 : (nb > (uint32_t)kBoundsBlocksMax ? (uint32_t)kBoundsBlocksMax : nb);
+    cudaMemsetAsync(&hdr->errors, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(bb.partials + 8 * bblocks, 0, sizeof(uint32_t), st);
+    k_bounds<<<bblocks, kBoundsThreads, 0, st>>>(in_pos, in_pow, n, reinterpret_cast<float*>(bb.partials), hdr);
+    ++nl;
+    if (n > 0) {
+        const uint32_t tb = 256, grid = (n + tb - 1) / tb;
+        k_morton<<<grid, tb, 0, st>>>(in_pos, n, hdr, bb.keys[0], bb.vals[0]);
+        uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
+        uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
+        const int cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl);
+        if (sort_done) cudaEventRecord(sort_done, st);
+        k_gather<<<grid, tb, 0, st>>>(in_pos, in_pow, vals[cur], n, format, out_pos, out_pow);
+        nl += 2;
+        if (n > 1) {
+            const uint32_t ni = n - 1, gi = (ni + tb - 1) / tb;
+            k_radix_tree<<<gi, tb, 0, st>>>(keys[cur], n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep);
+            uint32_t* total = bb.scratch + sort_scratch_words(n);
+            nl += 1 + exclusive_scan(bb.kkeep, bb.krank, ni, total + 1, total, st);
+            k_emit<<<gi, tb, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank,
+                                      total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
+            k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
+            return nl + 2;
+        }
+    } else if (sort_done) {
+        cudaEventRecord(sort_done, st);
+    }
+    k_emit<<<1, 32, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank, nullptr,
+                             nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
+    return nl + 1;
+}
+
+}  // namespace pm

@@ -1,0 +1,80 @@
+// pm_internal.h -- declarations shared by the engine's translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pm_common.cuh"
+
+namespace pm {
+
+// pm_sort.cu
+size_t scan_scratch_words(uint32_t n);
+int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch, uint32_t* total_out,
+                   cudaStream_t st);
+size_t sort_scratch_words(uint32_t n);
+int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
+                     cudaStream_t st, int* launches = nullptr);
+
+// Device buffers describing one built map (the build writes them, the
+// query reads them).  Pointers are device addresses.
+struct MapView {
+    const float4* pos;      // tree order: xyz, w = caller index bits
+    const float4* pow;      // tree order: rgb, w = octahedral direction bits
+    const Node* nodes;      // [0] = super-root, internal nodes from 1
+    MapHeader* hdr;
+    uint32_t n;             // photon count (host copy)
+};
+
+struct BuildBuffers {
+    uint64_t* keys[2];
+    uint32_t* vals[2];
+    uint32_t* scratch;      // sort / scan scratch
+    uint32_t* kfirst;       // Karras internal nodes: first, last, split
+    uint32_t* klast;
+    uint32_t* ksplit;
+    uint32_t* kkeep;        // keep flag (node holds more than leaf_size photons)
+    uint32_t* krank;        // exclusive scan of kkeep = compacted index - 1
+    uint32_t* parent;       // compacted node -> parent (node << 1 | side)
+    uint32_t* arrive;       // refit arrival counters per compacted node
+    uint32_t* nleaf;        // leaf children per compacted node
+    uint32_t* partials;     // bounds reduction partials (block count * 8 floats) + counter
+    uint32_t num_partials;
+};
+
+// pm_build.cu
+size_t build_bytes_needed(uint32_t n);
+// Returns the number of kernels launched; sort_done (if set) is recorded on
+// the stream right after the radix sort.
+int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
+              float4* out_pos, float4* out_pow, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
+              cudaStream_t st, cudaEvent_t sort_done = nullptr);
+void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st);
+
+// pm_query.cu
+struct QueryParams {
+    uint32_t k;
+    float r2;            // R^2 rounded in FP32
+    int filter;
+    float cone_k;
+    uint32_t min_found;
+};
+
+struct QueryOutputs {
+    float4* rad;         // required
+    uint32_t* nbr;       // optional
+    float* r2;           // optional
+    uint32_t* count;     // optional
+};
+
+int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint64_t* keys, uint32_t* vals,
+                       cudaStream_t st);
+int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
+               const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
+               int warps_per_block, int rounds_per_chunk, cudaStream_t st);
+int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
+                      uint32_t nq, const QueryOutputs& out, cudaStream_t st);
+int query_smem_bytes_per_warp(uint32_t k);
+
+}  // namespace pm

@@ -1,0 +1,473 @@
+// pm_query.cu -- exact-kNN photon-map radiance estimate.
+//
+// Replaces dev_RangeSearch + kernel_PhotonGather (GPU/photon_knn.cu:113-235,
+// 487-552) and the radius pipeline in front of it (KDTreePoint::
+// ComputeQueryRadii, KDTreePoint.cpp:229-248).  Where the reference runs
+// about three range searches per query (radius estimate, two histogram
+// refinements, gather) with one thread and a local-memory stack per query,
+// this kernel finds the exact k nearest photons in one pass:
+//
+//   * queries are processed in Morton order; one warp owns 32 consecutive
+//     queries (one per lane) and traverses the tree jointly: a child is
+//     visited when any lane's box lower bound passes its threshold, so
+//     control flow is warp-uniform and a leaf's photons are fetched once per
+//     warp with one coalesced load and broadcast by shuffles;
+//   * each lane keeps a max-heap of (d^2, tree position) keys in shared
+//     memory (k <= 128), ties broken by the photon's caller index;
+//   * a warp walks a chunk of consecutive rounds; the previous round's
+//     k-th distances bound the next round's search (triangle inequality:
+//     r_k(q) <= r_k(q') + |q - q'|), so most queries start with a tight
+//     radius instead of R;
+//   * the cone / Epanechnikov / box filter and the 1/(pi r^2)
+//     normalisation are fused into the epilogue; the weighted flux sum is
+//     accumulated in 64-bit fixed point, so the result does not depend on
+//     the order in which neighbours were found.
+#include "pm_internal.h"
+
+namespace pm {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+struct KnnArgs {
+    const float4* pos;
+    const float4* pow;
+    const Node* nodes;
+    MapHeader* hdr;
+    const float4* qpos;
+    const float4* qnrm;
+    const uint32_t* order;   // sorted slot -> caller query index (nullptr = identity)
+    uint32_t nq;
+    uint32_t k;
+    float r2max;
+    int filter;
+    float cone_k;
+    uint32_t min_found;
+    float4* out_rad;
+    uint32_t* out_nbr;
+    float* out_r2;
+    uint32_t* out_count;
+    uint32_t* work_counter;
+    uint32_t rounds_per_chunk;
+};
+
+// (d^2, position) keys; equal d^2 is resolved by the caller index stored in
+// pos[].w, which keeps the order identical to (d^2, caller index).
+__device__ __forceinline__ bool key_less(uint64_t a, uint64_t b, const float4* __restrict__ pos) {
+    const uint32_t ah = (uint32_t)(a >> 32), bh = (uint32_t)(b >> 32);
+    if (ah != bh) return ah < bh;
+    if (a == b) return false;
+    return __float_as_uint(pos[(uint32_t)a].w) < __float_as_uint(pos[(uint32_t)b].w);
+}
+
+// Max-heap helpers; element j of this lane lives at h[j * 32].
+__device__ __forceinline__ void heap_push(uint64_t* h, uint32_t& hn, uint64_t v, const float4* pos) {
+    uint32_t i = hn++;
+    while (i > 0) {
+        const uint32_t p = (i - 1) >> 1;
+        const uint64_t pv = h[p * 32];
+        if (!key_less(pv, v, pos)) break;
+        h[i * 32] = pv;
+        i = p;
+    }
+    h[i * 32] = v;
+}
+
+__device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t n, uint64_t v, const float4* pos) {
+    uint32_t i = 0;
+    for (;;) {
+        const uint32_t l = 2 * i + 1;
+        if (l >= n) break;
+        uint32_t c = l;
+        uint64_t cv = h[l * 32];
+        if (l + 1 < n) {
+            const uint64_t rv = h[(l + 1) * 32];
+            if (key_less(cv, rv, pos)) { c = l + 1; cv = rv; }
+        }
+        if (!key_less(v, cv, pos)) break;
+        h[i * 32] = cv;
+        i = c;
+    }
+    h[i * 32] = v;
+}
+
+__device__ __forceinline__ float filter_weight(int filter, float d2, float r2, float r, float cone_k) {
+    if (filter == 1) return __fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), __fmul_rn(cone_k, r)));
+    if (filter == 2) return __fsub_rn(1.0f, __fdiv_rn(d2, r2));
+    return 1.0f;
+}
+
+__device__ __forceinline__ double filter_norm(int filter, double r2, double cone_k) {
+    const double pi = 3.14159265358979323846;
+    if (filter == 1) return 1.0 / ((1.0 - 2.0 / (3.0 * cone_k)) * pi * r2);
+    if (filter == 2) return 2.0 / (pi * r2);
+    return 1.0 / (pi * r2);
+}
+
+// Epilogue for one lane: fixed-point filtered flux sum over the heap, optional
+// sorted neighbour list.  Shared by the tree and the brute-force kernels.
+// stride: distance between consecutive heap elements of this lane.
+__device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uint32_t hn, uint32_t qo, float nx,
+                             float ny, float nz) {
+    const uint32_t k = a.k;
+    const float r2 = (hn == k) ? __uint_as_float((uint32_t)(h[0] >> 32)) : a.r2max;
+    if (a.out_nbr) {   // heapsort in place -> ascending (d^2, index)
+        for (uint32_t end = hn; end > 1; --end) {
+            const uint64_t top = h[0];
+            const uint64_t last = h[(end - 1) * stride];
+            h[(end - 1) * stride] = top;
+            // sift `last` down within [0, end - 1)
+            uint32_t i = 0;
+            const uint32_t n = end - 1;
+            for (;;) {
+                const uint32_t l = 2 * i + 1;
+                if (l >= n) break;
+                uint32_t c = l;
+                uint64_t cv = h[l * stride];
+                if (l + 1 < n) {
+                    const uint64_t rv = h[(l + 1) * stride];
+                    if (key_less(cv, rv, a.pos)) { c = l + 1; cv = rv; }
+                }
+                if (!key_less(last, cv, a.pos)) break;
+                h[i * stride] = cv;
+                i = c;
+            }
+            h[i * stride] = last;
+        }
+        uint32_t* row = a.out_nbr + (size_t)qo * k;
+        for (uint32_t j = 0; j < k; ++j)
+            row[j] = (j < hn) ? __float_as_uint(a.pos[(uint32_t)h[j * stride]].w) : kInvalid;
+    }
+    float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)hn);
+    if (hn >= a.min_found && r2 > 0.0f) {
+        const float scale = a.hdr->fix_scale;
+        const float r = __fsqrt_rn(r2);
+        long long acc0 = 0, acc1 = 0, acc2 = 0;
+        for (uint32_t j = 0; j < hn; ++j) {
+            const uint64_t key = h[j * stride];
+            const float4 w = a.pow[(uint32_t)key];
+            if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
+            const float d2 = __uint_as_float((uint32_t)(key >> 32));
+            const float wt = filter_weight(a.filter, d2, r2, r, a.cone_k);
+            acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
+            acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
+            acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
+        }
+        if (scale > 0.0f) {
+            const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
+            rad.x = __double2float_rn((double)acc0 * f);
+            rad.y = __double2float_rn((double)acc1 * f);
+            rad.z = __double2float_rn((double)acc2 * f);
+        }
+    }
+    a.out_rad[qo] = rad;
+    if (a.out_r2) a.out_r2[qo] = r2;
+    if (a.out_count) a.out_count[qo] = hn;
+}
+
+__device__ __forceinline__ void load_slot(const Node* nodes, uint32_t node, uint32_t side, float* lo, float* hi,
+                                          uint32_t& ref, uint32_t& cnt) {
+    const float4* p = reinterpret_cast<const float4*>(&nodes[node].c[side]);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    lo[0] = a.x; lo[1] = a.y; lo[2] = a.z; hi[0] = a.w;
+    hi[1] = b.x; hi[2] = b.y; ref = __float_as_uint(b.z); cnt = __float_as_uint(b.w);
+}
+
+// One warp = 32 queries (one per lane) traversing together.
+__global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = lane_id();
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t k = a.k;
+    const size_t per_warp = (size_t)32 * k * sizeof(uint64_t) + kStackDepth * sizeof(uint32_t);
+    unsigned char* wbase = smem + per_warp * warp;
+    uint64_t* heap = reinterpret_cast<uint64_t*>(wbase) + lane;
+    uint32_t* stack = reinterpret_cast<uint32_t*>(wbase + (size_t)32 * k * sizeof(uint64_t));
+    const float r2max = a.r2max;
+    const uint32_t chunk_q = a.rounds_per_chunk * 32;
+    const uint32_t nchunks = (a.nq + chunk_q - 1) / chunk_q;
+
+    for (;;) {
+        uint32_t chunk = 0;
+        if (lane == 0) chunk = atomicAdd(a.work_counter, 1u);
+        chunk = __shfl_sync(kFull, chunk, 0);
+        if (chunk >= nchunks) break;
+        // previous round's result of this lane (for the radius bound)
+        float pqx = 0.f, pqy = 0.f, pqz = 0.f, pr = 0.f;
+        bool pvalid = false;
+        for (uint32_t round = 0; round < a.rounds_per_chunk; ++round) {
+            const uint32_t slot_q = chunk * chunk_q + round * 32 + lane;
+            const bool inrange = slot_q < a.nq;
+            if (!__any_sync(kFull, inrange)) break;
+            uint32_t qo = 0;
+            float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
+            bool active = false;
+            if (inrange) {
+                qo = a.order ? a.order[slot_q] : slot_q;
+                const float4 q = a.qpos[qo];
+                const float4 nn = a.qnrm[qo];
+                qx = q.x; qy = q.y; qz = q.z; nx = nn.x; ny = nn.y; nz = nn.z;
+                active = isfinite(qx) && isfinite(qy) && isfinite(qz);
+                if (!active) atomicOr(&a.hdr->errors, kErrQueryNonFinite);
+            }
+            // radius bound from the previous round's 32 queries
+            float tau0 = r2max;
+#pragma unroll 4
+            for (int s = 0; s < 32; ++s) {
+                const float sx = __shfl_sync(kFull, pqx, s), sy = __shfl_sync(kFull, pqy, s);
+                const float sz = __shfl_sync(kFull, pqz, s), sr = __shfl_sync(kFull, pr, s);
+                const bool sv = __shfl_sync(kFull, pvalid, s);
+                if (sv) {
+                    const float dq = __fsqrt_rn(d2_rn(qx, qy, qz, sx, sy, sz));
+                    const float b = __fmul_rn(__fadd_rn(sr, dq), 1.000244140625f);
+                    tau0 = fminf(tau0, __fmul_rn(__fmul_rn(b, b), 1.000244140625f));
+                }
+            }
+            uint32_t hn = 0;
+            bool full = false, todo = active;
+            while (__any_sync(kFull, todo)) {
+                // (re)start the search of the lanes in `todo`
+                const bool live = todo;
+                if (live) { hn = 0; full = false; }
+                uint64_t top = 0;
+                float tauf = 0.0f;
+                int sp = 0;
+                // current slot = the root slot of the super-root
+                float lo[3], hi[3];
+                uint32_t ref, cnt;
+                load_slot(a.nodes, 0, 0, lo, hi, ref, cnt);
+                bool have = true;
+                {
+                    const float lb = box_lb(qx, qy, qz, lo, hi);
+                    have = __any_sync(kFull, live && lb < tau0) && ref != kInvalid;
+                }
+                for (;;) {
+                    if (have) {
+                        if (cnt > 0) {
+                            // leaf: coalesced load, broadcast photon by photon
+                            float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (lane < cnt) mine = __ldg(a.pos + ref + lane);
+                            for (uint32_t j = 0; j < cnt; ++j) {
+                                const float px = __shfl_sync(kFull, mine.x, j);
+                                const float py = __shfl_sync(kFull, mine.y, j);
+                                const float pz = __shfl_sync(kFull, mine.z, j);
+                                if (!live) continue;
+                                const float d2 = d2_rn(qx, qy, qz, px, py, pz);
+                                const uint64_t key = ((uint64_t)__float_as_uint(d2) << 32) | (ref + j);
+                                if (!full) {
+                                    if (d2 < tau0) {
+                                        heap_push(heap, hn, key, a.pos);
+                                        if (hn == k) { full = true; top = heap[0]; tauf = __uint_as_float((uint32_t)(top >> 32)); }
+                                    }
+                                } else if (key_less(key, top, a.pos)) {
+                                    heap_sift_down(heap, k, key, a.pos);
+                                    top = heap[0];
+                                    tauf = __uint_as_float((uint32_t)(top >> 32));
+                                }
+                            }
+                            have = false;
+                        } else {
+                            float l0[3], h0[3], l1[3], h1[3];
+                            uint32_t r0, c0, r1, c1;
+                            load_slot(a.nodes, ref, 0, l0, h0, r0, c0);
+                            load_slot(a.nodes, ref, 1, l1, h1, r1, c1);
+                            const float lb0 = box_lb(qx, qy, qz, l0, h0);
+                            const float lb1 = box_lb(qx, qy, qz, l1, h1);
+                            const bool p0 = live && (full ? lb0 <= tauf : lb0 < tau0);
+                            const bool p1 = live && (full ? lb1 <= tauf : lb1 < tau0);
+                            const uint32_t b0 = __ballot_sync(kFull, p0), b1 = __ballot_sync(kFull, p1);
+                            const bool w0 = b0 != 0 && r0 != kInvalid, w1 = b1 != 0 && r1 != kInvalid;
+                            if (w0 && w1) {
+                                const uint32_t votes = __ballot_sync(kFull, (p0 || p1) && lb1 < lb0);
+                                const uint32_t voters = b0 | b1;
+                                const int near = (2 * __popc(votes) > __popc(voters)) ? 1 : 0;
+                                if (sp >= kStackDepth) {
+                                    if (lane == 0) atomicOr(&a.hdr->errors, kErrStack);
+                                } else {
+                                    if (lane == 0) stack[sp] = (ref << 1) | (uint32_t)(1 - near);
+                                    ++sp;
+                                }
+                                if (near) { lo[0] = l1[0]; lo[1] = l1[1]; lo[2] = l1[2]; hi[0] = h1[0]; hi[1] = h1[1]; hi[2] = h1[2]; ref = r1; cnt = c1; }
+                                else { lo[0] = l0[0]; lo[1] = l0[1]; lo[2] = l0[2]; hi[0] = h0[0]; hi[1] = h0[1]; hi[2] = h0[2]; ref = r0; cnt = c0; }
+                            } else if (w0) {
+                                ref = r0; cnt = c0;
+                            } else if (w1) {
+                                ref = r1; cnt = c1;
+                            } else {
+                                have = false;
+                            }
+                        }
+                        continue;
+                    }
+                    // pop until a slot passes some lane's current threshold
+                    bool found = false;
+                    while (sp > 0) {
+                        --sp;
+                        __syncwarp();
+                        const uint32_t e = stack[sp];
+                        load_slot(a.nodes, e >> 1, e & 1u, lo, hi, ref, cnt);
+                        const float lb = box_lb(qx, qy, qz, lo, hi);
+                        const bool p = live && (full ? lb <= tauf : lb < tau0);
+                        if (__any_sync(kFull, p)) { found = true; break; }
+                    }
+                    if (!found) break;
+                    have = true;
+                }
+                // a bound that admitted fewer than k photons was too tight: redo with R
+                todo = live && !full && tau0 < r2max;
+                if (todo) tau0 = r2max;
+                __syncwarp();
+            }
+            // k-th distance of this lane, read before the epilogue reorders the heap
+            const float rk2 = (active && full) ? __uint_as_float((uint32_t)(heap[0] >> 32)) : 0.0f;
+            if (inrange) {
+                if (active) {
+                    finish_query(a, heap, 32, hn, qo, nx, ny, nz);
+                } else {
+                    a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (a.out_r2) a.out_r2[qo] = r2max;
+                    if (a.out_count) a.out_count[qo] = 0;
+                    if (a.out_nbr)
+                        for (uint32_t j = 0; j < k; ++j) a.out_nbr[(size_t)qo * k + j] = kInvalid;
+                }
+            }
+            pqx = qx; pqy = qy; pqz = qz;
+            pvalid = active && full;
+            pr = pvalid ? __fsqrt_rn(rk2) : 0.0f;
+            __syncwarp();
+        }
+    }
+}
+
+// Brute force: thread per query, every photon staged through shared memory.
+constexpr int kBruteThreads = 64;
+constexpr int kBruteTile = 512;
+
+__global__ void __launch_bounds__(kBruteThreads) k_knn_brute(KnnArgs a, uint32_t n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float4* tile = reinterpret_cast<float4*>(smem);
+    uint64_t* heap = reinterpret_cast<uint64_t*>(smem + kBruteTile * sizeof(float4)) + threadIdx.x;
+    const uint32_t q = blockIdx.x * kBruteThreads + threadIdx.x;
+    const bool valid = q < a.nq;
+    float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
+    if (valid) {
+        const float4 p = a.qpos[q], nn = a.qnrm[q];
+        qx = p.x; qy = p.y; qz = p.z; nx = nn.x; ny = nn.y; nz = nn.z;
+    }
+    uint32_t hn = 0;
+    uint64_t top = 0;
+    const uint32_t k = a.k;
+    // the heap helpers use a stride of 32; this kernel uses its own stride
+    for (uint32_t base = 0; base < n; base += kBruteTile) {
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < kBruteTile && base + t < n; t += kBruteThreads) tile[t] = a.pos[base + t];
+        __syncthreads();
+        const uint32_t lim = min((uint32_t)kBruteTile, n - base);
+        if (!valid) continue;
+        for (uint32_t t = 0; t < lim; ++t) {
+            const float4 p = tile[t];
+            const float d2 = d2_rn(qx, qy, qz, p.x, p.y, p.z);
+            if (!(d2 < a.r2max)) continue;
+            const uint64_t key = ((uint64_t)__float_as_uint(d2) << 32) | (base + t);
+            if (hn < k) {
+                uint32_t i = hn++;
+                while (i > 0) {
+                    const uint32_t pi = (i - 1) >> 1;
+                    const uint64_t pv = heap[pi * kBruteThreads];
+                    if (!key_less(pv, key, a.pos)) break;
+                    heap[i * kBruteThreads] = pv;
+                    i = pi;
+                }
+                heap[i * kBruteThreads] = key;
+                top = heap[0];
+            } else if (key_less(key, top, a.pos)) {
+                uint32_t i = 0;
+                for (;;) {
+                    const uint32_t l = 2 * i + 1;
+                    if (l >= k) break;
+                    uint32_t c = l;
+                    uint64_t cv = heap[l * kBruteThreads];
+                    if (l + 1 < k) {
+                        const uint64_t rv = heap[(l + 1) * kBruteThreads];
+                        if (key_less(cv, rv, a.pos)) { c = l + 1; cv = rv; }
+                    }
+                    if (!key_less(key, cv, a.pos)) break;
+                    heap[i * kBruteThreads] = cv;
+                    i = c;
+                }
+                heap[i * kBruteThreads] = key;
+                top = heap[0];
+            }
+        }
+    }
+    if (valid) finish_query(a, heap, kBruteThreads, hn, q, nx, ny, nz);
+}
+
+__global__ void k_query_morton(const float4* __restrict__ qpos, uint32_t nq, const MapHeader* __restrict__ hdr,
+                               uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const float ext = fmaxf(fmaxf(__fsub_rn(hdr->hi[0], hdr->lo[0]), __fsub_rn(hdr->hi[1], hdr->lo[1])),
+                            __fsub_rn(hdr->hi[2], hdr->lo[2]));
+    const float scale = (ext > 0.0f && isfinite(ext)) ? __fdiv_rn(65536.0f, ext) : 0.0f;
+    const float4 p = qpos[i];
+    keys[i] = morton48(p.x, p.y, p.z, hdr->lo, scale);
+    vals[i] = i;
+}
+
+int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint64_t* keys, uint32_t* vals,
+                      cudaStream_t st) {
+    if (!nq) return 0;
+    k_query_morton<<<(nq + 255) / 256, 256, 0, st>>>(qpos, nq, hdr, keys, vals);
+    return 1;
+}
+
+int query_smem_bytes_per_warp(uint32_t k) {
+    return (int)(32 * k * sizeof(uint64_t) + kStackDepth * sizeof(uint32_t));
+}
+
+static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
+                         const uint32_t* order, uint32_t nq, const QueryOutputs& out) {
+    KnnArgs a;
+    a.pos = m.pos; a.pow = m.pow; a.nodes = m.nodes; a.hdr = m.hdr;
+    a.qpos = qpos; a.qnrm = qnrm; a.order = order; a.nq = nq;
+    a.k = p.k; a.r2max = p.r2; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
+    a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
+    a.work_counter = nullptr; a.rounds_per_chunk = 1;
+    return a;
+}
+
+int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
+              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
+              int warps_per_block, int rounds_per_chunk, cudaStream_t st) {
+    if (!nq) return 0;
+    KnnArgs a = make_args(m, p, qpos, qnrm, order, nq, out);
+    a.work_counter = work_counter;
+    a.rounds_per_chunk = (uint32_t)rounds_per_chunk;
+    const int smem = query_smem_bytes_per_warp(p.k) * warps_per_block;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_knn_tree, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_tree, 32 * warps_per_block, smem);
+    if (per_sm < 1) per_sm = 1;
+    const uint32_t chunk_q = (uint32_t)rounds_per_chunk * 32;
+    const uint32_t nchunks = (nq + chunk_q - 1) / chunk_q;
+    uint32_t grid = (uint32_t)(sms * per_sm);
+    const uint32_t need = (nchunks + warps_per_block - 1) / warps_per_block;
+    if (grid > need) grid = need;
+    cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st);
+    k_knn_tree<<<grid, 32 * warps_per_block, smem, st>>>(a);
+    return 1;
+}
+
+int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
+                     uint32_t nq, const QueryOutputs& out, cudaStream_t st) {
+    if (!nq) return 0;
+    KnnArgs a = make_args(m, p, qpos, qnrm, nullptr, nq, out);
+    const int smem = kBruteTile * (int)sizeof(float4) + kBruteThreads * (int)p.k * (int)sizeof(uint64_t);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_knn_brute, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_knn_brute<<<(nq + kBruteThreads - 1) / kBruteThreads, kBruteThreads, smem, st>>>(a, m.n);
+    return 1;
+}
+
+}  // namespace pm

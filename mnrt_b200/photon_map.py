@@ -1,0 +1,184 @@
+"""Host-side mirror of MNRT's PhotonMap / KDTreePoint interface over the C ABI.
+
+    pm = PhotonMap(max_photons, scene_min, scene_max, global_q_radius_max)
+    pm.merge(photon_data, d_is_valid)        # PhotonMap::Merge       (PhotonMap.cpp:181)
+    pm.scale_flux(1.0 / n_paths)             # PhotonMap::ScaleFlux   (PhotonMap.cpp:186)
+    pm.build_map()                           # PhotonMap::BuildMap    (PhotonMap.cpp:157)
+    pm.set_knn_target_count(100)             # PhotonMap::SetKNNTargetCount (PhotonMap.h:257)
+    pm.gather_for(sp, rays, clr, idx, rad, recip)   # PhotonMap::GatherFor (PhotonMap.cpp:234)
+
+plus the engine's direct calls (build / query / query_backward) on torch CUDA
+tensors.  Device memory and streams come from torch; all computation runs in
+libpmgpu.so.  Tensors are float32, contiguous, 4 floats per element.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib as L
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("engine buffers must be CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("engine buffers must be contiguous")
+    return t.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+@dataclass
+class PhotonData:
+    """MNRT's PhotonData (KernelDefs.h:537-629): positions (xyz, azimuth phi)
+    and powers (rgb, polar theta), or the engine's packed layout."""
+    positions: torch.Tensor   # (n, 4) float32, CUDA
+    powers: torch.Tensor      # (n, 4) float32, CUDA
+    packed: bool = False
+
+    @property
+    def num_photons(self) -> int:
+        return int(self.positions.shape[0])
+
+
+@dataclass
+class ShadingPoints:
+    """Query side of MNRT's ShadingPoints (KernelDefs.h:160-291)."""
+    pt_inter: torch.Tensor    # (n, 4) hit positions
+    normals_s: torch.Tensor   # (n, 4) shading normals
+
+
+@dataclass
+class RayChunk:
+    """The gather rays that produced the shading points (RayPool.h:162-178)."""
+    origins: torch.Tensor     # (n, 4)
+    dirs: torch.Tensor        # (n, 4)
+    influences: torch.Tensor  # (n, 4)
+
+
+class PhotonMap:
+    def __init__(self, max_photons: int, scene_aabb_min=(0.0, 0.0, 0.0), scene_aabb_max=(1.0, 1.0, 1.0),
+                 global_q_radius_max: float = 0.1, knn_target_count: int = 100):
+        self._lib = L.load()
+        h = C.c_void_p()
+        lo = (C.c_float * 3)(*scene_aabb_min)
+        hi = (C.c_float * 3)(*scene_aabb_max)
+        st = self._lib.pm_create(C.byref(h), int(max_photons), lo, hi, float(global_q_radius_max))
+        if st != L.PM_OK:
+            raise L.PMError(st, "pm_create failed")
+        self._h = h
+        self.max_photons = int(max_photons)
+        self.r_max = float(global_q_radius_max)
+        self.k = int(knn_target_count)   # MNRT PhotonMap default m_knnTargetCount = 100 (PhotonMap.cpp:111)
+        self._staged: list[PhotonData] = []
+        self._num_staged = 0
+        self.num_photons = 0
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.pm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- reference-shaped API ------------------------------------------------
+    def set_knn_target_count(self, k: int) -> None:
+        self.k = int(k)
+
+    def get_photon_count(self) -> int:
+        return self.num_photons
+
+    def set_tuning(self, leaf_size: int = 16, warps_per_block: int = 4, rounds_per_chunk: int = 8) -> None:
+        L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk), self._h)
+
+    def reserve(self, max_photons: int, max_queries: int) -> None:
+        L.check(self._lib.pm_reserve(self._h, int(max_photons), int(max_queries)), self._h)
+
+    # -- engine API --------------------------------------------------------------
+    def build(self, positions: torch.Tensor, powers: torch.Tensor, packed: bool = True, stream=None) -> None:
+        n = int(positions.shape[0])
+        if positions.dtype != torch.float32 or powers.dtype != torch.float32:
+            raise ValueError("photon arrays must be float32")
+        if positions.shape != (n, 4) or powers.shape != (n, 4):
+            raise ValueError("photon arrays must be (n, 4)")
+        fmt = L.PM_PHOTONS_PACKED if packed else L.PM_PHOTONS_REFERENCE
+        L.check(self._lib.pm_build(self._h, _ptr(positions) if n else None, _ptr(powers) if n else None, n, fmt,
+                                   _stream(stream)), self._h)
+        self.num_photons = n
+
+    def desc(self, k=None, r_max=None, filter="box", cone_k=1.0, min_found=0, sorted_queries=True,
+             mode=L.PM_MODE_EXACT, refine_iters=2) -> L.QueryDesc:
+        return L.QueryDesc(k=int(k if k is not None else self.k), r_max=float(r_max if r_max is not None else self.r_max),
+                           filter=L.FILTERS[filter] if isinstance(filter, str) else int(filter), cone_k=float(cone_k),
+                           mode=int(mode), min_found=int(min_found),
+                           order=L.PM_ORDER_SORTED if sorted_queries else L.PM_ORDER_AS_GIVEN,
+                           refine_iters=int(refine_iters))
+
+    def query(self, qpos: torch.Tensor, qnrm: torch.Tensor, want_nbr: bool = False, brute_force: bool = False,
+              out: dict | None = None, stream=None, **kw) -> dict:
+        """Exact-kNN radiance estimate; returns rad (nq,4) [, nbr (nq,k), r2, count]."""
+        d = self.desc(**kw)
+        nq = int(qpos.shape[0])
+        dev = qpos.device
+        if out is None:
+            out = {"rad": torch.empty((nq, 4), dtype=torch.float32, device=dev),
+                   "r2": torch.empty((nq,), dtype=torch.float32, device=dev),
+                   "count": torch.empty((nq,), dtype=torch.int32, device=dev)}
+            if want_nbr:
+                out["nbr"] = torch.empty((nq, d.k), dtype=torch.int32, device=dev)
+        fn = self._lib.pm_query_bruteforce if brute_force else self._lib.pm_query
+        L.check(fn(self._h, C.byref(d), _ptr(qpos), _ptr(qnrm), nq, _ptr(out["rad"]), _ptr(out.get("nbr")),
+                   _ptr(out.get("r2")), _ptr(out.get("count")), _stream(stream)), self._h)
+        return out
+
+    def info(self, stream=None) -> L.MapInfo:
+        i = L.MapInfo()
+        L.check(self._lib.pm_get_info(self._h, C.byref(i), _stream(stream)), self._h)
+        return i
+
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(self._lib.pm_set_profiling(self._h, int(enable)), self._h)
+
+    def last_timings(self) -> L.Timings:
+        t = L.Timings()
+        L.check(self._lib.pm_last_timings(self._h, C.byref(t)), self._h)
+        return t
+
+    def clear_errors(self, stream=None) -> None:
+        L.check(self._lib.pm_clear_errors(self._h, _stream(stream)), self._h)
+
+    def export_tree(self):
+        """(nodes uint32 (m+1, 16), pos float32 (n, 4), pow float32 (n, 4)) in tree order."""
+        import numpy as np
+        info = self.info()
+        m = info.num_nodes + 1
+        nodes = np.zeros((m, 16), np.uint32)
+        pos = np.zeros((max(self.num_photons, 1), 4), np.float32)
+        pw = np.zeros((max(self.num_photons, 1), 4), np.float32)
+        L.check(self._lib.pm_export_tree(self._h, nodes.ctypes.data, m, pos.ctypes.data, pw.ctypes.data,
+                                         pos.shape[0]), self._h)
+        return nodes, pos[: self.num_photons], pw[: self.num_photons]
+
+    def scale_flux(self, scale: float, stream=None) -> None:
+        """PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): RGB flux only."""
+        if self.num_photons == 0:
+            return
+        L.check(self._lib.pm_scale_flux(self._h, float(scale), _stream(stream)), self._h)

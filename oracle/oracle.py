@@ -1,0 +1,136 @@
+"""ctypes wrapper of the CPU oracle (oracle/pm_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs.  The engine never imports it.
+Parity is unpinned (the reference ships no golden vectors and cannot be
+compiled here); see the header of pm_oracle.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+
+_lib = None
+
+
+def _build() -> None:
+    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    src = HERE / "pm_oracle.cpp"
+    if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        _build()
+    lib = C.CDLL(str(LIB_PATH))
+    P = C.c_void_p
+    u32, f32, i32 = C.c_uint32, C.c_float, C.c_int
+    sig = {
+        "orc_version": (i32, []),
+        "orc_d2": (f32, [f32] * 6),
+        "orc_oct_encode": (u32, [f32, f32, f32]),
+        "orc_oct_decode": (None, [u32, P]),
+        "orc_front": (i32, [f32, f32, f32, u32]),
+        "orc_sincos": (None, [C.c_double, P]),
+        "orc_spherical_to_oct": (u32, [f32, f32]),
+        "orc_pack_reference_photons": (None, [P, P, u32, P, P]),
+        "orc_knn_brute": (None, [P, u32, P, u32, u32, f32, P, P, P, P, i32]),
+        "orc_kdtree_build": (P, [P, u32]),
+        "orc_kdtree_free": (None, [P]),
+        "orc_knn_kdtree": (None, [P, P, u32, u32, f32, P, P, P, P, i32]),
+        "orc_radiance_fp64": (None, [P, P, P, P, u32, P, P, u32, f32, i32, f32, u32, P, i32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _c(a: np.ndarray, dtype) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def pack_reference(pos4: np.ndarray, pow4: np.ndarray):
+    """Reference-layout photons -> packed records (pos.w = index, pow.w = oct)."""
+    lib = load()
+    pos4, pow4 = _c(pos4, np.float32), _c(pow4, np.float32)
+    n = pos4.shape[0]
+    op = np.empty_like(pos4)
+    ow = np.empty_like(pow4)
+    lib.orc_pack_reference_photons(pos4.ctypes.data, pow4.ctypes.data, n, op.ctypes.data, ow.ctypes.data)
+    return op, ow
+
+
+def knn_brute(pos4, q4, k: int, r_max: float, threads: int = 0):
+    """Exact kNN by definition.  Returns (idx (nq,k) uint32, d2 (nq,k), count (nq,), r2 (nq,))."""
+    lib = load()
+    pos4, q4 = _c(pos4, np.float32), _c(q4, np.float32)
+    n, nq = pos4.shape[0], q4.shape[0]
+    idx = np.empty((nq, k), np.uint32)
+    d2 = np.empty((nq, k), np.float32)
+    cnt = np.empty(nq, np.uint32)
+    r2 = np.empty(nq, np.float32)
+    lib.orc_knn_brute(pos4.ctypes.data, n, q4.ctypes.data, nq, k, r_max, idx.ctypes.data, d2.ctypes.data,
+                      cnt.ctypes.data, r2.ctypes.data, threads)
+    return idx, d2, cnt, r2
+
+
+class KdTree:
+    """The CPU baseline: median-split point kd-tree + bounded-heap kNN."""
+
+    def __init__(self, pos4: np.ndarray):
+        self._lib = load()
+        self._pos = _c(pos4, np.float32)
+        self._h = self._lib.orc_kdtree_build(self._pos.ctypes.data, self._pos.shape[0])
+
+    def knn(self, q4, k: int, r_max: float, threads: int = 0):
+        q4 = _c(q4, np.float32)
+        nq = q4.shape[0]
+        idx = np.empty((nq, k), np.uint32)
+        d2 = np.empty((nq, k), np.float32)
+        cnt = np.empty(nq, np.uint32)
+        r2 = np.empty(nq, np.float32)
+        self._lib.orc_knn_kdtree(self._h, q4.ctypes.data, nq, k, r_max, idx.ctypes.data, d2.ctypes.data,
+                                 cnt.ctypes.data, r2.ctypes.data, threads)
+        return idx, d2, cnt, r2
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_kdtree_free(self._h)
+            self._h = None
+
+
+FILTER_IDS = {"box": 0, "cone": 1, "epanechnikov": 2}
+
+
+def radiance_fp64(pos4, pow4, q4, n4, nbr, count, k: int, r_max: float, filt: str = "box", cone_k: float = 1.0,
+                  min_found: int = 0, threads: int = 0) -> np.ndarray:
+    """FP64 estimate over the given neighbour sets; (nq, 3) float64."""
+    lib = load()
+    pos4, pow4, q4, n4 = (_c(a, np.float32) for a in (pos4, pow4, q4, n4))
+    nbr, count = _c(nbr, np.uint32), _c(count, np.uint32)
+    nq = q4.shape[0]
+    out = np.empty((nq, 3), np.float64)
+    lib.orc_radiance_fp64(pos4.ctypes.data, pow4.ctypes.data, q4.ctypes.data, n4.ctypes.data, nq, nbr.ctypes.data,
+                          count.ctypes.data, k, r_max, FILTER_IDS[filt], cone_k, min_found, out.ctypes.data, threads)
+    return out
+
+
+def threads_available() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1

@@ -1,0 +1,414 @@
+// pm_oracle.cpp -- CPU oracle for the photon-map kNN radiance estimate.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine in
+// mnrt_b200/; it is linked only by tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference legs of bench.py.  The product never calls it.
+//
+// PARITY UNPINNED: the reference (jonike/mnrt) ships no tests, golden vectors
+// or fixtures for this path, and its path cannot be compiled here (legacy
+// texture<> references removed in CUDA 12, the absent CUDA-SDK cutil headers
+// and the absent, unvendored CUDPP library).  The oracle therefore restates
+// the reference's algorithm from its source and is cross-checked against an
+// independent numpy restatement and the committed fixtures in tests/golden/.
+//
+// What is restated, and from where (paths inside the reference project):
+//   * range membership is strict:  d^2 < r^2                GPU/photon_knn.cu:189
+//   * front-face test: dot(n, -inDir) > 0 -> weight 1 else 0 GPU/photon_knn.cu:196-208
+//   * estimate E = sum(alpha * flux) / (pi * r^2_used), with
+//     r^2_used = max d^2 of the found photons when >= k were found,
+//     otherwise the query radius^2; E = 0 when r^2_used == 0  GPU/photon_knn.cu:221-232
+//   * estimates from fewer than 8 photons are zeroed          GPU/photon_knn.cu:518-519
+//     (exposed as the min_found parameter)
+//   * photon layout: position.w = azimuth phi, power.w = polar theta,
+//     direction = (sin t cos p, sin t sin p, cos t)           GPU/photon_dev.h:71-113,
+//                                                              GPU/mncudautil_dev.h:345-352
+//   * Zhou histogram radius refinement (compat mode)          GPU/kdtree_point.cu:118-267
+//
+// The engine's own contract on top of that (it defines "exact kNN", which the
+// reference only approximates, Help/MNRT_Documentation.html section 4.2):
+//   * d^2 = ((dx*dx) + (dy*dy)) + (dz*dz), dx = px - qx, every operation
+//     rounded to nearest FP32 with no contraction (build with -ffp-contract=off)
+//   * N(q) = the k photons with the smallest (d^2, photon index) among those
+//     with d^2 < R^2;  count = |N(q)|;  r^2 = d^2 of the k-th when count == k,
+//     else R^2 (R^2 itself rounded in FP32)
+//   * incident directions are stored octahedral-encoded in 2 x 16 bits; the
+//     front test runs in FP32 on the decoded (unnormalised) vector
+//   * cone filter (Jensen 2001): w = 1 - d/(kc r), norm 1/((1 - 2/(3kc)) pi r^2)
+//     Epanechnikov (2-D):        w = 1 - d^2/r^2, norm 2/(pi r^2)
+//     box (the reference's):     w = 1,           norm 1/(pi r^2)
+//
+// Build: see oracle/Makefile (g++ -O2 -ffp-contract=off -fno-fast-math).
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#ifdef __FAST_MATH__
+#error "the oracle must be built without -ffast-math (IEEE rounding of every operation)"
+#endif
+// x86-64 evaluates float/double in SSE registers (FLT_EVAL_METHOD == 0) and
+// -ffp-contract=off keeps every a*b+c as two roundings.
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+inline uint32_t f2u(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float u2f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+// ---------------------------------------------------------------- contract --
+
+// Squared distance, fixed evaluation order, FP32, no contraction.
+inline float d2_f32(float qx, float qy, float qz, float px, float py, float pz) {
+    float dx = px - qx, dy = py - qy, dz = pz - qz;
+    float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    float s = xx + yy;
+    return s + zz;
+}
+
+// Octahedral direction code: 16-bit snorm u (low half) and v (high half).
+inline void oct_decode(uint32_t bits, float out[3]) {
+    int16_t iu = (int16_t)(bits & 0xffffu), iv = (int16_t)(bits >> 16);
+    const float s = 1.0f / 32767.0f;
+    float fu = (float)iu * s, fv = (float)iv * s;
+    float au = std::fabs(fu), av = std::fabs(fv);
+    float z = (1.0f - au) - av;
+    float x = fu, y = fv;
+    if (z < 0.0f) {
+        x = (1.0f - av) * (fu >= 0.0f ? 1.0f : -1.0f);
+        y = (1.0f - au) * (fv >= 0.0f ? 1.0f : -1.0f);
+    }
+    out[0] = x; out[1] = y; out[2] = z;
+}
+
+inline int32_t snorm16(float f) {
+    float t = f * 32767.0f;
+    float r = std::nearbyint(t);  // round half to even (default rounding mode)
+    if (r > 32767.0f) r = 32767.0f;
+    if (r < -32767.0f) r = -32767.0f;
+    return (int32_t)r;
+}
+
+inline uint32_t oct_encode(float dx, float dy, float dz) {
+    float s = (std::fabs(dx) + std::fabs(dy)) + std::fabs(dz);
+    if (!(s > 0.0f)) return 0u;  // degenerate direction -> (0,0,1)
+    float px = dx / s, py = dy / s;
+    if (dz < 0.0f) {
+        float ax = std::fabs(px), ay = std::fabs(py);
+        float nx = (1.0f - ay) * (px >= 0.0f ? 1.0f : -1.0f);
+        float ny = (1.0f - ax) * (py >= 0.0f ? 1.0f : -1.0f);
+        px = nx; py = ny;
+    }
+    uint32_t u = (uint32_t)(snorm16(px) & 0xffff), v = (uint32_t)(snorm16(py) & 0xffff);
+    return u | (v << 16);
+}
+
+// front: dot(n, -dir) > 0, FP32, fixed order.
+inline bool front_f32(float nx, float ny, float nz, uint32_t dirbits) {
+    float d[3];
+    oct_decode(dirbits, d);
+    float a = nx * (-d[0]), b = ny * (-d[1]), c = nz * (-d[2]);
+    float s = a + b;
+    return (s + c) > 0.0f;
+}
+
+// Deterministic sin/cos in FP64 for the spherical ingest: Cody-Waite
+// reduction by pi/2 (split into a 33-bit head and a tail) and Taylor series
+// to degree 21/22 on [-pi/4, pi/4].  Every operation is a single IEEE double
+// rounding, so the CUDA side (explicit __dmul_rn/__dadd_rn) gives the same bits.
+constexpr double kPio2Hi = 0x1.921fb544p+0;            // pi/2 to 33 bits
+constexpr double kPio2Lo = 0x1.0b4611a626331p-34;      // pi/2 - kPio2Hi
+constexpr double kTwoOverPi = 0x1.45f306dc9c883p-1;    // 2/pi
+
+inline void sincos_det(double x, double* s_out, double* c_out) {
+    double kq = std::nearbyint(x * kTwoOverPi);
+    double t1 = kq * kPio2Hi;
+    double r0 = x - t1;
+    double t2 = kq * kPio2Lo;
+    double r = r0 - t2;
+    double r2 = r * r;
+    // sin(r) = r * (1 - r2/3! + r2^2/5! - ...), Horner over r2
+    double ps = 1.0 / 51090942171709440000.0;  // 1/21!
+    const double sc[] = {1.0 / 121645100408832000.0, 1.0 / 355687428096000.0,
+                         1.0 / 1307674368000.0, 1.0 / 6227020800.0, 1.0 / 39916800.0,
+                         1.0 / 362880.0, 1.0 / 5040.0, 1.0 / 120.0, 1.0 / 6.0, 1.0};
+    const double sg[] = {-1.0, 1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0};
+    // coefficient of r^(2j+1) is (-1)^j / (2j+1)!; j = 10 .. 0
+    ps = ps;  // (-1)^10 = +1
+    for (int i = 0; i < 10; ++i) {
+        double m = ps * r2;
+        ps = m + sg[i] * sc[i];
+    }
+    double sv = ps * r;
+    // cos(r) = 1 - r2/2! + ..., coefficient of r^(2j) is (-1)^j/(2j)!; j = 11 .. 0
+    double pc = -1.0 / 1124000727777607680000.0;  // -1/22!
+    const double cc[] = {1.0 / 2432902008176640000.0, 1.0 / 6402373705728000.0,
+                         1.0 / 20922789888000.0, 1.0 / 87178291200.0, 1.0 / 479001600.0,
+                         1.0 / 3628800.0, 1.0 / 40320.0, 1.0 / 720.0, 1.0 / 24.0, 1.0 / 2.0, 1.0};
+    const double cg[] = {1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0, -1.0, 1.0};
+    for (int i = 0; i < 11; ++i) {
+        double m = pc * r2;
+        pc = m + cg[i] * cc[i];
+    }
+    double cv = pc;
+    long q = ((long)kq) & 3;
+    double s, c;
+    switch (q) {
+        case 0: s = sv; c = cv; break;
+        case 1: s = cv; c = -sv; break;
+        case 2: s = -sv; c = -cv; break;
+        default: s = -cv; c = sv; break;
+    }
+    *s_out = s; *c_out = c;
+}
+
+inline uint32_t spherical_to_oct(float phi, float theta) {
+    double sp, cp, st, ct;
+    sincos_det((double)phi, &sp, &cp);
+    sincos_det((double)theta, &st, &ct);
+    double x = st * cp, y = st * sp;
+    return oct_encode((float)x, (float)y, (float)ct);
+}
+
+inline uint64_t key_of(float d2, uint32_t idx) { return ((uint64_t)f2u(d2) << 32) | idx; }
+
+template <class F>
+void parallel_for_blocks(int64_t n, int64_t block, int nthreads, F&& f) {
+    if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (n <= 0) return;
+    std::atomic<int64_t> next(0);
+    auto worker = [&]() {
+        for (;;) {
+            int64_t b = next.fetch_add(block);
+            if (b >= n) break;
+            f(b, std::min(n, b + block));
+        }
+    };
+    if (nthreads == 1) { worker(); return; }
+    std::vector<std::thread> th;
+    th.reserve(nthreads);
+    for (int t = 0; t < nthreads; ++t) th.emplace_back(worker);
+    for (auto& t : th) t.join();
+}
+
+// Bounded max-heap of (d2, idx) keys, size <= k.
+struct KHeap {
+    uint64_t* a; uint32_t n; uint32_t k;
+    void push(uint64_t v) {
+        if (n < k) {
+            uint32_t i = n++;
+            while (i > 0) { uint32_t p = (i - 1) >> 1; if (a[p] >= v) break; a[i] = a[p]; i = p; }
+            a[i] = v;
+        } else if (v < a[0]) {
+            uint32_t i = 0;
+            for (;;) {
+                uint32_t l = 2 * i + 1; if (l >= n) break;
+                uint32_t c = (l + 1 < n && a[l + 1] > a[l]) ? l + 1 : l;
+                if (a[c] <= v) break;
+                a[i] = a[c]; i = c;
+            }
+            a[i] = v;
+        }
+    }
+    bool full() const { return n == k; }
+    uint64_t top() const { return a[0]; }
+};
+
+inline void finish_query(KHeap& h, float R2, uint32_t k, uint32_t* out_idx, float* out_d2,
+                         uint32_t* out_count, float* out_r2) {
+    std::sort(h.a, h.a + h.n);
+    for (uint32_t j = 0; j < k; ++j) {
+        if (j < h.n) { out_idx[j] = (uint32_t)(h.a[j] & 0xffffffffu); out_d2[j] = u2f((uint32_t)(h.a[j] >> 32)); }
+        else { out_idx[j] = 0xffffffffu; out_d2[j] = INFINITY; }
+    }
+    *out_count = h.n;
+    *out_r2 = (h.n == k) ? u2f((uint32_t)(h.a[k - 1] >> 32)) : R2;
+}
+
+// ------------------------------------------------------ CPU point kd-tree --
+// Median split on the longest axis of the node's point bounds (the
+// reference's large-node rule, GPU/kdtree.cu:629-682, without its
+// empty-space cuts), leaves of <= kLeaf points.
+constexpr int kLeaf = 12;
+
+struct KdNode { float split; int32_t axis; int32_t left, right; int32_t begin, end; };
+
+struct KdTree {
+    std::vector<float> x, y, z;    // points in tree order
+    std::vector<uint32_t> idx;     // original photon index
+    std::vector<KdNode> nodes;
+    uint32_t n = 0;
+};
+
+int kd_build_rec(KdTree& t, std::vector<uint32_t>& ord, const float* pos4, int b, int e) {
+    int me = (int)t.nodes.size();
+    t.nodes.push_back(KdNode{0.f, -1, -1, -1, b, e});
+    if (e - b <= kLeaf) return me;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = b; i < e; ++i)
+        for (int a = 0; a < 3; ++a) { float v = pos4[4 * (size_t)ord[i] + a]; lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a) if (hi[a] - lo[a] > hi[axis] - lo[axis]) axis = a;
+    int mid = b + (e - b) / 2;
+    std::nth_element(ord.begin() + b, ord.begin() + mid, ord.begin() + e, [&](uint32_t u, uint32_t v) {
+        float fu = pos4[4 * (size_t)u + axis], fv = pos4[4 * (size_t)v + axis];
+        return fu < fv || (fu == fv && u < v);
+    });
+    float split = pos4[4 * (size_t)ord[mid] + axis];
+    int l = kd_build_rec(t, ord, pos4, b, mid);
+    int r = kd_build_rec(t, ord, pos4, mid, e);
+    t.nodes[me].split = split; t.nodes[me].axis = axis; t.nodes[me].left = l; t.nodes[me].right = r;
+    return me;
+}
+
+void kd_query(const KdTree& t, float qx, float qy, float qz, float R2, KHeap& h) {
+    struct Ent { int32_t node; float lb; };
+    Ent stack[128];
+    int sp = 0;
+    stack[sp++] = Ent{0, 0.0f};
+    const float q[3] = {qx, qy, qz};
+    while (sp > 0) {
+        Ent e = stack[--sp];
+        if (e.lb >= R2) continue;
+        if (h.full() && e.lb > u2f((uint32_t)(h.top() >> 32))) continue;
+        const KdNode* nd = &t.nodes[e.node];
+        while (nd->axis >= 0) {
+            // plane lower bound: |p_a - q_a| >= |split - q_a| for the far side
+            float diff = nd->split - q[nd->axis];
+            float lbp = diff * diff;
+            int nearc, farc;
+            if (q[nd->axis] < nd->split) { nearc = nd->left; farc = nd->right; }
+            else { nearc = nd->right; farc = nd->left; }
+            float flb = std::max(e.lb, lbp);
+            if (flb < R2 && sp < 128) stack[sp++] = Ent{farc, flb};
+            nd = &t.nodes[nearc];
+        }
+        for (int i = nd->begin; i < nd->end; ++i) {
+            float d2 = d2_f32(qx, qy, qz, t.x[i], t.y[i], t.z[i]);
+            if (d2 < R2) h.push(key_of(d2, t.idx[i]));
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_version(void) { return 3; }
+
+float orc_d2(float qx, float qy, float qz, float px, float py, float pz) { return d2_f32(qx, qy, qz, px, py, pz); }
+uint32_t orc_oct_encode(float x, float y, float z) { return oct_encode(x, y, z); }
+void orc_oct_decode(uint32_t bits, float* out3) { oct_decode(bits, out3); }
+int orc_front(float nx, float ny, float nz, uint32_t dirbits) { return front_f32(nx, ny, nz, dirbits) ? 1 : 0; }
+void orc_sincos(double x, double* sc) { sincos_det(x, &sc[0], &sc[1]); }
+uint32_t orc_spherical_to_oct(float phi, float theta) { return spherical_to_oct(phi, theta); }
+
+// Convert reference-format photons (pos.w = azimuth, pow.w = polar angle) to
+// the engine's packed record (pos.w = photon index bits, pow.w = oct bits).
+void orc_pack_reference_photons(const float* pos4, const float* pow4, uint32_t n, float* out_pos4, float* out_pow4) {
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t dir = spherical_to_oct(pos4[4 * (size_t)i + 3], pow4[4 * (size_t)i + 3]);
+        for (int a = 0; a < 3; ++a) { out_pos4[4 * (size_t)i + a] = pos4[4 * (size_t)i + a]; out_pow4[4 * (size_t)i + a] = pow4[4 * (size_t)i + a]; }
+        out_pos4[4 * (size_t)i + 3] = u2f(i);
+        out_pow4[4 * (size_t)i + 3] = u2f(dir);
+    }
+}
+
+// Exact kNN by brute force (the definition itself).  pos4: photons in caller
+// order (index = position in the array); q4: query positions.
+void orc_knn_brute(const float* pos4, uint32_t n, const float* q4, uint32_t nq, uint32_t k, float R,
+                   uint32_t* out_idx, float* out_d2, uint32_t* out_count, float* out_r2, int nthreads) {
+    const float R2 = R * R;
+    parallel_for_blocks(nq, 64, nthreads, [&](int64_t b, int64_t e) {
+        std::vector<uint64_t> buf(k ? k : 1);
+        for (int64_t q = b; q < e; ++q) {
+            KHeap h{buf.data(), 0, k};
+            float qx = q4[4 * q], qy = q4[4 * q + 1], qz = q4[4 * q + 2];
+            if (k > 0)
+                for (uint32_t i = 0; i < n; ++i) {
+                    float d2 = d2_f32(qx, qy, qz, pos4[4 * (size_t)i], pos4[4 * (size_t)i + 1], pos4[4 * (size_t)i + 2]);
+                    if (d2 < R2) h.push(key_of(d2, i));
+                }
+            finish_query(h, R2, k, out_idx + (size_t)q * k, out_d2 + (size_t)q * k, out_count + q, out_r2 + q);
+        }
+    });
+}
+
+// CPU baseline: median-split point kd-tree + bounded-heap kNN, multithreaded
+// over query blocks.  Same results as orc_knn_brute (tree-independent).
+void* orc_kdtree_build(const float* pos4, uint32_t n) {
+    KdTree* t = new KdTree();
+    t->n = n;
+    std::vector<uint32_t> ord(n);
+    std::iota(ord.begin(), ord.end(), 0u);
+    t->nodes.reserve(2 * (n / kLeaf + 1) + 1);
+    if (n > 0) kd_build_rec(*t, ord, pos4, 0, (int)n);
+    else t->nodes.push_back(KdNode{0.f, -1, -1, -1, 0, 0});
+    t->x.resize(n); t->y.resize(n); t->z.resize(n); t->idx.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        t->x[i] = pos4[4 * (size_t)ord[i]]; t->y[i] = pos4[4 * (size_t)ord[i] + 1]; t->z[i] = pos4[4 * (size_t)ord[i] + 2];
+        t->idx[i] = ord[i];
+    }
+    return t;
+}
+
+void orc_kdtree_free(void* h) { delete (KdTree*)h; }
+
+void orc_knn_kdtree(const void* tree, const float* q4, uint32_t nq, uint32_t k, float R, uint32_t* out_idx,
+                    float* out_d2, uint32_t* out_count, float* out_r2, int nthreads) {
+    const KdTree& t = *(const KdTree*)tree;
+    const float R2 = R * R;
+    parallel_for_blocks(nq, 64, nthreads, [&](int64_t b, int64_t e) {
+        std::vector<uint64_t> buf(k ? k : 1);
+        for (int64_t q = b; q < e; ++q) {
+            KHeap h{buf.data(), 0, k};
+            if (k > 0 && t.n > 0) kd_query(t, q4[4 * q], q4[4 * q + 1], q4[4 * q + 2], R2, h);
+            finish_query(h, R2, k, out_idx + (size_t)q * k, out_d2 + (size_t)q * k, out_count + q, out_r2 + q);
+        }
+    });
+}
+
+// FP64 radiance over a given neighbour set (the FP32 contract decides the
+// set and the front test; weights, sums and the normalisation run in FP64).
+// filter: 0 box, 1 cone, 2 Epanechnikov.  out: 3 doubles per query.
+void orc_radiance_fp64(const float* pos4, const float* pow4, const float* q4, const float* n4, uint32_t nq,
+                       const uint32_t* nbr, const uint32_t* count, uint32_t k, float R, int filter, float cone_k,
+                       uint32_t min_found, double* out, int nthreads) {
+    parallel_for_blocks(nq, 256, nthreads, [&](int64_t b, int64_t e) {
+        for (int64_t q = b; q < e; ++q) {
+            double acc[3] = {0, 0, 0};
+            uint32_t cnt = count[q];
+            const double qx = q4[4 * q], qy = q4[4 * q + 1], qz = q4[4 * q + 2];
+            double r2 = (double)R * (double)R;
+            if (cnt == k && k > 0) {
+                uint32_t pk = nbr[(size_t)q * k + k - 1];
+                double dx = pos4[4 * (size_t)pk] - qx, dy = pos4[4 * (size_t)pk + 1] - qy, dz = pos4[4 * (size_t)pk + 2] - qz;
+                r2 = dx * dx + dy * dy + dz * dz;
+            }
+            if (cnt < min_found || !(r2 > 0.0)) { out[3 * q] = out[3 * q + 1] = out[3 * q + 2] = 0.0; continue; }
+            double r = std::sqrt(r2);
+            for (uint32_t j = 0; j < cnt; ++j) {
+                uint32_t p = nbr[(size_t)q * k + j];
+                if (!front_f32(n4[4 * q], n4[4 * q + 1], n4[4 * q + 2], f2u(pow4[4 * (size_t)p + 3]))) continue;
+                double dx = pos4[4 * (size_t)p] - qx, dy = pos4[4 * (size_t)p + 1] - qy, dz = pos4[4 * (size_t)p + 2] - qz;
+                double d2 = dx * dx + dy * dy + dz * dz;
+                double w = 1.0;
+                if (filter == 1) w = 1.0 - std::sqrt(d2) / ((double)cone_k * r);
+                else if (filter == 2) w = 1.0 - d2 / r2;
+                for (int c = 0; c < 3; ++c) acc[c] += w * (double)pow4[4 * (size_t)p + c];
+            }
+            double norm;
+            if (filter == 1) norm = 1.0 / ((1.0 - 2.0 / (3.0 * (double)cone_k)) * kPi * r2);
+            else if (filter == 2) norm = 2.0 / (kPi * r2);
+            else norm = 1.0 / (kPi * r2);
+            for (int c = 0; c < 3; ++c) out[3 * q + c] = acc[c] * norm;
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Bars (stated per test):
+  * neighbour index sets, their order, counts and r^2: bit-exact;
+  * radiance: max relative error <= 1e-5 against the FP64 oracle on the same
+    neighbour sets, where the FP64 value is above 1e-6 of the map's mean
+    estimate (smaller values are checked with that absolute floor).
+"""
+import numpy as np
+import pytest
+import torch
+
+from mnrt_b200 import gen
+from mnrt_b200 import _lib as L
+from mnrt_b200.photon_map import PhotonMap
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def to_dev(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def run(ph, q, dev, k, r_max, filt="box", cone_k=1.0, min_found=0, brute=False, sorted_queries=True, leaf=16,
+        packed=True, tuning=None):
+    pm = PhotonMap(max(ph.n, 1), global_q_radius_max=r_max)
+    pm.set_tuning(leaf_size=leaf, **(tuning or {}))
+    pm.build(to_dev(ph.pos, dev), to_dev(ph.pow, dev), packed=packed)
+    out = pm.query(to_dev(q.pos, dev), to_dev(q.nrm, dev), want_nbr=True, brute_force=brute, k=k, r_max=r_max,
+                   filter=filt, cone_k=cone_k, min_found=min_found, sorted_queries=sorted_queries)
+    torch.cuda.synchronize()
+    res = {kk: v.cpu().numpy() for kk, v in out.items()}
+    res["info"] = pm.info()
+    res["pm"] = pm
+    return res
+
+
+def check_against_oracle(oracle_mod, ph, q, res, k, r_max, filt, cone_k=1.0, min_found=0, pos_ref=None, pow_ref=None):
+    pos_ref = ph.pos if pos_ref is None else pos_ref
+    pow_ref = ph.pow if pow_ref is None else pow_ref
+    idx, d2, cnt, r2 = oracle_mod.KdTree(pos_ref).knn(q.pos, k, r_max)
+    nbr = res["nbr"].view(np.uint32)
+    assert np.array_equal(res["count"].view(np.uint32), cnt), "neighbour counts differ"
+    bad = np.where((nbr != idx).any(1))[0]
+    assert bad.size == 0, f"{bad.size} queries with different neighbour lists, first {bad[:5]}"
+    assert np.array_equal(res["r2"], r2), "r^2 differs"
+    ref = oracle_mod.radiance_fp64(pos_ref, pow_ref, q.pos, q.nrm, idx, cnt, k, r_max, filt, cone_k, min_found)
+    got = res["rad"][:, :3].astype(np.float64)
+    floor = 1e-6 * max(np.abs(ref).mean(), 1e-30)
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), floor)
+    assert rel.max() <= RTOL, f"max relative radiance error {rel.max():.3e}"
+    assert np.array_equal(res["rad"][:, 3], cnt.astype(np.float32))
+    return rel.max()
+
+
+@pytest.mark.parametrize("filt", ["box", "cone", "epanechnikov"])
+def test_small_config_parity(cuda, oracle_mod, filt):
+    """Small configuration: 65,536 room photons, 16,384 wall queries, k = 50, R = 0.1."""
+    cfg = gen.CONFIGS["small"]
+    ph = gen.photons(cfg["n"], seed=100, caustic_frac=0.0, power_mean=cfg["power_mean"])
+    q = gen.queries(cfg["nq"], seed=101)
+    res = run(ph, q, cuda, cfg["k"], cfg["r_max"], filt)
+    assert res["info"].device_errors == 0
+    err = check_against_oracle(oracle_mod, ph, q, res, cfg["k"], cfg["r_max"], filt)
+    print(f"small config {filt}: max rel err {err:.2e}")
+
+
+def test_tree_matches_bruteforce_and_order_invariance(cuda):
+    ph = gen.photons(40000, seed=7, caustic_frac=0.2)
+    q = gen.queries(5000, seed=8)
+    a = run(ph, q, cuda, 64, 0.05, "cone", cone_k=1.2)
+    b = run(ph, q, cuda, 64, 0.05, "cone", cone_k=1.2, brute=True)
+    c = run(ph, q, cuda, 64, 0.05, "cone", cone_k=1.2, sorted_queries=False)
+    for key in ("nbr", "count", "r2", "rad"):
+        assert np.array_equal(a[key], b[key]), key
+        assert np.array_equal(a[key], c[key]), key
+
+
+@pytest.mark.parametrize("leaf", [1, 4, 16, 32])
+def test_leaf_sizes_and_tuning(cuda, oracle_mod, leaf):
+    ph = gen.photons(20000, seed=9, caustic_frac=0.3, caustic_sigma=0.005)
+    q = gen.queries(3000, seed=10)
+    res = run(ph, q, cuda, 32, 0.08, "epanechnikov", leaf=leaf,
+              tuning=dict(warps_per_block=2, rounds_per_chunk=3))
+    check_against_oracle(oracle_mod, ph, q, res, 32, 0.08, "epanechnikov")
+
+
+@pytest.mark.parametrize("k", [1, 2, 100, 128])
+def test_k_extremes(cuda, oracle_mod, k):
+    ph = gen.photons(30000, seed=11 + k)
+    q = gen.queries(2000, seed=12)
+    res = run(ph, q, cuda, k, 0.07, "box", min_found=8)
+    check_against_oracle(oracle_mod, ph, q, res, k, 0.07, "box", min_found=8)
+
+
+def test_duplicates_and_ties(cuda, oracle_mod):
+    """Coincident photons and equal distances: ties broken by caller index."""
+    ph = gen.photons(5000, seed=13)
+    ph.pos[1000:1300, :3] = ph.pos[5, :3]           # 301 photons at one point
+    ph.pos[2000:2010, :3] = ph.pos[6, :3]
+    q = gen.queries(600, seed=14)
+    q.pos[:50, :3] = ph.pos[5, :3]                   # queries on the pile
+    q.pos[50:60, :3] = ph.pos[6, :3]
+    grid = np.stack(np.meshgrid(np.arange(8), np.arange(8), indexing="ij"), -1).reshape(-1, 2) / 8.0
+    ph.pos[3000:3064, 0] = grid[:, 0]                # lattice: many exactly equal distances
+    ph.pos[3000:3064, 1] = 0.0
+    ph.pos[3000:3064, 2] = grid[:, 1]
+    q.pos[60:70, :3] = [0.0625, 0.0, 0.0625]
+    for k in (16, 128):
+        res = run(ph, q, cuda, k, 0.3, "cone")
+        check_against_oracle(oracle_mod, ph, q, res, k, 0.3, "cone")
+
+
+def test_edge_maps(cuda, oracle_mod):
+    q = gen.queries(300, seed=15)
+    for n in (0, 1, 2, 5, 16, 17, 33):
+        ph = gen.photons(n, seed=16 + n) if n else gen.PhotonSet(np.zeros((0, 4), np.float32),
+                                                                  np.zeros((0, 4), np.float32),
+                                                                  np.zeros((0, 3), np.float32), "packed")
+        res = run(ph, q, cuda, 8, 2.0, "box")
+        if n == 0:
+            assert (res["count"] == 0).all() and (res["rad"] == 0).all()
+            assert (res["nbr"].view(np.uint32) == 0xFFFFFFFF).all()
+        else:
+            check_against_oracle(oracle_mod, ph, q, res, 8, 2.0, "box")
+
+
+def test_far_queries_and_nonfinite(cuda):
+    ph = gen.photons(2000, seed=17)
+    q = gen.queries(100, seed=18)
+    q.pos[:10, :3] += 50.0          # nothing within R
+    q.pos[10, 0] = np.nan           # flagged, zero output
+    res = run(ph, q, cuda, 10, 0.1, "box")
+    assert (res["count"][:11] == 0).all() and (res["rad"][:11] == 0).all()
+    assert res["info"].device_errors & L.PM_DEVERR_QNONFINITE
+
+
+def test_reference_layout_ingest(cuda, oracle_mod):
+    """MNRT's PhotonData layout (azimuth / polar angles in .w) gives the same
+    packed directions on the GPU as the oracle's ingest, bit for bit."""
+    ph = gen.photons(20000, seed=19, layout="reference")
+    q = gen.queries(2000, seed=20)
+    res = run(ph, q, cuda, 40, 0.06, "box", packed=False)
+    op, ow = oracle_mod.pack_reference(ph.pos, ph.pow)
+    _, tpos, tpow = res["pm"].export_tree()
+    order = tpos[:, 3].view(np.uint32)
+    assert np.array_equal(tpow[:, 3].view(np.uint32), ow[order, 3].view(np.uint32))
+    check_against_oracle(oracle_mod, ph, q, res, 40, 0.06, "box", pos_ref=op, pow_ref=ow)
+
+
+def test_tree_structure(cuda):
+    """Every photon in exactly one leaf; leaves <= leaf size; child boxes
+    bound their photons and nest in their parent's box; nodes 64-byte."""
+    ph = gen.photons(50000, seed=21, caustic_frac=0.2)
+    leaf = 16
+    pm = PhotonMap(ph.n, global_q_radius_max=0.1)
+    pm.set_tuning(leaf_size=leaf)
+    pm.build(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda))
+    nodes, tpos, tpow = pm.export_tree()
+    assert np.array_equal(np.sort(tpos[:, 3].view(np.uint32)), np.arange(ph.n, dtype=np.uint32))
+    assert np.array_equal(tpos[:, :3], ph.pos[tpos[:, 3].view(np.uint32), :3])
+    f = nodes.view(np.float32)
+    seen = np.zeros(ph.n, np.int32)
+    stack = [(0, 0, None)]
+    visited = 0
+    while stack:
+        node, side, pbox = stack.pop()
+        base = side * 8
+        lo, hi = f[node, base:base + 3], f[node, base + 3:base + 6]
+        ref, cnt = nodes[node, base + 6], nodes[node, base + 7]
+        if pbox is not None:
+            assert (lo >= pbox[0]).all() and (hi <= pbox[1]).all()
+        if cnt > 0:
+            assert cnt <= leaf
+            seen[ref:ref + cnt] += 1
+            pts = tpos[ref:ref + cnt, :3]
+            assert (pts >= lo).all() and (pts <= hi).all()
+        else:
+            visited += 1
+            stack.append((ref, 0, (lo, hi)))
+            stack.append((ref, 1, (lo, hi)))
+    assert (seen == 1).all()
+    assert visited == nodes.shape[0] - 1
