@@ -113,9 +113,15 @@ PM_API pm_status pm_destroy(pm_map* map);
  * restores cudaMalloc/cudaFree).  Must be set before the first build. */
 PM_API pm_status pm_set_allocator(pm_map* map, pm_alloc_fn alloc, pm_free_fn free_fn, void* user);
 
+/* k-buffer layouts of the query kernel. */
+enum { PM_KBUF_HEAP = 0,   /* one lane per query, max-heap in shared memory */
+       PM_KBUF_GROUP = 1   /* a group of lanes per query, candidate buffer + exact selection */ };
+
 /* Tuning knobs (chosen by the autotuner): photons per leaf (1..32), warps per
- * query block (1..8) and query rounds of 32 per work chunk (1..4096). */
-PM_API pm_status pm_set_tuning(pm_map* map, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk);
+ * query block (1..8), query rounds per work chunk (1..4096), queries per warp
+ * (1, 2, 4, 8; group layout) and the k-buffer layout (PM_KBUF_*). */
+PM_API pm_status pm_set_tuning(pm_map* map, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk,
+                               int queries_per_warp, int kbuf_layout);
 
 /* Reserves storage for up to max_photons photons and max_queries queries so
  * that later builds and queries allocate nothing (needed for stream capture). */

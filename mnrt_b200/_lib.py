@@ -18,6 +18,7 @@ PM_MODE_EXACT, PM_MODE_ZHOU_COMPAT = 0, 1
 PM_ORDER_SORTED, PM_ORDER_AS_GIVEN = 0, 1
 PM_MAX_K = 128
 PM_DEVERR_STACK, PM_DEVERR_NONFINITE, PM_DEVERR_QNONFINITE = 0x1, 0x2, 0x4
+PM_KBUF_HEAP, PM_KBUF_GROUP = 0, 1
 
 FILTERS = {"box": PM_FILTER_BOX, "cone": PM_FILTER_CONE, "epanechnikov": PM_FILTER_EPANECHNIKOV}
 
@@ -50,7 +51,7 @@ SIGNATURES = {
     "pm_create": (_I, [C.POINTER(C.c_void_p), _U32, C.POINTER(C.c_float), C.POINTER(C.c_float), _F]),
     "pm_destroy": (_I, [_VP]),
     "pm_set_allocator": (_I, [_VP, ALLOC_FN, FREE_FN, _VP]),
-    "pm_set_tuning": (_I, [_VP, _U32, _I, _I]),
+    "pm_set_tuning": (_I, [_VP, _U32, _I, _I, _I, _I]),
     "pm_reserve": (_I, [_VP, _U32, _U32]),
     "pm_build": (_I, [_VP, _FP, _FP, _U32, _I, _VP]),
     "pm_query": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),

@@ -27,7 +27,9 @@ struct pm_map {
     float r_max = 0.0f;
     uint32_t leaf_size = 16;
     int warps_per_block = 4;
-    int rounds_per_chunk = 8;
+    int rounds_per_chunk = 32;
+    int queries_per_warp = 4;
+    int kbuf_layout = 1;
     pm_alloc_fn alloc = nullptr;
     pm_free_fn free_fn = nullptr;
     void* alloc_user = nullptr;
@@ -187,6 +189,15 @@ MapView view_of(pm_map* m) {
     return v;
 }
 
+QueryTuning tuning_of(const pm_map* m) {
+    QueryTuning t;
+    t.layout = m->kbuf_layout;
+    t.queries_per_warp = m->queries_per_warp;
+    t.warps_per_block = m->warps_per_block;
+    t.rounds_per_chunk = m->rounds_per_chunk;
+    return t;
+}
+
 QueryParams params_of(const pm_query_desc* d) {
     QueryParams p;
     p.k = d->k;
@@ -267,14 +278,21 @@ pm_status pm_set_allocator(pm_map* m, pm_alloc_fn alloc, pm_free_fn free_fn, voi
     return PM_OK;
 }
 
-pm_status pm_set_tuning(pm_map* m, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk) {
+pm_status pm_set_tuning(pm_map* m, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk,
+                        int queries_per_warp, int kbuf_layout) {
     if (!m) return PM_ERR_INVALID;
     if (leaf_size < 1 || leaf_size > kLeafMax) return fail(m, PM_ERR_INVALID, "leaf_size must be in [1, %u]", kLeafMax);
     if (warps_per_block < 1 || warps_per_block > 8) return fail(m, PM_ERR_INVALID, "warps_per_block must be in [1, 8]");
     if (rounds_per_chunk < 1 || rounds_per_chunk > 4096) return fail(m, PM_ERR_INVALID, "rounds_per_chunk must be in [1, 4096]");
+    if (queries_per_warp != 1 && queries_per_warp != 2 && queries_per_warp != 4 && queries_per_warp != 8)
+        return fail(m, PM_ERR_INVALID, "queries_per_warp must be 1, 2, 4 or 8");
+    if (kbuf_layout != PM_KBUF_HEAP && kbuf_layout != PM_KBUF_GROUP)
+        return fail(m, PM_ERR_INVALID, "unknown k-buffer layout %d", kbuf_layout);
     m->leaf_size = leaf_size;
     m->warps_per_block = warps_per_block;
     m->rounds_per_chunk = rounds_per_chunk;
+    m->queries_per_warp = queries_per_warp;
+    m->kbuf_layout = kbuf_layout;
     return PM_OK;
 }
 
@@ -353,7 +371,7 @@ pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, c
     if (prof) cudaEventRecord(m->ev[4], st);
     QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
     nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
-                    P<uint32_t>(m->counter), m->warps_per_block, m->rounds_per_chunk, st);
+                    P<uint32_t>(m->counter), tuning_of(m), st);
     if (prof) cudaEventRecord(m->ev[5], st);
     m->have_query_ev = prof;
     m->query_launches = (uint32_t)nl;

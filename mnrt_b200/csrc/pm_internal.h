@@ -70,9 +70,15 @@ struct QueryOutputs {
 
 int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint64_t* keys, uint32_t* vals,
                        cudaStream_t st);
+struct QueryTuning {
+    int layout;             // 0: lane per query with a shared-memory heap; 1: group buffers
+    int queries_per_warp;   // group layout: 1, 2, 4 or 8 (32, 16, 8 or 4 lanes per query)
+    int warps_per_block;
+    int rounds_per_chunk;
+};
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
-               const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
-               int warps_per_block, int rounds_per_chunk, cudaStream_t st);
+              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
+              const QueryTuning& t, cudaStream_t st);
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);
 int query_smem_bytes_per_warp(uint32_t k);

@@ -48,6 +48,8 @@ struct KnnArgs {
     uint32_t* out_count;
     uint32_t* work_counter;
     uint32_t rounds_per_chunk;
+    uint32_t cap;             // group kernel: candidate buffer entries per query
+    uint32_t smem_per_warp;   // group kernel: shared bytes per warp
 };
 
 // (d^2, position) keys; equal d^2 is resolved by the caller index stored in
@@ -338,6 +340,386 @@ __global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
     }
 }
 
+// ------------------------------------------------------------------------
+// Group kernel: G lanes per query, 32 / G queries per warp.
+//
+// The warp traverses the tree jointly for its 32 / G queries (a child is
+// visited when any query's box bound passes its threshold).  At a leaf the G
+// lanes of a group split the leaf's photons; accepted candidates are
+// appended to the group's buffer in shared memory with one ballot per step
+// (no per-candidate dependent chains).  When the buffer fills, an exact
+// selection keeps the k smallest (d^2, caller index) keys and tightens the
+// threshold.  Selection = two 8-bit histogram rounds on d^2 quantised
+// linearly to 16 bits, then an exact pass over the few keys sharing the
+// boundary bucket.
+
+template <int G>
+struct GroupCtx {
+    static constexpr int QW = 32 / G;
+    uint32_t s;       // sub-lane 0..G-1
+    uint32_t gbase;   // first lane of the group
+    uint32_t gmask;   // lanes of the group
+};
+
+template <int G>
+__device__ __forceinline__ uint32_t gmax_u32(uint32_t v, uint32_t gmask) {
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) v = max(v, __shfl_xor_sync(gmask, v, o));
+    return v;
+}
+template <int G>
+__device__ __forceinline__ uint32_t gsum_u32(uint32_t v, uint32_t gmask) {
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+template <int G>
+__device__ __forceinline__ long long gsum_i64(long long v, uint32_t gmask) {
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+template <int G>
+__device__ __forceinline__ uint64_t gmin_u64(uint64_t v, uint32_t gmask) {
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+        const uint64_t w = __shfl_xor_sync(gmask, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+// exclusive prefix over the group's lanes
+template <int G>
+__device__ __forceinline__ uint32_t gexscan_u32(uint32_t v, uint32_t s, uint32_t gmask) {
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(gmask, x, o, G);
+        if (s >= (uint32_t)o) x += y;
+    }
+    return x - v;
+}
+
+__device__ __forceinline__ uint32_t q16(uint32_t d2bits, float scale) {
+    const float t = __fmul_rn(__uint_as_float(d2bits), scale);
+    return t >= 65535.0f ? 65535u : (uint32_t)t;
+}
+
+__device__ __forceinline__ uint64_t exact_key(uint64_t e, const float4* __restrict__ pos) {
+    return (e & 0xffffffff00000000ull) | __float_as_uint(pos[(uint32_t)e].w);
+}
+
+// One histogram round: finds the bucket (8-bit digit) holding the kk-th entry
+// among entries whose quantised key has `prefix` in the bits above `shift`
+// (prefix_shift = 16 means every entry).  Returns digit; kk is reduced by the
+// count of entries in lower buckets.
+template <int G>
+__device__ uint32_t hist_round(const uint64_t* buf, uint32_t n, float scale, int shift, uint32_t prefix,
+                               bool use_prefix, uint32_t& kk, uint32_t* hist, uint32_t s, uint32_t gmask) {
+    constexpr int BPL = 256 / G;   // buckets per lane
+#pragma unroll
+    for (int i = 0; i < BPL; ++i) hist[s * BPL + i] = 0;
+    __syncwarp(gmask);
+    for (uint32_t e = s; e < n; e += G) {
+        const uint32_t q = q16((uint32_t)(buf[e] >> 32), scale);
+        if (!use_prefix || (q >> 8) == prefix) atomicAdd(&hist[(q >> shift) & 255u], 1u);
+    }
+    __syncwarp(gmask);
+    uint32_t local = 0;
+#pragma unroll
+    for (int i = 0; i < BPL; ++i) local += hist[s * BPL + i];
+    const uint32_t base = gexscan_u32<G>(local, s, gmask);
+    uint32_t digit = 0, below = 0;
+    const bool mine = base < kk && kk <= base + local;
+    if (mine) {
+        uint32_t run = base;
+        for (int i = 0; i < BPL; ++i) {
+            const uint32_t h = hist[s * BPL + i];
+            if (run + h >= kk) { digit = s * BPL + i; below = run; break; }
+            run += h;
+        }
+    }
+    const uint32_t who = __ffs(__ballot_sync(gmask, mine)) - 1;
+    digit = __shfl_sync(gmask, digit, who);
+    below = __shfl_sync(gmask, below, who);
+    kk -= below;
+    __syncwarp(gmask);
+    return digit;
+}
+
+// Keeps exactly kk entries of buf[0, n): the kk smallest (d^2, caller index).
+// Returns the exact key (d^2 bits << 32 | caller index) of the kk-th.
+template <int G>
+__device__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
+                                 const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt) {
+    uint32_t mx = 0;
+    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+    mx = gmax_u32<G>(mx, gmask);
+    const float dmax = __uint_as_float(mx);
+    const float scale = dmax > 0.0f ? __fdiv_rn(65535.0f, dmax) : 0.0f;
+    uint32_t need = kk;
+    const uint32_t b1 = hist_round<G>(buf, n, scale, 8, 0, false, need, hist, s, gmask);
+    const uint32_t b2 = hist_round<G>(buf, n, scale, 0, b1, true, need, hist, s, gmask);
+    const uint32_t K16 = (b1 << 8) | b2;
+    // exact pass over the boundary bucket: `need` smallest exact keys
+    uint64_t T = 0;
+    bool first = true;
+    for (uint32_t t = 0; t < need; ++t) {
+        uint64_t best = ~0ull;
+        for (uint32_t e = s; e < n; e += G) {
+            const uint64_t v = buf[e];
+            if (q16((uint32_t)(v >> 32), scale) != K16) continue;
+            const uint64_t x = exact_key(v, pos);
+            if ((first || x > T) && x < best) best = x;
+        }
+        T = gmin_u64<G>(best, gmask);
+        first = false;
+    }
+    // compact in place, keeping order of appearance
+    uint32_t out = 0;
+    for (uint32_t base = 0; base < n; base += G) {
+        const uint32_t e = base + s;
+        uint64_t v = 0;
+        bool keep = false;
+        if (e < n) {
+            v = buf[e];
+            const uint32_t q = q16((uint32_t)(v >> 32), scale);
+            keep = q < K16 || (q == K16 && exact_key(v, pos) <= T);
+        }
+        const uint32_t bal = __ballot_sync(gmask, keep);
+        __syncwarp(gmask);
+        if (keep) buf[out + __popc(bal & lt)] = v;
+        out += __popc(bal);
+        __syncwarp(gmask);
+    }
+    n = out;
+    return T;
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
+    constexpr int QW = 32 / G;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = lane_id();
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t g = lane / G, s = lane % G;
+    const uint32_t gbase = g * G;
+    const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t k = a.k, C = a.cap;
+    unsigned char* wb = smem + (size_t)warp * a.smem_per_warp;
+    uint64_t* buf = reinterpret_cast<uint64_t*>(wb) + (size_t)g * C;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(wb + (size_t)QW * C * sizeof(uint64_t)) + g * 256;
+    uint32_t* stack = reinterpret_cast<uint32_t*>(wb + (size_t)QW * (C * sizeof(uint64_t) + 256 * sizeof(uint32_t)));
+    const float r2max = a.r2max;
+    const uint32_t chunk_q = a.rounds_per_chunk * QW;
+    const uint32_t nchunks = (a.nq + chunk_q - 1) / chunk_q;
+
+    for (;;) {
+        uint32_t chunk = 0;
+        if (lane == 0) chunk = atomicAdd(a.work_counter, 1u);
+        chunk = __shfl_sync(kFull, chunk, 0);
+        if (chunk >= nchunks) break;
+        float pqx = 0.f, pqy = 0.f, pqz = 0.f, pr = 0.f;
+        bool pvalid = false;
+        for (uint32_t round = 0; round < a.rounds_per_chunk; ++round) {
+            const uint32_t slot_q = chunk * chunk_q + round * QW + g;
+            const bool inrange = slot_q < a.nq;
+            if (!__any_sync(kFull, inrange)) break;
+            uint32_t qo = 0;
+            float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
+            bool active = false;
+            if (inrange) {
+                qo = a.order ? a.order[slot_q] : slot_q;
+                const float4 q = a.qpos[qo];
+                const float4 nn = a.qnrm[qo];
+                qx = q.x; qy = q.y; qz = q.z; nx = nn.x; ny = nn.y; nz = nn.z;
+                active = isfinite(qx) && isfinite(qy) && isfinite(qz);
+                if (!active && s == 0) atomicOr(&a.hdr->errors, kErrQueryNonFinite);
+            }
+            // radius bound from the previous round's queries of this warp
+            float tau0 = r2max;
+#pragma unroll
+            for (int h = 0; h < QW; ++h) {
+                const int src = h * G;
+                const float sx = __shfl_sync(kFull, pqx, src), sy = __shfl_sync(kFull, pqy, src);
+                const float sz = __shfl_sync(kFull, pqz, src), sr = __shfl_sync(kFull, pr, src);
+                const bool sv = __shfl_sync(kFull, pvalid, src);
+                if (sv) {
+                    const float dq = __fsqrt_rn(d2_rn(qx, qy, qz, sx, sy, sz));
+                    const float b = __fmul_rn(__fadd_rn(sr, dq), 1.000244140625f);
+                    tau0 = fminf(tau0, __fmul_rn(__fmul_rn(b, b), 1.000244140625f));
+                }
+            }
+            uint32_t n = 0;          // entries in this group's buffer
+            bool selected = false;   // a selection has run: threshold is inclusive
+            float thr = tau0;
+            bool todo = active;
+            while (__any_sync(kFull, todo)) {
+                const bool live = todo;
+                if (live) { n = 0; selected = false; thr = tau0; }
+                int sp = 0;
+                float lo[3], hi[3];
+                uint32_t ref, cnt;
+                load_slot(a.nodes, 0, 0, lo, hi, ref, cnt);
+                bool have;
+                {
+                    const float lb = box_lb(qx, qy, qz, lo, hi);
+                    have = __any_sync(kFull, live && lb < thr) && ref != kInvalid;
+                }
+                for (;;) {
+                    if (have) {
+                        if (cnt > 0) {
+                            float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (lane < cnt) mine = __ldg(a.pos + ref + lane);
+                            for (uint32_t j0 = 0; j0 < cnt; j0 += G) {
+                                // make room: a group whose buffer cannot take G more entries selects first
+                                const bool full = live && (n + G > C);
+                                if (__any_sync(kFull, full)) {
+                                    if (full) {
+                                        const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
+                                        selected = true;
+                                        thr = __uint_as_float((uint32_t)(T >> 32));
+                                    }
+                                    __syncwarp();
+                                }
+                                const uint32_t j = j0 + s;
+                                const uint32_t src = j < 32 ? j : 31;
+                                const float px = __shfl_sync(kFull, mine.x, src);
+                                const float py = __shfl_sync(kFull, mine.y, src);
+                                const float pz = __shfl_sync(kFull, mine.z, src);
+                                bool acc = false;
+                                float d2 = 0.f;
+                                if (live && j < cnt) {
+                                    d2 = d2_rn(qx, qy, qz, px, py, pz);
+                                    acc = selected ? (d2 <= thr) : (d2 < thr);
+                                }
+                                const uint32_t bal = __ballot_sync(kFull, acc) & gmask;
+                                if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | (ref + j);
+                                n += __popc(bal);
+                            }
+                            __syncwarp();
+                            have = false;
+                        } else {
+                            float l0[3], h0[3], l1[3], h1[3];
+                            uint32_t r0, c0, r1, c1;
+                            load_slot(a.nodes, ref, 0, l0, h0, r0, c0);
+                            load_slot(a.nodes, ref, 1, l1, h1, r1, c1);
+                            const float lb0 = box_lb(qx, qy, qz, l0, h0);
+                            const float lb1 = box_lb(qx, qy, qz, l1, h1);
+                            const bool p0 = live && (selected ? lb0 <= thr : lb0 < thr);
+                            const bool p1 = live && (selected ? lb1 <= thr : lb1 < thr);
+                            const uint32_t b0 = __ballot_sync(kFull, p0), b1 = __ballot_sync(kFull, p1);
+                            const bool w0 = b0 != 0 && r0 != kInvalid, w1 = b1 != 0 && r1 != kInvalid;
+                            if (w0 && w1) {
+                                const uint32_t votes = __ballot_sync(kFull, (p0 || p1) && lb1 < lb0);
+                                const int near = (2 * __popc(votes) > __popc(b0 | b1)) ? 1 : 0;
+                                if (sp >= kStackDepth) {
+                                    if (lane == 0) atomicOr(&a.hdr->errors, kErrStack);
+                                } else {
+                                    if (lane == 0) stack[sp] = (ref << 1) | (uint32_t)(1 - near);
+                                    ++sp;
+                                }
+                                if (near) { ref = r1; cnt = c1; } else { ref = r0; cnt = c0; }
+                            } else if (w0) {
+                                ref = r0; cnt = c0;
+                            } else if (w1) {
+                                ref = r1; cnt = c1;
+                            } else {
+                                have = false;
+                            }
+                        }
+                        continue;
+                    }
+                    bool found = false;
+                    while (sp > 0) {
+                        --sp;
+                        __syncwarp();
+                        const uint32_t e = stack[sp];
+                        load_slot(a.nodes, e >> 1, e & 1u, lo, hi, ref, cnt);
+                        const float lb = box_lb(qx, qy, qz, lo, hi);
+                        const bool p = live && (selected ? lb <= thr : lb < thr);
+                        if (__any_sync(kFull, p)) { found = true; break; }
+                    }
+                    if (!found) break;
+                    have = true;
+                }
+                // the bound admitted fewer than k photons: redo this query with R
+                todo = live && n < k && tau0 < r2max;
+                if (todo) tau0 = r2max;
+                __syncwarp();
+            }
+            // final selection and epilogue (group-local from here on)
+            float rk2 = r2max;
+            if (active) {
+                if (n > k) {
+                    const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
+                    rk2 = __uint_as_float((uint32_t)(T >> 32));
+                } else if (n == k) {
+                    uint32_t mx = 0;
+                    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+                    rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
+                }
+                const float r2 = (n == k) ? rk2 : r2max;
+                float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
+                if (n >= a.min_found && r2 > 0.0f) {
+                    const float scale = a.hdr->fix_scale;
+                    const float r = __fsqrt_rn(r2);
+                    long long acc0 = 0, acc1 = 0, acc2 = 0;
+                    for (uint32_t e = s; e < n; e += G) {
+                        const uint64_t key = buf[e];
+                        const float4 w = a.pow[(uint32_t)key];
+                        if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
+                        const float d2 = __uint_as_float((uint32_t)(key >> 32));
+                        const float wt = filter_weight(a.filter, d2, r2, r, a.cone_k);
+                        acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
+                        acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
+                        acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
+                    }
+                    acc0 = gsum_i64<G>(acc0, gmask);
+                    acc1 = gsum_i64<G>(acc1, gmask);
+                    acc2 = gsum_i64<G>(acc2, gmask);
+                    if (scale > 0.0f) {
+                        const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
+                        rad.x = __double2float_rn((double)acc0 * f);
+                        rad.y = __double2float_rn((double)acc1 * f);
+                        rad.z = __double2float_rn((double)acc2 * f);
+                    }
+                }
+                if (s == 0) {
+                    a.out_rad[qo] = rad;
+                    if (a.out_r2) a.out_r2[qo] = r2;
+                    if (a.out_count) a.out_count[qo] = n;
+                }
+                if (a.out_nbr) {
+                    // rank sort by exact (d^2, caller index)
+                    for (uint32_t e = s; e < n; e += G) buf[e] = exact_key(buf[e], a.pos);
+                    __syncwarp(gmask);
+                    uint32_t* row = a.out_nbr + (size_t)qo * k;
+                    for (uint32_t e = s; e < n; e += G) {
+                        const uint64_t v = buf[e];
+                        uint32_t rank = 0;
+                        for (uint32_t f = 0; f < n; ++f) rank += buf[f] < v ? 1u : 0u;
+                        row[rank] = (uint32_t)v;
+                    }
+                    for (uint32_t j = n + s; j < k; j += G) row[j] = kInvalid;
+                }
+                rk2 = r2;
+            } else if (inrange && s == 0) {
+                a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (a.out_r2) a.out_r2[qo] = r2max;
+                if (a.out_count) a.out_count[qo] = 0;
+            }
+            if (inrange && !active && a.out_nbr)
+                for (uint32_t j = s; j < k; j += G) a.out_nbr[(size_t)qo * k + j] = kInvalid;
+            __syncwarp();
+            pqx = qx; pqy = qy; pqz = qz;
+            pvalid = active && n == k;
+            pr = pvalid ? __fsqrt_rn(rk2) : 0.0f;
+        }
+    }
+}
+
 // Brute force: thread per query, every photon staged through shared memory.
 constexpr int kBruteThreads = 64;
 constexpr int kBruteTile = 512;
@@ -433,30 +815,63 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.k = p.k; a.r2max = p.r2; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
     a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
     a.work_counter = nullptr; a.rounds_per_chunk = 1;
+    a.cap = 0; a.smem_per_warp = 0;
     return a;
+}
+
+uint32_t group_capacity(uint32_t k) { return ((k + 31u) & ~31u) + 64u; }
+
+int group_smem_bytes_per_warp(uint32_t k, int qpw) {
+    return qpw * (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) +
+           kStackDepth * (int)sizeof(uint32_t);
+}
+
+template <class K>
+static uint32_t grid_for(K kernel, int threads, int smem, uint32_t work_items, int warps_per_block) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (per_sm < 1) per_sm = 1;
+    uint32_t grid = (uint32_t)(sms * per_sm);
+    const uint32_t need = (work_items + warps_per_block - 1) / warps_per_block;
+    return grid > need ? need : (grid ? grid : 1);
 }
 
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
               const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
-              int warps_per_block, int rounds_per_chunk, cudaStream_t st) {
+              const QueryTuning& t, cudaStream_t st) {
     if (!nq) return 0;
     KnnArgs a = make_args(m, p, qpos, qnrm, order, nq, out);
     a.work_counter = work_counter;
-    a.rounds_per_chunk = (uint32_t)rounds_per_chunk;
-    const int smem = query_smem_bytes_per_warp(p.k) * warps_per_block;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_knn_tree, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_tree, 32 * warps_per_block, smem);
-    if (per_sm < 1) per_sm = 1;
-    const uint32_t chunk_q = (uint32_t)rounds_per_chunk * 32;
-    const uint32_t nchunks = (nq + chunk_q - 1) / chunk_q;
-    uint32_t grid = (uint32_t)(sms * per_sm);
-    const uint32_t need = (nchunks + warps_per_block - 1) / warps_per_block;
-    if (grid > need) grid = need;
+    a.rounds_per_chunk = (uint32_t)t.rounds_per_chunk;
+    const int threads = 32 * t.warps_per_block;
     cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st);
-    k_knn_tree<<<grid, 32 * warps_per_block, smem, st>>>(a);
+    if (t.layout == 0) {   // one lane per query, shared-memory heap
+        const int smem = query_smem_bytes_per_warp(p.k) * t.warps_per_block;
+        const uint32_t nchunks = (nq + 32u * a.rounds_per_chunk - 1) / (32u * a.rounds_per_chunk);
+        const uint32_t grid = grid_for(k_knn_tree, threads, smem, nchunks, t.warps_per_block);
+        k_knn_tree<<<grid, threads, smem, st>>>(a);
+        return 1;
+    }
+    const int qpw = t.queries_per_warp;
+    a.cap = group_capacity(p.k);
+    a.smem_per_warp = (uint32_t)group_smem_bytes_per_warp(p.k, qpw);
+    const int smem = (int)a.smem_per_warp * t.warps_per_block;
+    const uint32_t nchunks = (nq + (uint32_t)qpw * a.rounds_per_chunk - 1) / ((uint32_t)qpw * a.rounds_per_chunk);
+#define PM_LAUNCH_GROUP(G)                                                                 \
+    {                                                                                      \
+        const uint32_t grid = grid_for(k_knn_group<G>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G><<<grid, threads, smem, st>>>(a);                                    \
+    }
+    switch (qpw) {
+        case 1: PM_LAUNCH_GROUP(32) break;
+        case 2: PM_LAUNCH_GROUP(16) break;
+        case 4: PM_LAUNCH_GROUP(8) break;
+        default: PM_LAUNCH_GROUP(4) break;
+    }
+#undef PM_LAUNCH_GROUP
     return 1;
 }
 

@@ -106,8 +106,10 @@ class PhotonMap:
     def get_photon_count(self) -> int:
         return self.num_photons
 
-    def set_tuning(self, leaf_size: int = 16, warps_per_block: int = 4, rounds_per_chunk: int = 8) -> None:
-        L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk), self._h)
+    def set_tuning(self, leaf_size: int = 16, warps_per_block: int = 4, rounds_per_chunk: int = 32,
+                   queries_per_warp: int = 4, kbuf_layout: int = L.PM_KBUF_GROUP) -> None:
+        L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk, queries_per_warp,
+                                        kbuf_layout), self._h)
 
     def reserve(self, max_photons: int, max_queries: int) -> None:
         L.check(self._lib.pm_reserve(self._h, int(max_photons), int(max_queries)), self._h)

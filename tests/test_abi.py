@@ -68,10 +68,12 @@ def test_build_validation_without_gpu(engine_lib):
     assert lib.pm_build(h, 16, 32, 10, 5, None) == L.PM_ERR_INVALID
     assert lib.pm_build(h, 17, 32, 10, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID   # misaligned
     assert lib.pm_build(h, 16, 32, 5000, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID  # > max_photons
-    assert lib.pm_set_tuning(h, 0, 4, 8) == L.PM_ERR_INVALID
-    assert lib.pm_set_tuning(h, 33, 4, 8) == L.PM_ERR_INVALID
-    assert lib.pm_set_tuning(h, 16, 9, 8) == L.PM_ERR_INVALID
-    assert lib.pm_set_tuning(h, 16, 4, 8) == L.PM_OK
+    assert lib.pm_set_tuning(h, 0, 4, 8, 4, 1) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 33, 4, 8, 4, 1) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 16, 9, 8, 4, 1) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 16, 4, 8, 3, 1) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 16, 4, 8, 4, 2) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 16, 4, 8, 4, 1) == L.PM_OK
     assert lib.pm_scale_flux(h, 2.0, None) == L.PM_ERR_STATE
     lib.pm_destroy(h)
 

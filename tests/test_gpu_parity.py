@@ -67,6 +67,26 @@ def test_small_config_parity(cuda, oracle_mod, filt):
     print(f"small config {filt}: max rel err {err:.2e}")
 
 
+KERNELS = [dict(kbuf_layout=0), dict(kbuf_layout=1, queries_per_warp=1), dict(kbuf_layout=1, queries_per_warp=2),
+           dict(kbuf_layout=1, queries_per_warp=4), dict(kbuf_layout=1, queries_per_warp=8)]
+
+
+@pytest.mark.parametrize("kern", KERNELS, ids=["heap", "g32", "g16", "g8", "g4"])
+@pytest.mark.parametrize("k,filt", [(100, "cone"), (16, "box"), (128, "epanechnikov")])
+def test_kernel_variants_bitwise_equal(cuda, oracle_mod, kern, k, filt):
+    """Every k-buffer layout / queries-per-warp variant gives the same bits."""
+    ph = gen.photons(60000, seed=31, caustic_frac=0.2)
+    ph.pos[100:160, :3] = ph.pos[7, :3]               # a pile of coincident photons
+    q = gen.queries(6000, seed=32)
+    q.pos[:20, :3] = ph.pos[7, :3]
+    ref = run(ph, q, cuda, k, 0.05, filt, brute=True)
+    res = run(ph, q, cuda, k, 0.05, filt, tuning=dict(rounds_per_chunk=5, **kern))
+    for key in ("nbr", "count", "r2", "rad"):
+        assert np.array_equal(res[key], ref[key]), key
+    assert res["info"].device_errors == 0
+    check_against_oracle(oracle_mod, ph, q, res, k, 0.05, filt)
+
+
 def test_tree_matches_bruteforce_and_order_invariance(cuda):
     ph = gen.photons(40000, seed=7, caustic_frac=0.2)
     q = gen.queries(5000, seed=8)
