@@ -213,8 +213,9 @@ def run_ours(args, cfg) -> dict | None:
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
 
     pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
-    if args.leaf or args.wpb or args.rounds:
-        pm.set_tuning(leaf_size=args.leaf or 16, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 8)
+    if args.leaf or args.wpb or args.rounds or args.qpw or args.layout >= 0:
+        pm.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 32,
+                      queries_per_warp=args.qpw or 1, kbuf_layout=args.layout if args.layout >= 0 else 1)
     pm.reserve(N, Q)
     pm.set_profiling(True)
     out = {"rad": d_rad}
@@ -341,6 +342,8 @@ def main(argv=None) -> int:
     ap.add_argument("--leaf", type=int, default=0)
     ap.add_argument("--wpb", type=int, default=0)
     ap.add_argument("--rounds", type=int, default=0)
+    ap.add_argument("--qpw", type=int, default=0, help="queries per warp (group layout)")
+    ap.add_argument("--layout", type=int, default=-1, help="k-buffer layout: 0 heap, 1 group")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -200,6 +200,13 @@ typedef struct pm_timings {
 PM_API pm_status pm_set_profiling(pm_map* map, int enable);
 PM_API pm_status pm_last_timings(pm_map* map, pm_timings* out);
 
+/* Traversal counters of the last pm_query with the group layout, collected
+ * when profiling is enabled with level 2 (costs some speed).  Synchronous.
+ * out[0..7]: queries, internal nodes visited (per warp), leaves visited (per
+ * warp), photons tested (per warp), candidates appended, selections, radius
+ * redos, queries started without a radius bound. */
+PM_API pm_status pm_query_stats(pm_map* map, uint64_t* out, uint32_t count);
+
 /* Blocks until the stream is idle, then fills info (including device error bits). */
 PM_API pm_status pm_get_info(pm_map* map, pm_map_info* info, void* stream);
 PM_API pm_status pm_clear_errors(pm_map* map, void* stream);

@@ -63,6 +63,7 @@ SIGNATURES = {
     "pm_get_info": (_I, [_VP, C.POINTER(MapInfo), _VP]),
     "pm_set_profiling": (_I, [_VP, _I]),
     "pm_last_timings": (_I, [_VP, C.POINTER(Timings)]),
+    "pm_query_stats": (_I, [_VP, _VP, _U32]),
     "pm_clear_errors": (_I, [_VP, _VP]),
     "pm_export_tree": (_I, [_VP, _VP, _U32, _VP, _VP, _U32]),
     "pm_last_error": (C.c_char_p, [_VP]),

@@ -25,10 +25,12 @@ struct pm_map {
     uint32_t max_photons = 0;
     float scene_min[3] = {0, 0, 0}, scene_max[3] = {0, 0, 0};
     float r_max = 0.0f;
-    uint32_t leaf_size = 16;
+    // defaults: the fastest setting measured on the 1M-photon / 2M-query
+    // workload (k = 100); pm_set_tuning / the autotuner override them
+    uint32_t leaf_size = 32;
     int warps_per_block = 4;
     int rounds_per_chunk = 32;
-    int queries_per_warp = 4;
+    int queries_per_warp = 1;
     int kbuf_layout = 1;
     pm_alloc_fn alloc = nullptr;
     pm_free_fn free_fn = nullptr;
@@ -43,8 +45,10 @@ struct pm_map {
     DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
     // query-sized
     DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter;
+    DevBuf stats;           // query counters (profiling level 2)
     // profiling: events recorded on the call's stream when enabled
     bool profiling = false;
+    int profile_level = 0;
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // b0 b1 b2 q0 q1 q2
     bool have_build_ev = false, have_query_ev = false;
     uint32_t build_launches = 0, query_launches = 0;
@@ -195,6 +199,7 @@ QueryTuning tuning_of(const pm_map* m) {
     t.queries_per_warp = m->queries_per_warp;
     t.warps_per_block = m->warps_per_block;
     t.rounds_per_chunk = m->rounds_per_chunk;
+    t.stats = (m->profile_level >= 2 && m->stats.ptr) ? P<unsigned long long>(m->stats) : nullptr;
     return t;
 }
 
@@ -259,7 +264,7 @@ pm_status pm_destroy(pm_map* m) {
     DevBuf* all[] = {&m->pos, &m->pow, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
-                     &m->qscratch, &m->counter};
+                     &m->qscratch, &m->counter, &m->stats};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -449,7 +454,22 @@ pm_status pm_set_profiling(pm_map* m, int enable) {
         for (cudaEvent_t& e : m->ev)
             if (!e && cudaEventCreate(&e) != cudaSuccess) return check_cuda(m, "pm_set_profiling");
     }
+    if (enable >= 2) {
+        pm_status s = buf_ensure(m, m->stats, 16 * sizeof(unsigned long long), "stats");
+        if (s != PM_OK) return s;
+    }
     m->profiling = enable != 0;
+    m->profile_level = enable;
+    return PM_OK;
+}
+
+pm_status pm_query_stats(pm_map* m, uint64_t* out, uint32_t count) {
+    if (!m || !out) return fail(m, PM_ERR_INVALID, "stats output is NULL");
+    if (!m->stats.ptr || m->profile_level < 2) return fail(m, PM_ERR_STATE, "enable profiling level 2 first");
+    const uint32_t c = count < 8 ? count : 8;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(out, m->stats.ptr, c * sizeof(uint64_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return check_cuda(m, "pm_query_stats");
     return PM_OK;
 }
 

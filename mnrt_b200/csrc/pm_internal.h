@@ -75,6 +75,7 @@ struct QueryTuning {
     int queries_per_warp;   // group layout: 1, 2, 4 or 8 (32, 16, 8 or 4 lanes per query)
     int warps_per_block;
     int rounds_per_chunk;
+    unsigned long long* stats;   // 8 traversal counters (group layout), nullptr = off
 };
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
               const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,

@@ -50,7 +50,12 @@ struct KnnArgs {
     uint32_t rounds_per_chunk;
     uint32_t cap;             // group kernel: candidate buffer entries per query
     uint32_t smem_per_warp;   // group kernel: shared bytes per warp
+    unsigned long long* stats;   // optional traversal counters (kStat*), nullptr = off
 };
+
+// Counters of the group kernel, accumulated when KnnArgs::stats is set.
+enum { kStatQueries = 0, kStatNodes, kStatLeaves, kStatPhotons, kStatCandidates, kStatSelections, kStatRedo,
+       kStatUnbounded, kStatCount };
 
 // (d^2, position) keys; equal d^2 is resolved by the caller index stored in
 // pos[].w, which keeps the order identical to (d^2, caller index).
@@ -92,9 +97,21 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t n, uint64_t
     h[i * 32] = v;
 }
 
-__device__ __forceinline__ float filter_weight(int filter, float d2, float r2, float r, float cone_k) {
-    if (filter == 1) return __fsub_rn(1.0f, __fdiv_rn(__fsqrt_rn(d2), __fmul_rn(cone_k, r)));
-    if (filter == 2) return __fsub_rn(1.0f, __fdiv_rn(d2, r2));
+// Per-query factor of the filter weight: 1 / (k_c r) for the cone, 1 / r^2
+// for Epanechnikov (the weights only enter the FP64-checked estimate, they
+// are not part of the exact neighbour contract).
+__device__ __forceinline__ float filter_factor(int filter, float r2, float cone_k) {
+    if (filter == 1) return __frcp_rn(__fmul_rn(cone_k, __fsqrt_rn(r2)));
+    if (filter == 2) return __frcp_rn(r2);
+    return 0.0f;
+}
+
+__device__ __forceinline__ float filter_weight(int filter, float d2, float inv) {
+    if (filter == 1) {
+        const float d = d2 > 0.0f ? __fmul_rn(d2, rsqrtf(d2)) : 0.0f;
+        return fmaxf(__fsub_rn(1.0f, __fmul_rn(d, inv)), 0.0f);
+    }
+    if (filter == 2) return fmaxf(__fsub_rn(1.0f, __fmul_rn(d2, inv)), 0.0f);
     return 1.0f;
 }
 
@@ -142,14 +159,14 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
     float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)hn);
     if (hn >= a.min_found && r2 > 0.0f) {
         const float scale = a.hdr->fix_scale;
-        const float r = __fsqrt_rn(r2);
+        const float inv = filter_factor(a.filter, r2, a.cone_k);
         long long acc0 = 0, acc1 = 0, acc2 = 0;
         for (uint32_t j = 0; j < hn; ++j) {
             const uint64_t key = h[j * stride];
             const float4 w = a.pow[(uint32_t)key];
             if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
             const float d2 = __uint_as_float((uint32_t)(key >> 32));
-            const float wt = filter_weight(a.filter, d2, r2, r, a.cone_k);
+            const float wt = filter_weight(a.filter, d2, inv);
             acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
             acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
             acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
@@ -400,6 +417,11 @@ __device__ __forceinline__ uint32_t gexscan_u32(uint32_t v, uint32_t s, uint32_t
     return x - v;
 }
 
+// A query started without a radius bound when its first search used R.
+__device__ __forceinline__ bool pvalid_any_bound(float tau0, float r2max, uint32_t redo) {
+    return redo == 0 && tau0 < r2max;
+}
+
 __device__ __forceinline__ uint32_t q16(uint32_t d2bits, float scale) {
     const float t = __fmul_rn(__uint_as_float(d2bits), scale);
     return t >= 65535.0f ? 65535u : (uint32_t)t;
@@ -496,6 +518,70 @@ __device__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32
     return T;
 }
 
+// Final selection and outputs for one query held by a group of G lanes:
+// keeps the k nearest, writes radiance / r^2 / count / sorted neighbours and
+// returns the r^2 used by the filter.
+template <int G>
+__device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, uint32_t s,
+                              uint32_t gmask, uint32_t lt, uint32_t qo, float nx, float ny, float nz) {
+    const uint32_t k = a.k;
+    float rk2 = a.r2max;
+    if (n > k) {
+        const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
+        rk2 = __uint_as_float((uint32_t)(T >> 32));
+    } else if (n == k) {
+        uint32_t mx = 0;
+        for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+        rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
+    }
+    const float r2 = (n == k) ? rk2 : a.r2max;
+    float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
+    if (n >= a.min_found && r2 > 0.0f) {
+        const float scale = a.hdr->fix_scale;
+        const float inv = filter_factor(a.filter, r2, a.cone_k);
+        long long acc0 = 0, acc1 = 0, acc2 = 0;
+        for (uint32_t e = s; e < n; e += G) {
+            const uint64_t key = buf[e];
+            const float4 w = a.pow[(uint32_t)key];
+            if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
+            const float d2 = __uint_as_float((uint32_t)(key >> 32));
+            const float wt = filter_weight(a.filter, d2, inv);
+            acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
+            acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
+            acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
+        }
+        acc0 = gsum_i64<G>(acc0, gmask);
+        acc1 = gsum_i64<G>(acc1, gmask);
+        acc2 = gsum_i64<G>(acc2, gmask);
+        if (scale > 0.0f) {
+            const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
+            rad.x = __double2float_rn((double)acc0 * f);
+            rad.y = __double2float_rn((double)acc1 * f);
+            rad.z = __double2float_rn((double)acc2 * f);
+        }
+    }
+    if (s == 0) {
+        a.out_rad[qo] = rad;
+        if (a.out_r2) a.out_r2[qo] = r2;
+        if (a.out_count) a.out_count[qo] = n;
+    }
+    if (a.out_nbr) {
+        // rank sort by exact (d^2, caller index)
+        for (uint32_t e = s; e < n; e += G) buf[e] = exact_key(buf[e], a.pos);
+        __syncwarp(gmask);
+        uint32_t* row = a.out_nbr + (size_t)qo * k;
+        for (uint32_t e = s; e < n; e += G) {
+            const uint64_t v = buf[e];
+            uint32_t rank = 0;
+            for (uint32_t f = 0; f < n; ++f) rank += buf[f] < v ? 1u : 0u;
+            row[rank] = (uint32_t)v;
+        }
+        for (uint32_t j = n + s; j < k; j += G) row[j] = kInvalid;
+        __syncwarp(gmask);
+    }
+    return r2;
+}
+
 template <int G>
 __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
     constexpr int QW = 32 / G;
@@ -555,6 +641,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
             bool selected = false;   // a selection has run: threshold is inclusive
             float thr = tau0;
             bool todo = active;
+            uint32_t st_nodes = 0, st_leaves = 0, st_photons = 0, st_cand = 0, st_sel = 0, st_redo = 0;
             while (__any_sync(kFull, todo)) {
                 const bool live = todo;
                 if (live) { n = 0; selected = false; thr = tau0; }
@@ -570,6 +657,8 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 for (;;) {
                     if (have) {
                         if (cnt > 0) {
+                            ++st_leaves;
+                            st_photons += cnt;
                             float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
                             if (lane < cnt) mine = __ldg(a.pos + ref + lane);
                             for (uint32_t j0 = 0; j0 < cnt; j0 += G) {
@@ -578,6 +667,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                                 if (__any_sync(kFull, full)) {
                                     if (full) {
                                         const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
+                                        ++st_sel;
                                         selected = true;
                                         thr = __uint_as_float((uint32_t)(T >> 32));
                                     }
@@ -597,10 +687,12 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                                 const uint32_t bal = __ballot_sync(kFull, acc) & gmask;
                                 if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | (ref + j);
                                 n += __popc(bal);
+                                st_cand += __popc(bal);
                             }
                             __syncwarp();
                             have = false;
                         } else {
+                            ++st_nodes;
                             float l0[3], h0[3], l1[3], h1[3];
                             uint32_t r0, c0, r1, c1;
                             load_slot(a.nodes, ref, 0, l0, h0, r0, c0);
@@ -646,64 +738,25 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 }
                 // the bound admitted fewer than k photons: redo this query with R
                 todo = live && n < k && tau0 < r2max;
-                if (todo) tau0 = r2max;
+                if (todo) { tau0 = r2max; ++st_redo; }
                 __syncwarp();
             }
             // final selection and epilogue (group-local from here on)
             float rk2 = r2max;
+            if (a.stats && s == 0 && active) {
+                atomicAdd(a.stats + kStatQueries, 1ull);
+                atomicAdd(a.stats + kStatCandidates, (unsigned long long)st_cand);
+                atomicAdd(a.stats + kStatSelections, (unsigned long long)(st_sel + (n > k ? 1 : 0)));
+                atomicAdd(a.stats + kStatRedo, (unsigned long long)st_redo);
+                if (!pvalid_any_bound(tau0, r2max, st_redo)) atomicAdd(a.stats + kStatUnbounded, 1ull);
+            }
+            if (a.stats && lane == 0) {
+                atomicAdd(a.stats + kStatNodes, (unsigned long long)st_nodes);
+                atomicAdd(a.stats + kStatLeaves, (unsigned long long)st_leaves);
+                atomicAdd(a.stats + kStatPhotons, (unsigned long long)st_photons);
+            }
             if (active) {
-                if (n > k) {
-                    const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
-                    rk2 = __uint_as_float((uint32_t)(T >> 32));
-                } else if (n == k) {
-                    uint32_t mx = 0;
-                    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
-                    rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
-                }
-                const float r2 = (n == k) ? rk2 : r2max;
-                float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
-                if (n >= a.min_found && r2 > 0.0f) {
-                    const float scale = a.hdr->fix_scale;
-                    const float r = __fsqrt_rn(r2);
-                    long long acc0 = 0, acc1 = 0, acc2 = 0;
-                    for (uint32_t e = s; e < n; e += G) {
-                        const uint64_t key = buf[e];
-                        const float4 w = a.pow[(uint32_t)key];
-                        if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
-                        const float d2 = __uint_as_float((uint32_t)(key >> 32));
-                        const float wt = filter_weight(a.filter, d2, r2, r, a.cone_k);
-                        acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
-                        acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
-                        acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
-                    }
-                    acc0 = gsum_i64<G>(acc0, gmask);
-                    acc1 = gsum_i64<G>(acc1, gmask);
-                    acc2 = gsum_i64<G>(acc2, gmask);
-                    if (scale > 0.0f) {
-                        const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
-                        rad.x = __double2float_rn((double)acc0 * f);
-                        rad.y = __double2float_rn((double)acc1 * f);
-                        rad.z = __double2float_rn((double)acc2 * f);
-                    }
-                }
-                if (s == 0) {
-                    a.out_rad[qo] = rad;
-                    if (a.out_r2) a.out_r2[qo] = r2;
-                    if (a.out_count) a.out_count[qo] = n;
-                }
-                if (a.out_nbr) {
-                    // rank sort by exact (d^2, caller index)
-                    for (uint32_t e = s; e < n; e += G) buf[e] = exact_key(buf[e], a.pos);
-                    __syncwarp(gmask);
-                    uint32_t* row = a.out_nbr + (size_t)qo * k;
-                    for (uint32_t e = s; e < n; e += G) {
-                        const uint64_t v = buf[e];
-                        uint32_t rank = 0;
-                        for (uint32_t f = 0; f < n; ++f) rank += buf[f] < v ? 1u : 0u;
-                        row[rank] = (uint32_t)v;
-                    }
-                    for (uint32_t j = n + s; j < k; j += G) row[j] = kInvalid;
-                }
+                const float r2 = group_finish<G>(a, buf, n, hist, s, gmask, lt, qo, nx, ny, nz);
                 rk2 = r2;
             } else if (inrange && s == 0) {
                 a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -815,7 +868,7 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.k = p.k; a.r2max = p.r2; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
     a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
     a.work_counter = nullptr; a.rounds_per_chunk = 1;
-    a.cap = 0; a.smem_per_warp = 0;
+    a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
     return a;
 }
 
@@ -845,6 +898,8 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
     if (!nq) return 0;
     KnnArgs a = make_args(m, p, qpos, qnrm, order, nq, out);
     a.work_counter = work_counter;
+    a.stats = t.stats;
+    if (t.stats) cudaMemsetAsync(t.stats, 0, kStatCount * sizeof(unsigned long long), st);
     a.rounds_per_chunk = (uint32_t)t.rounds_per_chunk;
     const int threads = 32 * t.warps_per_block;
     cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st);

@@ -106,8 +106,8 @@ class PhotonMap:
     def get_photon_count(self) -> int:
         return self.num_photons
 
-    def set_tuning(self, leaf_size: int = 16, warps_per_block: int = 4, rounds_per_chunk: int = 32,
-                   queries_per_warp: int = 4, kbuf_layout: int = L.PM_KBUF_GROUP) -> None:
+    def set_tuning(self, leaf_size: int = 32, warps_per_block: int = 4, rounds_per_chunk: int = 32,
+                   queries_per_warp: int = 1, kbuf_layout: int = L.PM_KBUF_GROUP) -> None:
         L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk, queries_per_warp,
                                         kbuf_layout), self._h)
 
@@ -156,8 +156,19 @@ class PhotonMap:
         L.check(self._lib.pm_get_info(self._h, C.byref(i), _stream(stream)), self._h)
         return i
 
-    def set_profiling(self, enable: bool = True) -> None:
+    def set_profiling(self, enable: int = 1) -> None:
+        """1: phase timings with CUDA events; 2: also traversal counters."""
         L.check(self._lib.pm_set_profiling(self._h, int(enable)), self._h)
+
+    STAT_NAMES = ("queries", "nodes_per_warp", "leaves_per_warp", "photons_per_warp", "candidates", "selections",
+                  "redos", "unbounded")
+
+    def query_stats(self) -> dict:
+        """Traversal counters of the last query (needs set_profiling(2))."""
+        import numpy as np
+        out = np.zeros(8, np.uint64)
+        L.check(self._lib.pm_query_stats(self._h, out.ctypes.data, 8), self._h)
+        return dict(zip(self.STAT_NAMES, (int(x) for x in out)))
 
     def last_timings(self) -> L.Timings:
         t = L.Timings()

@@ -68,10 +68,11 @@ def test_small_config_parity(cuda, oracle_mod, filt):
 
 
 KERNELS = [dict(kbuf_layout=0), dict(kbuf_layout=1, queries_per_warp=1), dict(kbuf_layout=1, queries_per_warp=2),
-           dict(kbuf_layout=1, queries_per_warp=4), dict(kbuf_layout=1, queries_per_warp=8)]
+           dict(kbuf_layout=1, queries_per_warp=4), dict(kbuf_layout=1, queries_per_warp=8),
+           dict(kbuf_layout=1, queries_per_warp=1, rounds_per_chunk=1)]
 
 
-@pytest.mark.parametrize("kern", KERNELS, ids=["heap", "g32", "g16", "g8", "g4"])
+@pytest.mark.parametrize("kern", KERNELS, ids=["heap", "g32", "g16", "g8", "g4", "g32r1"])
 @pytest.mark.parametrize("k,filt", [(100, "cone"), (16, "box"), (128, "epanechnikov")])
 def test_kernel_variants_bitwise_equal(cuda, oracle_mod, kern, k, filt):
     """Every k-buffer layout / queries-per-warp variant gives the same bits."""
@@ -80,7 +81,7 @@ def test_kernel_variants_bitwise_equal(cuda, oracle_mod, kern, k, filt):
     q = gen.queries(6000, seed=32)
     q.pos[:20, :3] = ph.pos[7, :3]
     ref = run(ph, q, cuda, k, 0.05, filt, brute=True)
-    res = run(ph, q, cuda, k, 0.05, filt, tuning=dict(rounds_per_chunk=5, **kern))
+    res = run(ph, q, cuda, k, 0.05, filt, tuning={"rounds_per_chunk": 5, **kern})
     for key in ("nbr", "count", "r2", "rad"):
         assert np.array_equal(res[key], ref[key]), key
     assert res["info"].device_errors == 0
