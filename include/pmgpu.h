@@ -152,6 +152,35 @@ PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, con
                               const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,
                               uint32_t* d_count, void* stream);
 
+/* Largest query count pm_query_noalloc accepts. */
+#define PM_NOALLOC_MAX_QUERIES 262144u
+
+/* pm_query without any device allocation.  No counterpart in the reference
+ * (which allocates from its memory pool inside every gather).
+ *
+ * For callers that cannot allocate device memory when they query: a render
+ * loop that must not stall (cudaMalloc and cudaFree synchronise the device),
+ * or a host application that gives the engine a fixed memory budget and lets
+ * nothing grow after start-up.  Same arguments and the same results, bit for
+ * bit, as pm_query on a built map.
+ *   - The map must already be built.  The caller passes every input and
+ *     output buffer, as for pm_query.
+ *   - The query scratch (Morton sort keys and the work counter) lives in one
+ *     fixed array of about 6.2 MiB inside this library.  Every GPU that loads
+ *     the library holds it until the process exits.
+ *   - nq > PM_NOALLOC_MAX_QUERIES is rejected with PM_ERR_INVALID; split
+ *     larger query sets into several calls.
+ *   - The first call on each device looks up the array's device address,
+ *     with that device current.  Make that first call before any stream
+ *     capture.
+ *   - Every call, on every handle and stream, shares the one array.  Calls
+ *     that overlap on the GPU (two streams, two threads) race and give wrong
+ *     results.  Serialise them, e.g. on one stream.
+ *   - PM_MODE_ZHOU_COMPAT is not supported here (PM_ERR_UNSUPPORTED). */
+PM_API pm_status pm_query_noalloc(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
+                                  const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,
+                                  uint32_t* d_count, void* stream);
+
 /* Reverse-mode adjoint of pm_query (exact mode).  Given dL/dE per query
  * (d_grad_rad4, rgb), writes dL/dpower (d_grad_pow4, rgb, w = 0) and
  * dL/dposition (d_grad_pos4, xyz, w = 0) for every photon in caller order.

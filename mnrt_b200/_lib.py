@@ -17,6 +17,7 @@ PM_FILTER_BOX, PM_FILTER_CONE, PM_FILTER_EPANECHNIKOV = 0, 1, 2
 PM_MODE_EXACT, PM_MODE_ZHOU_COMPAT = 0, 1
 PM_ORDER_SORTED, PM_ORDER_AS_GIVEN = 0, 1
 PM_MAX_K = 128
+PM_NOALLOC_MAX_QUERIES = 262144
 PM_DEVERR_STACK, PM_DEVERR_NONFINITE, PM_DEVERR_QNONFINITE = 0x1, 0x2, 0x4
 PM_KBUF_HEAP, PM_KBUF_GROUP = 0, 1
 
@@ -56,6 +57,7 @@ SIGNATURES = {
     "pm_build": (_I, [_VP, _FP, _FP, _U32, _I, _VP]),
     "pm_query": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_bruteforce": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
+    "pm_query_noalloc": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_backward": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _FP, _FP, _VP]),
     "pm_gather_for": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _FP, _FP, _FP, _FP, _UP, _U32, _FP, _FP, _VP]),
     "pm_scale_flux": (_I, [_VP, _F, _VP]),

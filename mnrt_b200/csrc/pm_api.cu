@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "pm_internal.h"
@@ -525,3 +526,103 @@ pm_status pm_export_tree(pm_map* m, uint32_t* host_nodes, uint32_t max_nodes, fl
 }
 
 }  // extern "C"
+// ---------------------------------------------------------------------------
+// pm_query_noalloc: the query with its scratch in a fixed array.
+//
+// Some callers cannot allocate device memory when they query: cudaMalloc and
+// cudaFree synchronise the whole device, which stalls a render loop, and some
+// host applications hand the engine a fixed memory budget up front and let
+// nothing grow afterwards.  This entry point runs the same kernels as
+// pm_query, but the scratch they need beyond the caller's inputs and outputs
+// (query Morton keys, radix-sort histograms, the work counter) is carved from
+// one file-scope device array of a fixed size.  The map itself must already
+// be built.  Nothing here calls cudaMalloc, cudaFree or any allocating
+// library routine.
+//
+// The array is shared by every call on every handle.  Each call rewrites all
+// of it that it reads (the keys, the histograms) and query_knn clears the
+// work counter on the stream before the kernel starts, so one call's leftovers
+// never leak into the next; calls that overlap on the GPU race.
+namespace {
+
+constexpr uint32_t kNoallocMaxQ = PM_NOALLOC_MAX_QUERIES;
+constexpr size_t kNoallocSortWords = 32768;   // >= sort_scratch_words(kNoallocMaxQ), checked at set-up
+constexpr size_t kNoallocAlign = 256;
+constexpr size_t noalloc_round(size_t b) { return (b + kNoallocAlign - 1) / kNoallocAlign * kNoallocAlign; }
+constexpr size_t kNoallocKeys0 = 0;
+constexpr size_t kNoallocKeys1 = kNoallocKeys0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint64_t));
+constexpr size_t kNoallocVals0 = kNoallocKeys1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint64_t));
+constexpr size_t kNoallocVals1 = kNoallocVals0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
+constexpr size_t kNoallocSort = kNoallocVals1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
+constexpr size_t kNoallocCounter = kNoallocSort + noalloc_round(kNoallocSortWords * sizeof(uint32_t));
+constexpr size_t kNoallocBytes = kNoallocCounter + kNoallocAlign;
+
+// In host code this name is only a host-side handle for the runtime: its
+// device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up on
+// the first call per device, with that device current).
+pm_status noalloc_scratch(pm_map* m, unsigned char** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(m, "pm_query_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= kNoallocMaxDevices)
+        return fail(m, PM_ERR_UNSUPPORTED, "pm_query_noalloc supports device ordinals below %d", kNoallocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        if (sort_scratch_words(kNoallocMaxQ) > kNoallocSortWords)
+            return fail(m, PM_ERR_STATE, "pm_query_noalloc: sort scratch of the fixed array is too small");
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return fail(m, PM_ERR_CUDA, "pm_query_noalloc: cudaGetSymbolAddress of the scratch array failed: %s",
+                        cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return PM_OK;
+}
+
+}  // namespace
+
+extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, const float* d_qpos4,
+                                      const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,
+                                      uint32_t* d_count, void* stream) {
+    pm_status s = query_common(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, false);
+    if (s != PM_OK) return s;
+    if (desc->mode == PM_MODE_ZHOU_COMPAT)
+        return fail(m, PM_ERR_UNSUPPORTED, "pm_query_noalloc supports PM_MODE_EXACT only");
+    if (nq > kNoallocMaxQ)
+        return fail(m, PM_ERR_INVALID, "nq = %u exceeds PM_NOALLOC_MAX_QUERIES = %u; split the queries", nq,
+                    kNoallocMaxQ);
+    if (nq == 0) return PM_OK;
+    unsigned char* base = nullptr;
+    s = noalloc_scratch(m, &base);
+    if (s != PM_OK) return s;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
+    int nl = 0;
+    const uint32_t* order = nullptr;
+    if (desc->order == PM_ORDER_SORTED) {
+        uint64_t* keys[2] = {reinterpret_cast<uint64_t*>(base + kNoallocKeys0),
+                             reinterpret_cast<uint64_t*>(base + kNoallocKeys1)};
+        uint32_t* vals[2] = {reinterpret_cast<uint32_t*>(base + kNoallocVals0),
+                             reinterpret_cast<uint32_t*>(base + kNoallocVals1)};
+        nl += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), keys[0], vals[0], st);
+        const int cur = radix_sort_pairs(keys, vals, nq, 48, reinterpret_cast<uint32_t*>(base + kNoallocSort), st, &nl);
+        order = vals[cur];
+    }
+    QueryTuning t = tuning_of(m);
+    t.stats = nullptr;
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
+    nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
+                    reinterpret_cast<uint32_t*>(base + kNoallocCounter), t, st);
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_query_noalloc");
+}
