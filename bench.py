@@ -301,7 +301,7 @@ def run_ours(args, cfg) -> dict | None:
         "build_ms": build_ms, "query_ms": float(np.mean(queries)), "query_sort_ms": float(np.mean(sorts)),
         "query_kernel_ms": kern_ms, "query_only_mqueries_per_s": Q / (float(np.mean(queries)) / 1000.0) / 1e6,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profiled_traffic("k_knn_tree", args.config), "kernel": "k_knn_tree",
+                     "traffic": profiled_traffic("k_knn_group", args.config), "kernel": "k_knn_group",
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
         "roofline_build": {"bound": "hbm", "achieved": build_bytes / (build_ms / 1000.0) / 1e9, "peak": peak,
                            "unit": "GB/s", "frac": build_bytes / (build_ms / 1000.0) / 1e9 / peak,

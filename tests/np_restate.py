@@ -60,7 +60,7 @@ def radiance_fp64(pos4, pow4, q4, n4, nbr, cnt, k, r_max, filt="box", cone_k=1.0
     dirbits = pow4[:, 3].view(np.uint32)
     for q in range(nq):
         c = int(cnt[q])
-        r2 = float(np.float64(r_max) ** 2)
+        r2 = float(np.float64(np.float32(r_max)) ** 2)   # R is an FP32 parameter of the C ABI
         if c == k:
             dv = pos4[nbr[q, k - 1], :3].astype(np.float64) - q4[q, :3].astype(np.float64)
             r2 = float(dv @ dv)
