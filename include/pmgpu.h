@@ -181,16 +181,27 @@ PM_API pm_status pm_query_noalloc(pm_map* map, const pm_query_desc* desc, const 
                                   const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,
                                   uint32_t* d_count, void* stream);
 
-/* Reverse-mode adjoint of pm_query (exact mode).  Given dL/dE per query
- * (d_grad_rad4, rgb), writes dL/dpower (d_grad_pow4, rgb, w = 0) and
- * dL/dposition (d_grad_pos4, xyz, w = 0) for every photon in caller order.
- * d_nbr / d_r2 / d_count: the forward outputs (NULL = recompute the kNN).
- * Scatter is a deterministic sort-by-photon segmented reduction: the result
- * is bitwise reproducible. */
+/* Reverse-mode adjoint of pm_query (exact mode; no counterpart in the
+ * reference).  Given dL/dE per query (d_grad_rad4, rgb), writes dL/dpower
+ * (d_grad_pow4, rgb, w = 0) and dL/dposition (d_grad_pos4, xyz, w = 0) for
+ * every photon in caller order; either output may be NULL.
+ *   d_nbr, d_count: the forward's neighbour lists and counts (pm_query with
+ *          the same desc); d_nbr == NULL recomputes the kNN in chunks.
+ *   d_r2:  not read (r^2 is re-derived in FP64 from the k-th neighbour).
+ * Position gradients flow through the filter weights and through r^2, which
+ * the k-th neighbour sets.  Contributions are evaluated in FP64 and scattered
+ * by a sort by photon plus an ordered segmented sum (no float atomics): the
+ * result is bitwise reproducible, and identical with or without reuse and
+ * for any chunking. */
 PM_API pm_status pm_query_backward(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
                             const float* d_qnrm4, uint32_t nq, const float* d_grad_rad4, const uint32_t* d_nbr,
                             const float* d_r2, const uint32_t* d_count, float* d_grad_pow4, float* d_grad_pos4,
                             void* stream);
+
+/* Largest number of queries one backward pass handles at once (0 =
+ * automatic: up to 2^27 neighbour pairs per pass).  Smaller chunks need less
+ * scratch; results do not change. */
+PM_API pm_status pm_set_backward_chunk(pm_map* map, uint32_t max_queries);
 
 /* PhotonMap::GatherFor (PhotonMap.cpp:234-270, kernel_PhotonGather
  * GPU/photon_knn.cu:493-551): estimate at gather-ray hits and accumulate

@@ -59,6 +59,7 @@ SIGNATURES = {
     "pm_query_bruteforce": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_noalloc": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_backward": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _FP, _FP, _VP]),
+    "pm_set_backward_chunk": (_I, [_VP, _U32]),
     "pm_gather_for": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _FP, _FP, _FP, _FP, _UP, _U32, _FP, _FP, _VP]),
     "pm_scale_flux": (_I, [_VP, _F, _VP]),
     "pm_compute_query_radii": (_I, [_VP, C.POINTER(QueryDesc), _FP, _U32, _FP, _VP]),

@@ -42,11 +42,18 @@ struct pm_map {
     uint32_t cap_photons = 0;   // capacity of photon-sized buffers
     uint32_t cap_queries = 0;   // capacity of query-sized buffers
     // photon-sized
-    DevBuf pos, pow, nodes, hdr;
+    DevBuf pos, pow, inv, nodes, hdr;
     DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
     // query-sized
     DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter;
     DevBuf stats;           // query counters (profiling level 2)
+    // backward (pm_query_backward): pair sort, per-query records, segments,
+    // FP64 running sums, and the forward outputs when the kNN is recomputed
+    DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, qr2, qcnt, seg_start, seg_end, acc;
+    DevBuf rnbr, rcnt, rr2, rrad;
+    uint64_t cap_pairs = 0;
+    uint32_t cap_bq = 0, cap_bn = 0, cap_rq = 0;
+    uint32_t bwd_chunk = 0;   // max queries per backward chunk (0 = automatic)
     // profiling: events recorded on the call's stream when enabled
     bool profiling = false;
     int profile_level = 0;
@@ -126,6 +133,7 @@ pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
 #define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
     ENSURE(pos, cap * sizeof(float4));
     ENSURE(pow, cap * sizeof(float4));
+    ENSURE(inv, cap * sizeof(uint32_t));
     ENSURE(nodes, (cap + 1) * sizeof(Node));
     ENSURE(hdr, sizeof(MapHeader));
     ENSURE(keys0, cap * sizeof(uint64_t));
@@ -188,6 +196,7 @@ MapView view_of(pm_map* m) {
     MapView v;
     v.pos = P<float4>(m->pos);
     v.pow = P<float4>(m->pow);
+    v.inv = P<uint32_t>(m->inv);
     v.nodes = P<Node>(m->nodes);
     v.hdr = P<MapHeader>(m->hdr);
     v.n = m->n;
@@ -262,10 +271,12 @@ pm_status pm_create(pm_map** out, uint32_t max_photons, const float* aabb_min, c
 
 pm_status pm_destroy(pm_map* m) {
     if (!m) return PM_ERR_INVALID;
-    DevBuf* all[] = {&m->pos, &m->pow, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
+    DevBuf* all[] = {&m->pos, &m->pow, &m->inv, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
-                     &m->qscratch, &m->counter, &m->stats};
+                     &m->qscratch, &m->counter, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
+                     &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
+                     &m->rcnt, &m->rr2, &m->rrad};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -333,7 +344,7 @@ pm_status pm_build(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t
     const bool prof = m->profiling && !capturing(st);
     if (prof) cudaEventRecord(m->ev[0], st);
     const int nl = build_map(reinterpret_cast<const float4*>(d_pos4), reinterpret_cast<const float4*>(d_pow4), n,
-                             format, m->leaf_size, P<float4>(m->pos), P<float4>(m->pow), P<Node>(m->nodes),
+                             format, m->leaf_size, P<float4>(m->pos), P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes),
                              P<MapHeader>(m->hdr), bb, st, prof ? m->ev[1] : nullptr);
     if (prof) cudaEventRecord(m->ev[2], st);
     m->have_build_ev = prof;
@@ -398,12 +409,124 @@ pm_status pm_query_bruteforce(pm_map* m, const pm_query_desc* desc, const float*
     return check_cuda(m, "pm_query_bruteforce");
 }
 
+pm_status pm_set_backward_chunk(pm_map* m, uint32_t max_queries) {
+    if (!m) return PM_ERR_INVALID;
+    m->bwd_chunk = max_queries;
+    return PM_OK;
+}
+
+static pm_status ensure_bwd_capacity(pm_map* m, uint32_t chunk_q, uint32_t k, bool recompute, bool chunked,
+                                     cudaStream_t st) {
+    const uint64_t pairs = (uint64_t)chunk_q * k;
+    const uint32_t n = m->n ? m->n : 1;
+    const bool grow = pairs > m->cap_pairs || chunk_q > m->cap_bq || n > m->cap_bn || (chunked && !m->acc.ptr) ||
+                      (chunked && m->acc.bytes < (size_t)n * 6 * sizeof(double)) ||
+                      (recompute && (chunk_q > m->cap_rq || !m->rnbr.ptr || m->rnbr.bytes < pairs * 4));
+    if (!grow) return PM_OK;
+    if (capturing(st))
+        return fail(m, PM_ERR_STATE, "backward storage must grow during stream capture; run one backward first");
+    pm_status s;
+#define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
+    const uint64_t pc = pairs ? pairs : 1;
+    const size_t qc = chunk_q ? chunk_q : 1;
+    ENSURE(bkeys0, pc * sizeof(uint32_t));
+    ENSURE(bkeys1, pc * sizeof(uint32_t));
+    ENSURE(bvals0, pc * sizeof(uint32_t));
+    ENSURE(bvals1, pc * sizeof(uint32_t));
+    ENSURE(bscratch, bwd_sort_scratch_words(pc) * sizeof(uint32_t));
+    ENSURE(qrec, qc * sizeof(double4));
+    ENSURE(qr2, qc * sizeof(double));
+    ENSURE(qcnt, qc * sizeof(uint32_t));
+    ENSURE(seg_start, (size_t)n * sizeof(uint32_t));
+    ENSURE(seg_end, (size_t)n * sizeof(uint32_t));
+    if (chunked) ENSURE(acc, (size_t)n * 6 * sizeof(double));
+    if (recompute) {
+        ENSURE(rnbr, pc * sizeof(uint32_t));
+        ENSURE(rcnt, qc * sizeof(uint32_t));
+        ENSURE(rr2, qc * sizeof(float));
+        ENSURE(rrad, qc * sizeof(float4));
+        if (chunk_q > m->cap_rq) m->cap_rq = chunk_q;
+    }
+#undef ENSURE
+    if (pairs > m->cap_pairs) m->cap_pairs = pairs;
+    if (chunk_q > m->cap_bq) m->cap_bq = chunk_q;
+    if (n > m->cap_bn) m->cap_bn = n;
+    return PM_OK;
+}
+
 pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
                             uint32_t nq, const float* d_grad_rad4, const uint32_t* d_nbr, const float* d_r2,
                             const uint32_t* d_count, float* d_grad_pow4, float* d_grad_pos4, void* stream) {
-    (void)desc; (void)d_qpos4; (void)d_qnrm4; (void)nq; (void)d_grad_rad4; (void)d_nbr; (void)d_r2; (void)d_count;
-    (void)d_grad_pow4; (void)d_grad_pos4; (void)stream;
-    return fail(m, PM_ERR_UNSUPPORTED, "pm_query_backward is not available in this build");
+    (void)d_r2;   // r^2 is re-derived in FP64 from the k-th neighbour
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = validate_desc(m, desc, true);
+    if (s != PM_OK) return s;
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (!d_grad_pow4 && !d_grad_pos4) return fail(m, PM_ERR_INVALID, "both gradient outputs are NULL");
+    if ((d_grad_pow4 && !aligned16(d_grad_pow4)) || (d_grad_pos4 && !aligned16(d_grad_pos4)))
+        return fail(m, PM_ERR_INVALID, "gradient arrays must be 16-byte aligned");
+    if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_grad_rad4))
+        return fail(m, PM_ERR_INVALID, "query positions, normals and dL/dE must be non-NULL");
+    if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_grad_rad4)))
+        return fail(m, PM_ERR_INVALID, "query and dL/dE arrays must be 16-byte aligned");
+    if (m->n == 0) return PM_OK;   // no photons: nothing to differentiate
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t k = desc->k;
+    const uint64_t kMaxPairs = 1ull << 27;   // pairs sorted at once (about 2 GB of sort buffers)
+    uint32_t chunk = (uint32_t)(kMaxPairs / k);
+    if (m->bwd_chunk) chunk = m->bwd_chunk < chunk ? m->bwd_chunk : chunk;
+    if (nq > 0 && chunk > nq) chunk = nq;
+    if (chunk == 0) chunk = 1;
+    const uint32_t nchunks = nq ? (nq + chunk - 1) / chunk : 1;
+    const bool recompute = d_nbr == nullptr;
+    s = ensure_bwd_capacity(m, chunk, k, recompute, nchunks > 1, st);
+    if (s != PM_OK) return s;
+    if (recompute) {
+        s = ensure_query_capacity(m, chunk, st);
+        if (s != PM_OK) return s;
+    }
+    BwdArgs a;
+    a.pos = P<float4>(m->pos); a.pow = P<float4>(m->pow); a.inv = P<uint32_t>(m->inv);
+    a.qpos = reinterpret_cast<const float4*>(d_qpos4);
+    a.qnrm = reinterpret_cast<const float4*>(d_qnrm4);
+    a.grad = reinterpret_cast<const float4*>(d_grad_rad4);
+    a.n = m->n; a.k = k; a.r_max = desc->r_max; a.filter = desc->filter;
+    a.cone_k = desc->filter == PM_FILTER_CONE ? desc->cone_k : 1.0f;
+    a.min_found = desc->min_found;
+    a.qrec = P<double4>(m->qrec); a.qr2 = P<double>(m->qr2); a.qcnt = P<uint32_t>(m->qcnt);
+    a.keys = nullptr; a.vals = nullptr;
+    a.nbr = nullptr; a.count_in = nullptr;
+    BwdBuffers b;
+    b.keys[0] = P<uint32_t>(m->bkeys0); b.keys[1] = P<uint32_t>(m->bkeys1);
+    b.vals[0] = P<uint32_t>(m->bvals0); b.vals[1] = P<uint32_t>(m->bvals1);
+    b.scratch = P<uint32_t>(m->bscratch);
+    b.seg_start = P<uint32_t>(m->seg_start); b.seg_end = P<uint32_t>(m->seg_end);
+    b.acc = P<double>(m->acc);
+    int nl = 0;
+    for (uint32_t c = 0; c < nchunks; ++c) {
+        const uint32_t q0 = c * chunk;
+        const uint32_t nqc = nq ? ((nq - q0) < chunk ? (nq - q0) : chunk) : 0;
+        if (recompute) {
+            if (nqc > 0) {
+                const float4* qp = a.qpos + q0;
+                const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, qp, nqc, st, &nl) : nullptr;
+                QueryOutputs out{P<float4>(m->rrad), P<uint32_t>(m->rnbr), P<float>(m->rr2), P<uint32_t>(m->rcnt)};
+                QueryTuning t = tuning_of(m);
+                t.stats = nullptr;
+                nl += query_knn(view_of(m), params_of(desc), qp, a.qnrm + q0, order, nqc, out, P<uint32_t>(m->counter),
+                                t, st);
+            }
+            a.nbr = P<uint32_t>(m->rnbr);
+            a.count_in = P<uint32_t>(m->rcnt);
+        } else {
+            a.nbr = d_nbr + (size_t)q0 * k;
+            a.count_in = d_count ? d_count + q0 : nullptr;
+        }
+        nl += backward_chunk(a, q0, nqc, c == 0, c + 1 == nchunks, b, reinterpret_cast<float4*>(d_grad_pow4),
+                             reinterpret_cast<float4*>(d_grad_pos4), st);
+    }
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_query_backward");
 }
 
 pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit_pos4, const float* d_hit_nrm4,

@@ -1,0 +1,253 @@
+// pm_backward.cu -- reverse-mode adjoint of the exact-kNN radiance estimate.
+//
+// The reference has no adjoint; the forward it differentiates is the
+// estimate of GPU/photon_knn.cu:113-235 (E = norm(r^2) * sum front * w * flux,
+// r^2 = d^2 of the k-th neighbour when k were found, else R^2) with the
+// engine's filters.  For query q, channel c and neighbour p:
+//
+//   E_qc   = norm(r2_q) * S_qc,   S_qc = sum_p f_qp * w(d2_qp, r2_q) * Phi_pc
+//   dL/dPhi_pc  = sum_q g_qc * norm_q * f_qp * w_qp                  (exact, linear)
+//   dL/dx_p     = sum_q 2 (x_p - q) * [ f_qp * (sum_c g_qc norm_q Phi_pc) * dw/dd2
+//                                      + [p is the k-th of q] * G_q ]
+//   G_q         = sum_c g_qc * (dnorm/dr2 * S_qc + norm_q * sum_p f_qp Phi_pc dw/dr2)
+//
+// The k-th neighbour moves r^2 = d2(q, x_k), which feeds every weight and the
+// normalisation of q; that is the G_q path.  Set changes (a photon entering or
+// leaving N(q)) are measure-zero kinks and contribute nothing.
+//
+// Scatter without float atomics, deterministic by construction:
+//   1. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
+//                   -> per-query record (g * norm, G), count, r^2
+//   2. k_bwd_pairs  one (photon tree position, pair id) key-value per
+//                   neighbour slot; empty slots get the sentinel key n
+//   3. stable LSD radix sort by photon (pair ids of one photon stay in
+//      query order)
+//   4. k_bwd_bounds segment [start, end) of every photon in the sorted array
+//   5. k_bwd_reduce thread per photon: walks its segment in order and sums
+//                   the FP64 contributions; the running sum carries across
+//                   query chunks, so chunked and single-pass runs give the
+//                   same bits
+// Contributions are evaluated in FP64 from the FP32 inputs (the neighbour set
+// and the front test follow the FP32 forward contract).
+#include "pm_internal.h"
+
+namespace pm {
+
+namespace {
+
+constexpr double kPiD = 3.14159265358979323846;
+
+__device__ __forceinline__ double norm_of(int filter, double r2, double cone_k) {
+    if (filter == 1) return 1.0 / ((1.0 - 2.0 / (3.0 * cone_k)) * kPiD * r2);
+    if (filter == 2) return 2.0 / (kPiD * r2);
+    return 1.0 / (kPiD * r2);
+}
+
+// w, dw/dd2 and dw/dr2 of the filters (FP64).
+__device__ __forceinline__ void weight_terms(int filter, double d2, double r2, double cone_k, double& w, double& dw_dd2,
+                                             double& dw_dr2) {
+    if (filter == 1) {   // cone: w = 1 - d / (k_c r)
+        const double d = sqrt(d2), r = sqrt(r2);
+        w = 1.0 - d / (cone_k * r);
+        dw_dd2 = d > 0.0 ? -1.0 / (2.0 * d * cone_k * r) : 0.0;
+        dw_dr2 = d / (2.0 * cone_k * r2 * r);
+    } else if (filter == 2) {   // Epanechnikov: w = 1 - d^2 / r^2
+        w = 1.0 - d2 / r2;
+        dw_dd2 = -1.0 / r2;
+        dw_dr2 = d2 / (r2 * r2);
+    } else {   // box
+        w = 1.0;
+        dw_dd2 = 0.0;
+        dw_dr2 = 0.0;
+    }
+}
+
+__device__ __forceinline__ double dist2_d(const float4& a, const float4& b) {
+    const double dx = (double)a.x - (double)b.x, dy = (double)a.y - (double)b.y, dz = (double)a.z - (double)b.z;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One warp per query of the chunk.
+__global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp_global >= nq_chunk) return;
+    const uint32_t ql = warp_global, q = q0 + ql;
+    const uint32_t k = a.k;
+    const uint32_t* row = a.nbr + (size_t)ql * k;
+    // neighbours found: the count output, else the valid prefix of the row
+    uint32_t cnt;
+    if (a.count_in) {
+        cnt = a.count_in[ql];
+    } else {
+        uint32_t c = 0;
+        for (uint32_t j = lane; j < k; j += 32) c += row[j] != kInvalid ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        cnt = c;
+    }
+    if (cnt > k) cnt = k;
+    const float4 qp = a.qpos[q];
+    const float4 qn = a.qnrm[q];
+    const double R2 = (double)a.r_max * (double)a.r_max;
+    double r2 = R2;
+    if (cnt == k) r2 = dist2_d(a.pos[a.inv[row[k - 1]]], qp);
+    const bool active = cnt > 0 && cnt >= a.min_found && r2 > 0.0 && isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
+    double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
+    if (active) {
+        for (uint32_t j = lane; j < cnt; j += 32) {
+            const uint32_t p = a.inv[row[j]];
+            const float4 pp = a.pos[p], pw = a.pow[p];
+            if (!front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) continue;
+            double w, dwd, dwr;
+            weight_terms(a.filter, dist2_d(pp, qp), r2, (double)a.cone_k, w, dwd, dwr);
+            S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
+            T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
+        }
+    }
+    S0 = warp_sum_d(S0); S1 = warp_sum_d(S1); S2 = warp_sum_d(S2);
+    T0 = warp_sum_d(T0); T1 = warp_sum_d(T1); T2 = warp_sum_d(T2);
+    if (lane != 0) return;
+    double4 rec = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (active) {
+        const float4 g = a.grad[q];
+        const double nrm = norm_of(a.filter, r2, (double)a.cone_k);
+        rec.x = (double)g.x * nrm;
+        rec.y = (double)g.y * nrm;
+        rec.z = (double)g.z * nrm;
+        if (cnt == k) {
+            const double dn = -nrm / r2;
+            rec.w = (double)g.x * (dn * S0 + nrm * T0) + (double)g.y * (dn * S1 + nrm * T1) +
+                    (double)g.z * (dn * S2 + nrm * T2);
+        }
+    }
+    a.qrec[ql] = rec;
+    a.qr2[ql] = active ? r2 : 0.0;
+    a.qcnt[ql] = active ? cnt : 0u;
+}
+
+// One thread per neighbour slot of the chunk.
+__global__ void k_bwd_pairs(BwdArgs a, uint32_t nq_chunk) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t total = (uint64_t)nq_chunk * a.k;
+    if (i >= total) return;
+    const uint32_t ql = (uint32_t)(i / a.k), j = (uint32_t)(i % a.k);
+    uint32_t key = a.n;   // sentinel: sorts after every photon
+    if (j < a.qcnt[ql]) key = a.inv[a.nbr[i]];
+    a.keys[i] = key;
+    a.vals[i] = (uint32_t)i;
+}
+
+// Segment bounds of every photon in the sorted keys (start = end = 0 when
+// the photon has no pair; both arrays are cleared before).
+__global__ void k_bwd_bounds(const uint32_t* __restrict__ keys, uint64_t m, uint32_t n, uint32_t* __restrict__ start,
+                             uint32_t* __restrict__ end) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t key = keys[i];
+    if (key >= n) return;
+    if (i == 0 || keys[i - 1] != key) start[key] = (uint32_t)i;
+    if (i + 1 == m || keys[i + 1] != key) end[key] = (uint32_t)(i + 1);
+}
+
+// One thread per photon (tree position).  acc holds 6 doubles per photon
+// between chunks.
+__global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict__ sorted_vals,
+                             const uint32_t* __restrict__ start, const uint32_t* __restrict__ end, int first, int last,
+                             double* __restrict__ acc, float4* __restrict__ grad_pow, float4* __restrict__ grad_pos) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    double g0 = 0, g1 = 0, g2 = 0, x0 = 0, x1 = 0, x2 = 0;
+    if (!first) {
+        const double* s = acc + (size_t)p * 6;
+        g0 = s[0]; g1 = s[1]; g2 = s[2]; x0 = s[3]; x1 = s[4]; x2 = s[5];
+    }
+    const uint32_t b = start[p], e = end[p];
+    if (b < e) {
+        const float4 pp = a.pos[p], pw = a.pow[p];
+        const uint32_t dir = __float_as_uint(pw.w);
+        const uint32_t k = a.k;
+        for (uint32_t i = b; i < e; ++i) {
+            const uint32_t v = sorted_vals[i];
+            const uint32_t ql = v / k, j = v % k;
+            const uint32_t q = q0 + ql;
+            const double4 rec = a.qrec[ql];
+            const double r2 = a.qr2[ql];
+            if (!(r2 > 0.0)) continue;
+            const float4 qp = a.qpos[q];
+            const float4 qn = a.qnrm[q];
+            const double dx = (double)pp.x - (double)qp.x, dy = (double)pp.y - (double)qp.y,
+                         dz = (double)pp.z - (double)qp.z;
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            double coef = 0.0;
+            if (front_rn(qn.x, qn.y, qn.z, dir)) {
+                double w, dwd, dwr;
+                weight_terms(a.filter, d2, r2, (double)a.cone_k, w, dwd, dwr);
+                g0 += w * rec.x;
+                g1 += w * rec.y;
+                g2 += w * rec.z;
+                coef = (rec.x * pw.x + rec.y * pw.y + rec.z * pw.z) * dwd;
+            }
+            if (j == k - 1) coef += rec.w;   // the k-th neighbour sets r^2 of q
+            x0 += 2.0 * coef * dx;
+            x1 += 2.0 * coef * dy;
+            x2 += 2.0 * coef * dz;
+        }
+    }
+    if (last) {
+        const uint32_t caller = __float_as_uint(a.pos[p].w);
+        if (grad_pow) grad_pow[caller] = make_float4((float)g0, (float)g1, (float)g2, 0.0f);
+        if (grad_pos) grad_pos[caller] = make_float4((float)x0, (float)x1, (float)x2, 0.0f);
+    } else {
+        double* s = acc + (size_t)p * 6;
+        s[0] = g0; s[1] = g1; s[2] = g2; s[3] = x0; s[4] = x1; s[5] = x2;
+    }
+}
+
+int key_bits_for(uint32_t n) {
+    int b = 1;
+    while (b < 32 && (1ull << b) <= (uint64_t)n) ++b;   // sentinel n must fit
+    return b;
+}
+
+}  // namespace
+
+size_t bwd_sort_scratch_words(uint64_t pairs) { return sort_scratch_words((uint32_t)pairs) + 64; }
+
+int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
+                   float4* grad_pow, float4* grad_pos, cudaStream_t st) {
+    int nl = 0;
+    const uint64_t pairs = (uint64_t)nq_chunk * a.k;
+    BwdArgs x = a;
+    x.keys = b.keys[0];
+    x.vals = b.vals[0];
+    if (nq_chunk > 0) {
+        const uint32_t warps_per_block = 8;
+        k_bwd_prep<<<(nq_chunk + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
+        k_bwd_pairs<<<(uint32_t)((pairs + 255) / 256), 256, 0, st>>>(x, nq_chunk);
+        nl += 2;
+    }
+    uint32_t* keys[2] = {b.keys[0], b.keys[1]};
+    uint32_t* vals[2] = {b.vals[0], b.vals[1]};
+    const int cur = radix_sort_pairs32(keys, vals, (uint32_t)pairs, key_bits_for(a.n), b.scratch, st, &nl);
+    cudaMemsetAsync(b.seg_start, 0, (size_t)a.n * sizeof(uint32_t), st);
+    cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
+    if (pairs > 0) {
+        k_bwd_bounds<<<(uint32_t)((pairs + 255) / 256), 256, 0, st>>>(keys[cur], pairs, a.n, b.seg_start, b.seg_end);
+        ++nl;
+    }
+    if (a.n > 0) {
+        k_bwd_reduce<<<(a.n + 127) / 128, 128, 0, st>>>(x, q0, vals[cur], b.seg_start, b.seg_end, first ? 1 : 0,
+                                                        last ? 1 : 0, b.acc, grad_pow, grad_pos);
+        ++nl;
+    }
+    return nl;
+}
+
+}  // namespace pm

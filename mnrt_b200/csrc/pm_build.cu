@@ -13,7 +13,8 @@
 //                     order -- and the whole tree -- is deterministic
 //                     (the reference picks sides of split-plane ties at
 //                     random, GPU/kdtree.cu:806-815)
-//   4. k_gather       photons into tree order as SoA float4 records
+//   4. k_gather       photons into tree order as SoA float4 records, and the
+//                     inverse permutation (caller index -> tree position)
 //   5. k_radix_tree   binary radix tree over the sorted codes (Karras 2012):
 //                     each internal node splits at the highest Morton bit
 //                     that differs inside its range, i.e. at the spatial
@@ -118,7 +119,7 @@ __global__ void k_morton(const float4* __restrict__ pos, uint32_t n, const MapHe
 
 __global__ void k_gather(const float4* __restrict__ pos, const float4* __restrict__ pw,
                          const uint32_t* __restrict__ order, uint32_t n, int format, float4* __restrict__ out_pos,
-                         float4* __restrict__ out_pow) {
+                         float4* __restrict__ out_pow, uint32_t* __restrict__ inv) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t src = order[i];
@@ -127,6 +128,7 @@ __global__ void k_gather(const float4* __restrict__ pos, const float4* __restric
     const uint32_t dir = (format == 0) ? spherical_to_oct(p.w, w.w) : __float_as_uint(w.w);
     out_pos[i] = make_float4(p.x, p.y, p.z, __uint_as_float(src));
     out_pow[i] = make_float4(w.x, w.y, w.z, __uint_as_float(dir));
+    inv[src] = i;
 }
 
 // Common-prefix length of sorted codes i and j, caller index breaking ties.
@@ -298,7 +300,7 @@ void scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr, cudaStream_
 }
 
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
-              float4* out_pos, float4* out_pow, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
+              float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
               cudaStream_t st, cudaEvent_t sort_done) {
     int nl = 0;
     const uint32_t nb = (uint32_t)((n + kBoundsThreads - 1) / kBoundsThreads);
@@ -314,7 +316,7 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
         uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
         const int cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl);
         if (sort_done) cudaEventRecord(sort_done, st);
-        k_gather<<<grid, tb, 0, st>>>(in_pos, in_pow, vals[cur], n, format, out_pos, out_pow);
+        k_gather<<<grid, tb, 0, st>>>(in_pos, in_pow, vals[cur], n, format, out_pos, out_pow, inv);
         nl += 2;
         if (n > 1) {
             const uint32_t ni = n - 1, gi = (ni + tb - 1) / tb;

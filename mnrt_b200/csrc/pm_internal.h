@@ -16,12 +16,15 @@ int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scra
 size_t sort_scratch_words(uint32_t n);
 int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
                      cudaStream_t st, int* launches = nullptr);
+int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
+                       cudaStream_t st, int* launches = nullptr);
 
 // Device buffers describing one built map (the build writes them, the
 // query reads them).  Pointers are device addresses.
 struct MapView {
     const float4* pos;      // tree order: xyz, w = caller index bits
     const float4* pow;      // tree order: rgb, w = octahedral direction bits
+    const uint32_t* inv;    // caller index -> tree position
     const Node* nodes;      // [0] = super-root, internal nodes from 1
     MapHeader* hdr;
     uint32_t n;             // photon count (host copy)
@@ -48,7 +51,7 @@ size_t build_bytes_needed(uint32_t n);
 // Returns the number of kernels launched; sort_done (if set) is recorded on
 // the stream right after the radix sort.
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
-              float4* out_pos, float4* out_pow, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
+              float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
               cudaStream_t st, cudaEvent_t sort_done = nullptr);
 void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st);
 
@@ -83,5 +86,38 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);
 int query_smem_bytes_per_warp(uint32_t k);
+
+// pm_backward.cu
+struct BwdArgs {
+    const float4* pos;        // tree order
+    const float4* pow;
+    const uint32_t* inv;      // caller index -> tree position
+    const float4* qpos;       // all queries (indexed by global query id)
+    const float4* qnrm;
+    const float4* grad;       // dL/dE per query (rgb)
+    const uint32_t* nbr;      // this chunk's neighbour rows (caller indices, sorted by (d^2, index))
+    const uint32_t* count_in; // this chunk's counts, or nullptr (derived from the rows)
+    uint32_t n, k;
+    float r_max;
+    int filter;
+    float cone_k;
+    uint32_t min_found;
+    double4* qrec;            // per chunk query: g * norm (xyz), G (w)
+    double* qr2;              // per chunk query: r^2 (0 = no gradient)
+    uint32_t* qcnt;           // per chunk query: neighbours carrying gradient
+    uint32_t* keys;           // pair keys / values (set by backward_chunk)
+    uint32_t* vals;
+};
+struct BwdBuffers {
+    uint32_t* keys[2];
+    uint32_t* vals[2];
+    uint32_t* scratch;
+    uint32_t* seg_start;
+    uint32_t* seg_end;
+    double* acc;              // 6 doubles per photon, carried between chunks
+};
+size_t bwd_sort_scratch_words(uint64_t pairs);
+int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
+                   float4* grad_pow, float4* grad_pos, cudaStream_t st);
 
 }  // namespace pm

@@ -122,7 +122,8 @@ int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scra
 
 // ------------------------------------------------------------ radix sort --
 
-__global__ void __launch_bounds__(kSortThreads) k_digit_hist(const uint64_t* __restrict__ keys, uint32_t n,
+template <class Key>
+__global__ void __launch_bounds__(kSortThreads) k_digit_hist(const Key* __restrict__ keys, uint32_t n,
                                                                int shift, uint32_t ntiles, uint32_t* __restrict__ hist) {
     __shared__ uint32_t s_hist[256];
     s_hist[threadIdx.x] = 0;
@@ -137,11 +138,12 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_hist(const uint64_t* __r
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s_hist[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint64_t* __restrict__ keys_in,
+template <class Key>
+__global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __restrict__ keys_in,
                                                                   const uint32_t* __restrict__ vals_in, uint32_t n,
                                                                   int shift, uint32_t ntiles,
                                                                   const uint32_t* __restrict__ offsets,
-                                                                  uint64_t* __restrict__ keys_out,
+                                                                  Key* __restrict__ keys_out,
                                                                   uint32_t* __restrict__ vals_out) {
     __shared__ uint32_t s_base[256];              // global offset + keys of this digit seen so far
     __shared__ uint32_t s_warp[kSortWarps][256];  // per-warp count, then per-warp start
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const uint64_t* 
     for (int i = 0; i < kSortItems; ++i) {
         const uint64_t g = base + (uint64_t)i * kSortThreads + threadIdx.x;
         const bool valid = g < n;
-        uint64_t key = valid ? keys_in[g] : 0ull;
+        Key key = valid ? keys_in[g] : Key(0);
         uint32_t val = valid ? vals_in[g] : 0u;
         const uint32_t digit = valid ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
 #pragma unroll
@@ -191,8 +193,9 @@ size_t sort_scratch_words(uint32_t n) {
 // Sorts by bits [0, key_bits) of the keys.  Returns which buffer holds the
 // result (0: keys[0]/vals[0], 1: keys[1]/vals[1]).  Buffers of the other
 // index are clobbered.
-int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
-                     cudaStream_t st, int* launches) {
+template <class Key>
+static int radix_sort_impl(Key* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
+                           cudaStream_t st, int* launches) {
     if (n <= 1) return 0;
     int nl = 0;
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
@@ -200,14 +203,24 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_b
     uint32_t* scan_tmp = scratch + (size_t)tiles * 256;
     int cur = 0;
     for (int shift = 0; shift < key_bits; shift += 8) {
-        k_digit_hist<<<tiles, kSortThreads, 0, st>>>(keys[cur], n, shift, tiles, hist);
+        k_digit_hist<Key><<<tiles, kSortThreads, 0, st>>>(keys[cur], n, shift, tiles, hist);
         nl += 2 + exclusive_scan(hist, hist, tiles * 256u, scan_tmp, nullptr, st);
-        k_digit_scatter<<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
-                                                         keys[cur ^ 1], vals[cur ^ 1]);
+        k_digit_scatter<Key><<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
+                                                              keys[cur ^ 1], vals[cur ^ 1]);
         cur ^= 1;
     }
     if (launches) *launches += nl;
     return cur;
+}
+
+int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
+                     cudaStream_t st, int* launches) {
+    return radix_sort_impl<uint64_t>(keys, vals, n, key_bits, scratch, st, launches);
+}
+
+int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
+                       cudaStream_t st, int* launches) {
+    return radix_sort_impl<uint32_t>(keys, vals, n, key_bits > 32 ? 32 : key_bits, scratch, st, launches);
 }
 
 }  // namespace pm

@@ -195,3 +195,29 @@ class PhotonMap:
         if self.num_photons == 0:
             return
         L.check(self._lib.pm_scale_flux(self._h, float(scale), _stream(stream)), self._h)
+
+    def query_backward(self, qpos: torch.Tensor, qnrm: torch.Tensor, grad_rad: torch.Tensor, nbr=None, count=None,
+                       grad_pow: torch.Tensor | None = None, grad_pos: torch.Tensor | None = None, stream=None,
+                       want_pow: bool = True, want_pos: bool = True, **kw):
+        """Adjoint of query(): dL/dpower and dL/dposition (n, 4) in caller order.
+        nbr / count: the forward's outputs (None recomputes the kNN)."""
+        d = self.desc(**kw)
+        nq = int(qpos.shape[0])
+        dev = qpos.device
+        n = max(self.num_photons, 1)
+        if want_pow and grad_pow is None:
+            grad_pow = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        if want_pos and grad_pos is None:
+            grad_pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        grad_rad = grad_rad.contiguous()
+        if grad_rad.shape[1] != 4:
+            g4 = torch.zeros((nq, 4), dtype=torch.float32, device=dev)
+            g4[:, :3] = grad_rad
+            grad_rad = g4
+        L.check(self._lib.pm_query_backward(self._h, C.byref(d), _ptr(qpos), _ptr(qnrm), nq, _ptr(grad_rad),
+                                            _ptr(nbr), None, _ptr(count), _ptr(grad_pow) if want_pow else None,
+                                            _ptr(grad_pos) if want_pos else None, _stream(stream)), self._h)
+        return grad_pow, grad_pos
+
+    def set_backward_chunk(self, max_queries: int) -> None:
+        L.check(self._lib.pm_set_backward_chunk(self._h, int(max_queries)), self._h)

@@ -50,6 +50,7 @@ def load() -> C.CDLL:
         "orc_kdtree_free": (None, [P]),
         "orc_knn_kdtree": (None, [P, P, u32, u32, f32, P, P, P, P, i32]),
         "orc_radiance_fp64": (None, [P, P, P, P, u32, P, P, u32, f32, i32, f32, u32, P, i32]),
+        "orc_backward_fp64": (None, [P, P, P, P, u32, u32, P, P, u32, f32, i32, f32, u32, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -127,6 +128,23 @@ def radiance_fp64(pos4, pow4, q4, n4, nbr, count, k: int, r_max: float, filt: st
     lib.orc_radiance_fp64(pos4.ctypes.data, pow4.ctypes.data, q4.ctypes.data, n4.ctypes.data, nq, nbr.ctypes.data,
                           count.ctypes.data, k, r_max, FILTER_IDS[filt], cone_k, min_found, out.ctypes.data, threads)
     return out
+
+
+def backward_fp64(pos4, pow4, q4, n4, nbr, count, k: int, r_max: float, grad, filt: str = "box",
+                  cone_k: float = 1.0, min_found: int = 0):
+    """FP64 host reference gradient of L given dL/dE (grad, (nq, 3)): returns
+    (dL/dpower (n, 3), dL/dposition (n, 3)) for the given neighbour sets."""
+    lib = load()
+    pos4, pow4, q4, n4 = (_c(a, np.float32) for a in (pos4, pow4, q4, n4))
+    nbr, count = _c(nbr, np.uint32), _c(count, np.uint32)
+    grad = _c(grad, np.float64)
+    n, nq = pos4.shape[0], q4.shape[0]
+    gp = np.empty((n, 3), np.float64)
+    gx = np.empty((n, 3), np.float64)
+    lib.orc_backward_fp64(pos4.ctypes.data, pow4.ctypes.data, q4.ctypes.data, n4.ctypes.data, n, nq, nbr.ctypes.data,
+                          count.ctypes.data, k, r_max, FILTER_IDS[filt], cone_k, min_found, grad.ctypes.data,
+                          gp.ctypes.data, gx.ctypes.data)
+    return gp, gx
 
 
 def threads_available() -> int:

@@ -22,7 +22,6 @@
 //   * photon layout: position.w = azimuth phi, power.w = polar theta,
 //     direction = (sin t cos p, sin t sin p, cos t)           GPU/photon_dev.h:71-113,
 //                                                              GPU/mncudautil_dev.h:345-352
-//   * Zhou histogram radius refinement (compat mode)          GPU/kdtree_point.cu:118-267
 //
 // The engine's own contract on top of that (it defines "exact kNN", which the
 // reference only approximates, Help/MNRT_Documentation.html section 4.2):
@@ -409,6 +408,80 @@ void orc_radiance_fp64(const float* pos4, const float* pow4, const float* q4, co
             for (int c = 0; c < 3; ++c) out[3 * q + c] = acc[c] * norm;
         }
     });
+}
+
+// Host reference gradient of a loss L through the FP64 estimate above, for
+// given neighbour sets (rows sorted by (d^2, index)).  grad: dL/dE, 3 doubles
+// per query.  Writes dL/dpower and dL/dposition, 3 doubles per photon.  The
+// adjoint has no reference counterpart; it differentiates E = norm(r^2) *
+// sum front * w(d^2, r^2) * flux with r^2 = d^2 of the k-th neighbour (when k
+// were found), so the k-th neighbour's position also moves every weight and
+// the normalisation of its query.  Single-threaded, queries in order.
+void orc_backward_fp64(const float* pos4, const float* pow4, const float* q4, const float* n4, uint32_t n,
+                       uint32_t nq, const uint32_t* nbr, const uint32_t* count, uint32_t k, float R, int filter,
+                       float cone_k, uint32_t min_found, const double* grad, double* out_gpow, double* out_gpos) {
+    std::fill(out_gpow, out_gpow + 3 * (size_t)n, 0.0);
+    std::fill(out_gpos, out_gpos + 3 * (size_t)n, 0.0);
+    const double kc = (double)cone_k;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const uint32_t cnt = count[q];
+        const double qx = q4[4 * (size_t)q], qy = q4[4 * (size_t)q + 1], qz = q4[4 * (size_t)q + 2];
+        if (!(std::isfinite(qx) && std::isfinite(qy) && std::isfinite(qz))) continue;
+        double r2 = (double)R * (double)R;
+        const uint32_t* row = nbr + (size_t)q * k;
+        if (cnt == k && k > 0) {
+            const uint32_t pk = row[k - 1];
+            const double dx = pos4[4 * (size_t)pk] - qx, dy = pos4[4 * (size_t)pk + 1] - qy, dz = pos4[4 * (size_t)pk + 2] - qz;
+            r2 = dx * dx + dy * dy + dz * dz;
+        }
+        if (cnt == 0 || cnt < min_found || !(r2 > 0.0)) continue;
+        double norm;
+        if (filter == 1) norm = 1.0 / ((1.0 - 2.0 / (3.0 * kc)) * kPi * r2);
+        else if (filter == 2) norm = 2.0 / (kPi * r2);
+        else norm = 1.0 / (kPi * r2);
+        const double g[3] = {grad[3 * (size_t)q], grad[3 * (size_t)q + 1], grad[3 * (size_t)q + 2]};
+        const double gn[3] = {g[0] * norm, g[1] * norm, g[2] * norm};
+        double S[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+        for (int pass = 0; pass < 2; ++pass) {
+            double Gr = 0.0;
+            if (pass == 1 && cnt == k) {
+                const double dn = -norm / r2;
+                for (int c = 0; c < 3; ++c) Gr += g[c] * (dn * S[c] + norm * T[c]);
+            }
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t p = row[j];
+                const double dx = pos4[4 * (size_t)p] - qx, dy = pos4[4 * (size_t)p + 1] - qy, dz = pos4[4 * (size_t)p + 2] - qz;
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const bool fr = front_f32(n4[4 * (size_t)q], n4[4 * (size_t)q + 1], n4[4 * (size_t)q + 2], f2u(pow4[4 * (size_t)p + 3]));
+                double w = 1.0, dwd = 0.0, dwr = 0.0;
+                if (filter == 1) {
+                    const double d = std::sqrt(d2), r = std::sqrt(r2);
+                    w = 1.0 - d / (kc * r);
+                    dwd = d > 0.0 ? -1.0 / (2.0 * d * kc * r) : 0.0;
+                    dwr = d / (2.0 * kc * r2 * r);
+                } else if (filter == 2) {
+                    w = 1.0 - d2 / r2;
+                    dwd = -1.0 / r2;
+                    dwr = d2 / (r2 * r2);
+                }
+                const double phi[3] = {pow4[4 * (size_t)p], pow4[4 * (size_t)p + 1], pow4[4 * (size_t)p + 2]};
+                if (pass == 0) {
+                    if (fr)
+                        for (int c = 0; c < 3; ++c) { S[c] += w * phi[c]; T[c] += dwr * phi[c]; }
+                    continue;
+                }
+                double coef = 0.0;
+                if (fr) {
+                    for (int c = 0; c < 3; ++c) out_gpow[3 * (size_t)p + c] += w * gn[c];
+                    coef = (gn[0] * phi[0] + gn[1] * phi[1] + gn[2] * phi[2]) * dwd;
+                }
+                if (j == k - 1) coef += Gr;
+                out_gpos[3 * (size_t)p] += 2.0 * coef * dx;
+                out_gpos[3 * (size_t)p + 1] += 2.0 * coef * dy;
+                out_gpos[3 * (size_t)p + 2] += 2.0 * coef * dz;
+            }
+        }
+    }
 }
 
 }  // extern "C"

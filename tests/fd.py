@@ -1,0 +1,154 @@
+"""FP64 central finite differences of the squared-error loss through the
+photon-map estimate (test infrastructure for the adjoint checks).
+
+    L(x, Phi) = sum_q sum_c (E_qc - T_qc)^2
+
+E follows the engine's contract: the neighbour set of a query is the k
+photons with the smallest (FP32 d^2, index) below R^2, and the estimate over
+that set is evaluated in FP64 (the oracle's radiance_fp64).  Moving one
+photon p changes only the queries whose set contains p or could gain p, and
+their new set is the k nearest among their old k + 1 nearest plus p, so each
+finite difference re-evaluates a few hundred queries exactly instead of the
+whole map.  A sample whose neighbour set (or k-th neighbour) changes inside
+[-h, +h] sits on a kink of L and is excluded; the count is reported.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+from scipy.spatial import cKDTree
+
+
+def _d2_f32(q: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """FP32 d^2 with the engine's operation order; q (m, 3), p (m, c, 3)."""
+    q = q[:, None, :].astype(np.float32)
+    p = p.astype(np.float32)
+    dx = (p[..., 0] - q[..., 0]).astype(np.float32)
+    dy = (p[..., 1] - q[..., 1]).astype(np.float32)
+    dz = (p[..., 2] - q[..., 2]).astype(np.float32)
+    return ((dx * dx + dy * dy).astype(np.float32) + dz * dz).astype(np.float32)
+
+
+@dataclass
+class FDResult:
+    fd: np.ndarray          # (s, 3) finite differences (nan where excluded)
+    excluded: np.ndarray    # (s, 3) bool
+    num_excluded: int
+
+
+class LossFD:
+    def __init__(self, oracle_mod, pos4, pow4, q4, n4, target, k: int, r_max: float, filt: str, cone_k: float = 1.0,
+                 min_found: int = 0):
+        self.o = oracle_mod
+        self.pos = np.ascontiguousarray(pos4, np.float32)
+        self.pw = np.ascontiguousarray(pow4, np.float32)
+        self.q = np.ascontiguousarray(q4, np.float32)
+        self.n = np.ascontiguousarray(n4, np.float32)
+        self.t = np.asarray(target, np.float64)
+        self.k, self.R, self.filt, self.cone_k, self.min_found = k, r_max, filt, cone_k, min_found
+        self.r2max = np.float32(r_max) * np.float32(r_max)
+        idx, _d2, cnt, r2 = oracle_mod.KdTree(self.pos).knn(self.q, k + 1, r_max)
+        self.idx1, self.cnt1 = idx, cnt
+        self.rk = np.sqrt(r2.astype(np.float64))            # k+1-th distance bound (or R)
+        self.qtree = cKDTree(self.q[:, :3].astype(np.float64))
+
+    def _rows(self, qsel: np.ndarray, p: int, newpos: np.ndarray):
+        """New k-NN rows (caller indices, -1 padded) and counts of queries qsel
+        with photon p at newpos."""
+        k = self.k
+        cand = self.idx1[qsel].astype(np.int64)
+        cand = np.where(cand == 0xFFFFFFFF, -1, cand)
+        cand = np.where(cand == p, -1, cand)                 # p is re-added below
+        cand = np.concatenate([cand, np.full((len(qsel), 1), p, np.int64)], axis=1)
+        pts = np.where(cand[..., None] >= 0, self.pos[np.maximum(cand, 0), :3], np.float32(np.inf))
+        pts[cand == p] = newpos
+        d2 = _d2_f32(self.q[qsel, :3], pts)
+        d2 = np.where(cand >= 0, d2, np.float32(np.inf))
+        ok = d2 < self.r2max
+        key_d = np.where(ok, d2, np.float32(np.inf))
+        key_i = np.where(ok, cand, np.iinfo(np.int64).max)
+        order = np.lexsort((key_i, key_d), axis=1)
+        rows = np.take_along_axis(np.where(ok, cand, -1), order, axis=1)[:, :k]
+        cnt = np.minimum(ok.sum(1), k)
+        return rows, cnt
+
+    def _loss(self, qsel, rows, cnt, pos):
+        nbr = np.where(rows >= 0, rows, 0).astype(np.uint32)
+        e = self.o.radiance_fp64(pos, self.pw, self.q[qsel], self.n[qsel], nbr, cnt.astype(np.uint32), self.k,
+                                 self.R, self.filt, self.cone_k, self.min_found)
+        return float(((e - self.t[qsel]) ** 2).sum())
+
+    def _affected(self, p: int, h: float) -> np.ndarray:
+        x = self.pos[p, :3].astype(np.float64)
+        near = np.array(self.qtree.query_ball_point(x, self.R + 2 * h), dtype=np.int64)
+        if near.size == 0:
+            return near
+        dist = np.sqrt(((self.q[near, :3].astype(np.float64) - x) ** 2).sum(1))
+        has_p = (self.idx1[near] == p).any(1)
+        could_enter = dist - 2 * h < self.rk[near]
+        return near[has_p | could_enter]
+
+    def _central(self, p: int, qsel, base_rows, a: int, h: float):
+        """Central difference along axis a with step h, or None if the
+        neighbour sets change inside [-h, +h]."""
+        xp, xm = self.pos[p, :3].copy(), self.pos[p, :3].copy()
+        xp[a] = np.float32(float(self.pos[p, a]) + h)
+        xm[a] = np.float32(float(self.pos[p, a]) - h)
+        rp, cp = self._rows(qsel, p, xp)
+        rm, cm = self._rows(qsel, p, xm)
+        if not (np.array_equal(rp, base_rows) and np.array_equal(rm, base_rows)):
+            return None
+        pp, pm = self.pos.copy(), self.pos.copy()
+        pp[p, :3], pm[p, :3] = xp, xm
+        lp, lm = self._loss(qsel, rp, cp, pp), self._loss(qsel, rm, cm, pm)
+        return (lp - lm) / (float(xp[a]) - float(xm[a]))   # the FP32-rounded step actually taken
+
+    def position(self, photons, h: float = 1e-4) -> FDResult:
+        """dL/dx_p by FP64 central differences with step h and h/2, combined by
+        Richardson extrapolation (4 D(h/2) - D(h)) / 3 (fourth order); plain
+        D(h) is kept in .plain."""
+        out = np.full((len(photons), 3), np.nan)
+        plain = np.full((len(photons), 3), np.nan)
+        excl = np.zeros((len(photons), 3), bool)
+        for s, p in enumerate(photons):
+            p = int(p)
+            qsel = self._affected(p, h)
+            if qsel.size == 0:
+                out[s] = plain[s] = 0.0
+                continue
+            base_rows, _ = self._rows(qsel, p, self.pos[p, :3])
+            for a in range(3):
+                d1 = self._central(p, qsel, base_rows, a, h)
+                d2 = self._central(p, qsel, base_rows, a, h / 2) if d1 is not None else None
+                if d1 is None or d2 is None:
+                    excl[s, a] = True
+                    continue
+                plain[s, a] = d1
+                out[s, a] = (4.0 * d2 - d1) / 3.0
+        r = FDResult(out, excl, int(excl.sum()))
+        r.plain = plain
+        return r
+
+    def power(self, photons, h: float = 1e-4) -> np.ndarray:
+        """d L / d Phi_p by central differences (the sets do not depend on power)."""
+        out = np.zeros((len(photons), 3))
+        for s, p in enumerate(photons):
+            qsel = self._affected(int(p), 0.0)
+            if qsel.size == 0:
+                continue
+            rows, cnt = self._rows(qsel, int(p), self.pos[p, :3])
+            for c in range(3):
+                keep = self.pw.copy()
+                scale = max(abs(float(keep[p, c])), 1e-12)
+                dh = h * scale
+                self.pw = keep.copy()
+                self.pw[p, c] = keep[p, c] + dh
+                up = float(self.pw[p, c])
+                lp = self._loss(qsel, rows, cnt, self.pos)
+                self.pw[p, c] = keep[p, c] - dh
+                dn = float(self.pw[p, c])
+                lm = self._loss(qsel, rows, cnt, self.pos)
+                self.pw = keep
+                out[s, c] = (lp - lm) / (up - dn)
+        return out

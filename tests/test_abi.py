@@ -103,3 +103,16 @@ def test_allocator_failure_is_reported(engine_lib):
 def test_status_strings(engine_lib):
     for s in (0, -1, -2, -3, -4, -5, -6):
         assert engine_lib.pm_status_string(s)
+
+
+def test_backward_validation_without_gpu(engine_lib):
+    lib = engine_lib
+    h = _create(lib)
+    d = L.QueryDesc(k=10, r_max=0.1, filter=L.PM_FILTER_EPANECHNIKOV, cone_k=1.0, mode=0, min_found=0, order=0,
+                    refine_iters=2)
+    assert lib.pm_query_backward(h, C.byref(d), None, None, 0, None, None, None, None, 16, 16, None) == L.PM_ERR_STATE
+    dz = L.QueryDesc(**{**{f: getattr(d, f) for f, _ in L.QueryDesc._fields_}, "mode": L.PM_MODE_ZHOU_COMPAT})
+    assert lib.pm_query_backward(h, C.byref(dz), None, None, 0, None, None, None, None, 16, 16, None) == L.PM_ERR_INVALID
+    assert lib.pm_set_backward_chunk(h, 1000) == L.PM_OK
+    assert lib.pm_set_backward_chunk(None, 1000) == L.PM_ERR_INVALID
+    lib.pm_destroy(h)
