@@ -330,6 +330,106 @@ def run_ours(args, cfg) -> dict | None:
     return result
 
 
+def run_diff(args, cfg) -> dict:
+    """Differentiation workload: forward (build + query with neighbour lists)
+    and adjoint (dL/dpower, dL/dposition) of L = sum |E - T|^2, T from powers
+    scaled by seeded U[0.5, 1.5]; then gradient descent on the powers."""
+    import torch
+    from mnrt_b200.photon_map import PhotonMap
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    ph, q = make_inputs(cfg, 0)
+    N, Q, k, R, filt = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"], cfg["filter"]
+    rng = np.random.default_rng(4242)
+    tpow = ph.pow.copy()
+    tpow[:, :3] *= rng.uniform(0.5, 1.5, size=(N, 3)).astype(np.float32)
+    d_pos, d_pow = torch.from_numpy(ph.pos).to(dev), torch.from_numpy(ph.pow).to(dev)
+    d_tpow = torch.from_numpy(tpow).to(dev)
+    d_qpos, d_qnrm = torch.from_numpy(q.pos).to(dev), torch.from_numpy(q.nrm).to(dev)
+    pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
+    pm.reserve(N, Q)
+    kw = dict(k=k, r_max=R, filter=filt)
+    pm.build(d_pos, d_tpow)
+    target = pm.query(d_qpos, d_qnrm, **kw)["rad"][:, :3].clone()
+    out = {"rad": torch.empty((Q, 4), dtype=torch.float32, device=dev),
+           "nbr": torch.empty((Q, k), dtype=torch.int32, device=dev),
+           "count": torch.empty((Q,), dtype=torch.int32, device=dev)}
+    out_plain = {"rad": torch.empty((Q, 4), dtype=torch.float32, device=dev)}
+    g = torch.zeros((Q, 4), dtype=torch.float32, device=dev)
+    gpow = torch.empty((N, 4), dtype=torch.float32, device=dev)
+    gpos = torch.empty((N, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def fwd(o):
+        pm.build(d_pos, d_pow)
+        pm.query(d_qpos, d_qnrm, out=o, **kw)
+
+    def bwd():
+        g[:, :3] = 2.0 * (out["rad"][:, :3] - target)
+        pm.query_backward(d_qpos, d_qnrm, g, nbr=out["nbr"], count=out["count"], grad_pow=gpow, grad_pos=gpos, **kw)
+
+    for _ in range(args.warmup):
+        fwd(out_plain); fwd(out); bwd()
+    t_fwd, t_bwd = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
+        flush.zero_()
+        ev[0].record(); fwd(out); ev[2].record(); bwd(); ev[3].record(); ev[3].synchronize()
+        t_fwd.append(ev[0].elapsed_time(ev[2]))
+        t_bwd.append(ev[2].elapsed_time(ev[3]))
+    # forward without neighbour lists, timed on its own
+    plain = []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
+        plain.append(ev[0].elapsed_time(ev[1]))
+    fwd_ms, bwd_ms, plain_ms = float(np.mean(t_fwd)), float(np.mean(t_bwd)), float(np.mean(plain))
+
+    # gradient descent on the powers; E is linear in them, so the step along
+    # -dL/dpower is the exact line-search minimiser alpha = |grad|^2 / |A grad|^2
+    steps = args.gd_steps
+    losses = []
+    pw = d_pow.clone()
+    dirp = torch.zeros_like(pw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in range(steps + 1):
+        pm.build(d_pos, pw)
+        pm.query(d_qpos, d_qnrm, out=out, **kw)
+        res = out["rad"][:, :3] - target
+        losses.append(float((res.double() ** 2).sum()))
+        if it == steps:
+            break
+        g[:, :3] = 2.0 * res
+        pm.query_backward(d_qpos, d_qnrm, g, nbr=out["nbr"], count=out["count"], grad_pow=gpow, want_pos=False, **kw)
+        dirp[:, :3] = gpow[:, :3]
+        dirp[:, 3] = pw[:, 3]                       # direction bits ride along
+        pm.build(d_pos, dirp)
+        ag = pm.query(d_qpos, d_qnrm, out=out_plain, **kw)["rad"][:, :3].double()
+        num = float((gpow[:, :3].double() ** 2).sum())
+        den = 2.0 * float((ag ** 2).sum())
+        alpha = num / den if den > 0 else 0.0
+        pw[:, :3] -= float(alpha) * gpow[:, :3]
+    torch.cuda.synchronize()
+    gd_s = time.perf_counter() - t0
+    pm.close()
+    return {
+        "metric": "forward + adjoint time of the radiance estimate (differentiation workload)",
+        "value": fwd_ms + bwd_ms, "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "dtype": "f32 (adjoint sums in f64)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R, "filter": filt,
+                   "l2": "flushed between steps (256 MiB write, untimed)"},
+        "forward_ms": fwd_ms, "forward_no_lists_ms": plain_ms, "backward_ms": bwd_ms,
+        "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms, "fwd_bwd_over_fwd_no_lists": (fwd_ms + bwd_ms) / plain_ms,
+        "gradient_descent": {"steps": steps, "loss_first": losses[0], "loss_last": losses[-1],
+                             "loss_ratio": losses[-1] / losses[0] if losses[0] > 0 else None,
+                             "seconds": gd_s, "line_search": "exact (E is linear in the powers)"},
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,6 +439,7 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff"])
     ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gd-steps", type=int, default=200, help="gradient-descent steps of the diff workload")
     ap.add_argument("--leaf", type=int, default=0)
     ap.add_argument("--wpb", type=int, default=0)
     ap.add_argument("--rounds", type=int, default=0)
@@ -352,6 +453,9 @@ def main(argv=None) -> int:
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
         print(json.dumps(run_reference(args, cfg)), flush=True)
+        return 0
+    if args.config == "diff":
+        print(json.dumps(run_diff(args, cfg)), flush=True)
         return 0
     res = run_ours(args, cfg)
     if res is not None:

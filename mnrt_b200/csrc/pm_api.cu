@@ -216,6 +216,7 @@ QueryTuning tuning_of(const pm_map* m) {
 QueryParams params_of(const pm_query_desc* d) {
     QueryParams p;
     p.k = d->k;
+    p.r = d->r_max;
     p.r2 = d->r_max * d->r_max;
     p.filter = d->filter;
     p.cone_k = d->filter == PM_FILTER_CONE ? d->cone_k : 1.0f;

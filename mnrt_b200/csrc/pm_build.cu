@@ -83,16 +83,37 @@ __global__ void __launch_bounds__(kBoundsThreads) k_bounds(const float4* __restr
         s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (!s_last || threadIdx.x != 0) return;
+    if (!s_last) return;
+    // last block: all threads reduce the block partials, strided
     __threadfence();
     float r[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, 0.0f};
     uint32_t rb = 0;
-    for (uint32_t b = 0; b < gridDim.x; ++b) {
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
         const float* q = partials + 8 * b;
         for (int a = 0; a < 3; ++a) { r[a] = fminf(r[a], __ldcg(q + a)); r[a + 3] = fmaxf(r[a + 3], __ldcg(q + a + 3)); }
         r[6] = fmaxf(r[6], __ldcg(q + 6));
         rb |= __float_as_uint(__ldcg(q + 7));
     }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { r[a] = warp_min(r[a]); r[a + 3] = warp_max(r[a + 3]); }
+    r[6] = warp_max(r[6]);
+    rb = __any_sync(0xffffffffu, rb != 0) ? 1u : 0u;
+    __syncthreads();   // s_v is reused
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 7; ++a) s_v[warp][a] = r[a];
+        s_v[warp][7] = __uint_as_float(rb);
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < kBoundsThreads / 32; ++w) {
+        for (int a = 0; a < 3; ++a) { s_v[0][a] = fminf(s_v[0][a], s_v[w][a]); s_v[0][a + 3] = fmaxf(s_v[0][a + 3], s_v[w][a + 3]); }
+        s_v[0][6] = fmaxf(s_v[0][6], s_v[w][6]);
+        s_v[0][7] = __uint_as_float(__float_as_uint(s_v[0][7]) | __float_as_uint(s_v[w][7]));
+    }
+    for (int a = 0; a < 3; ++a) { r[a] = s_v[0][a]; r[a + 3] = s_v[0][a + 3]; }
+    r[6] = s_v[0][6];
+    rb = __float_as_uint(s_v[0][7]);
     for (int a = 0; a < 3; ++a) { hdr->lo[a] = r[a]; hdr->hi[a] = r[a + 3]; }
     hdr->max_power = r[6];
     hdr->fix_scale = (r[6] > 0.0f) ? __fdiv_rn(1099511627776.0f, r[6]) : 0.0f;   // 2^40 / max

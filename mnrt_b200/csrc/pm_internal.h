@@ -58,6 +58,7 @@ void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream
 // pm_query.cu
 struct QueryParams {
     uint32_t k;
+    float r;             // R
     float r2;            // R^2 rounded in FP32
     int filter;
     float cone_k;

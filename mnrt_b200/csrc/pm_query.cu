@@ -39,6 +39,7 @@ struct KnnArgs {
     uint32_t nq;
     uint32_t k;
     float r2max;
+    float rmax;
     int filter;
     float cone_k;
     uint32_t min_found;
@@ -97,22 +98,45 @@ __device__ __forceinline__ void heap_sift_down(uint64_t* h, uint32_t n, uint64_t
     h[i * 32] = v;
 }
 
-// Per-query factor of the filter weight: 1 / (k_c r) for the cone, 1 / r^2
-// for Epanechnikov (the weights only enter the FP64-checked estimate, they
-// are not part of the exact neighbour contract).
-__device__ __forceinline__ float filter_factor(int filter, float r2, float cone_k) {
-    if (filter == 1) return __frcp_rn(__fmul_rn(cone_k, __fsqrt_rn(r2)));
-    if (filter == 2) return __frcp_rn(r2);
-    return 0.0f;
+// The estimate's arithmetic after the neighbour set is fixed runs in FP64,
+// as the oracle's: weights from FP64 distances to the query, r^2 = FP64 d^2 of
+// the k-th neighbour (or R^2).  Explicit roundings keep every kernel on the
+// same bits.  The FP32 contract decides only the set, the front test and the
+// reported r^2.
+__device__ __forceinline__ double d2_64(double qx, double qy, double qz, const float4& p) {
+    const double dx = __dsub_rn((double)p.x, qx), dy = __dsub_rn((double)p.y, qy), dz = __dsub_rn((double)p.z, qz);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-__device__ __forceinline__ float filter_weight(int filter, float d2, float inv) {
-    if (filter == 1) {
-        const float d = d2 > 0.0f ? __fmul_rn(d2, rsqrtf(d2)) : 0.0f;
-        return fmaxf(__fsub_rn(1.0f, __fmul_rn(d, inv)), 0.0f);
+struct Filter64 {
+    int filter;
+    double qx, qy, qz;
+    double inv;   // 1 / (k_c r) for the cone, 1 / r^2 for Epanechnikov
+    __device__ __forceinline__ void init(int f, float cone_k, float x, float y, float z, double r2) {
+        filter = f;
+        qx = x; qy = y; qz = z;
+        if (f == 1) inv = __drcp_rn(__dmul_rn((double)cone_k, __dsqrt_rn(r2)));
+        else if (f == 2) inv = __drcp_rn(r2);
+        else inv = 0.0;
     }
-    if (filter == 2) return fmaxf(__fsub_rn(1.0f, __fmul_rn(d2, inv)), 0.0f);
-    return 1.0f;
+    __device__ __forceinline__ double weight(const float4& p) const {
+        if (filter == 0) return 1.0;
+        const double d2 = d2_64(qx, qy, qz, p);
+        if (filter == 1) return __dsub_rn(1.0, __dmul_rn(__dsqrt_rn(d2), inv));
+        return __dsub_rn(1.0, __dmul_rn(d2, inv));
+    }
+};
+
+// r^2 of the filter: FP64 d^2 of the k-th neighbour (tree position kth) when k
+// were found, else R^2.
+__device__ __forceinline__ double filter_r2(const float4* __restrict__ pos, bool full, uint32_t kth, float qx, float qy,
+                                            float qz, float rmax) {
+    if (!full) return __dmul_rn((double)rmax, (double)rmax);
+    return d2_64(qx, qy, qz, __ldg(pos + kth));
+}
+
+__device__ __forceinline__ long long fixed_term(double w, float phi, float scale) {
+    return __double2ll_rn(__dmul_rn(__dmul_rn(w, (double)phi), (double)scale));
 }
 
 __device__ __forceinline__ double filter_norm(int filter, double r2, double cone_k) {
@@ -125,10 +149,11 @@ __device__ __forceinline__ double filter_norm(int filter, double r2, double cone
 // Epilogue for one lane: fixed-point filtered flux sum over the heap, optional
 // sorted neighbour list.  Shared by the tree and the brute-force kernels.
 // stride: distance between consecutive heap elements of this lane.
-__device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uint32_t hn, uint32_t qo, float nx,
-                             float ny, float nz) {
+__device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uint32_t hn, uint32_t qo, float qx,
+                             float qy, float qz, float nx, float ny, float nz) {
     const uint32_t k = a.k;
     const float r2 = (hn == k) ? __uint_as_float((uint32_t)(h[0] >> 32)) : a.r2max;
+    const uint32_t kth = (uint32_t)h[0];   // tree position of the k-th (heap top) when hn == k
     if (a.out_nbr) {   // heapsort in place -> ascending (d^2, index)
         for (uint32_t end = hn; end > 1; --end) {
             const uint64_t top = h[0];
@@ -157,22 +182,23 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
             row[j] = (j < hn) ? __float_as_uint(a.pos[(uint32_t)h[j * stride]].w) : kInvalid;
     }
     float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)hn);
-    if (hn >= a.min_found && r2 > 0.0f) {
+    const double r2d = filter_r2(a.pos, hn == k, kth, qx, qy, qz, a.rmax);
+    if (hn > 0 && hn >= a.min_found && r2d > 0.0) {
         const float scale = a.hdr->fix_scale;
-        const float inv = filter_factor(a.filter, r2, a.cone_k);
+        Filter64 flt;
+        flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
         long long acc0 = 0, acc1 = 0, acc2 = 0;
         for (uint32_t j = 0; j < hn; ++j) {
-            const uint64_t key = h[j * stride];
-            const float4 w = a.pow[(uint32_t)key];
+            const uint32_t t = (uint32_t)h[j * stride];
+            const float4 w = a.pow[t];
             if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
-            const float d2 = __uint_as_float((uint32_t)(key >> 32));
-            const float wt = filter_weight(a.filter, d2, inv);
-            acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
-            acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
-            acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
+            const double wt = flt.weight(__ldg(a.pos + t));
+            acc0 += fixed_term(wt, w.x, scale);
+            acc1 += fixed_term(wt, w.y, scale);
+            acc2 += fixed_term(wt, w.z, scale);
         }
         if (scale > 0.0f) {
-            const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
+            const double f = filter_norm(a.filter, r2d, (double)a.cone_k) / (double)scale;
             rad.x = __double2float_rn((double)acc0 * f);
             rad.y = __double2float_rn((double)acc1 * f);
             rad.z = __double2float_rn((double)acc2 * f);
@@ -340,7 +366,7 @@ __global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
             const float rk2 = (active && full) ? __uint_as_float((uint32_t)(heap[0] >> 32)) : 0.0f;
             if (inrange) {
                 if (active) {
-                    finish_query(a, heap, 32, hn, qo, nx, ny, nz);
+                    finish_query(a, heap, 32, hn, qo, qx, qy, qz, nx, ny, nz);
                 } else {
                     a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (a.out_r2) a.out_r2[qo] = r2max;
@@ -523,38 +549,51 @@ __device__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32
 // returns the r^2 used by the filter.
 template <int G>
 __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, uint32_t s,
-                              uint32_t gmask, uint32_t lt, uint32_t qo, float nx, float ny, float nz) {
+                              uint32_t gmask, uint32_t lt, uint32_t qo, float qx, float qy, float qz, float nx,
+                              float ny, float nz) {
     const uint32_t k = a.k;
+    if (n > k) group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
     float rk2 = a.r2max;
-    if (n > k) {
-        const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
-        rk2 = __uint_as_float((uint32_t)(T >> 32));
-    } else if (n == k) {
-        uint32_t mx = 0;
-        for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
-        rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
+    uint32_t kth = 0;   // tree position of the k-th neighbour (n == k)
+    if (n == k) {       // the largest exact key (d^2, caller index), carried with its tree position
+        uint64_t best = 0;   // exact key + 1; 0 = no entry in this lane
+        uint32_t bpos = 0;
+        for (uint32_t e = s; e < n; e += G) {
+            const uint64_t v = buf[e];
+            const uint64_t x = exact_key(v, a.pos) + 1ull;
+            if (x > best) { best = x; bpos = (uint32_t)v; }
+        }
+#pragma unroll
+        for (int o = G / 2; o; o >>= 1) {
+            const uint64_t ob = __shfl_xor_sync(gmask, best, o);
+            const uint32_t op = __shfl_xor_sync(gmask, bpos, o);
+            if (ob > best) { best = ob; bpos = op; }
+        }
+        rk2 = __uint_as_float((uint32_t)((best - 1ull) >> 32));
+        kth = bpos;
     }
-    const float r2 = (n == k) ? rk2 : a.r2max;
+    const float r2 = rk2;
     float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
-    if (n >= a.min_found && r2 > 0.0f) {
+    const double r2d = filter_r2(a.pos, n == k, kth, qx, qy, qz, a.rmax);
+    if (n > 0 && n >= a.min_found && r2d > 0.0) {
         const float scale = a.hdr->fix_scale;
-        const float inv = filter_factor(a.filter, r2, a.cone_k);
+        Filter64 flt;
+        flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
         long long acc0 = 0, acc1 = 0, acc2 = 0;
         for (uint32_t e = s; e < n; e += G) {
-            const uint64_t key = buf[e];
-            const float4 w = a.pow[(uint32_t)key];
+            const uint32_t t = (uint32_t)buf[e];
+            const float4 w = a.pow[t];
             if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
-            const float d2 = __uint_as_float((uint32_t)(key >> 32));
-            const float wt = filter_weight(a.filter, d2, inv);
-            acc0 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.x), scale));
-            acc1 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.y), scale));
-            acc2 += __float2ll_rn(__fmul_rn(__fmul_rn(wt, w.z), scale));
+            const double wt = flt.weight(__ldg(a.pos + t));
+            acc0 += fixed_term(wt, w.x, scale);
+            acc1 += fixed_term(wt, w.y, scale);
+            acc2 += fixed_term(wt, w.z, scale);
         }
         acc0 = gsum_i64<G>(acc0, gmask);
         acc1 = gsum_i64<G>(acc1, gmask);
         acc2 = gsum_i64<G>(acc2, gmask);
         if (scale > 0.0f) {
-            const double f = filter_norm(a.filter, (double)r2, (double)a.cone_k) / (double)scale;
+            const double f = filter_norm(a.filter, r2d, (double)a.cone_k) / (double)scale;
             rad.x = __double2float_rn((double)acc0 * f);
             rad.y = __double2float_rn((double)acc1 * f);
             rad.z = __double2float_rn((double)acc2 * f);
@@ -756,7 +795,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 atomicAdd(a.stats + kStatPhotons, (unsigned long long)st_photons);
             }
             if (active) {
-                const float r2 = group_finish<G>(a, buf, n, hist, s, gmask, lt, qo, nx, ny, nz);
+                const float r2 = group_finish<G>(a, buf, n, hist, s, gmask, lt, qo, qx, qy, qz, nx, ny, nz);
                 rk2 = r2;
             } else if (inrange && s == 0) {
                 a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -834,7 +873,7 @@ __global__ void __launch_bounds__(kBruteThreads) k_knn_brute(KnnArgs a, uint32_t
             }
         }
     }
-    if (valid) finish_query(a, heap, kBruteThreads, hn, q, nx, ny, nz);
+    if (valid) finish_query(a, heap, kBruteThreads, hn, q, qx, qy, qz, nx, ny, nz);
 }
 
 __global__ void k_query_morton(const float4* __restrict__ qpos, uint32_t nq, const MapHeader* __restrict__ hdr,
@@ -865,7 +904,7 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     KnnArgs a;
     a.pos = m.pos; a.pow = m.pow; a.nodes = m.nodes; a.hdr = m.hdr;
     a.qpos = qpos; a.qnrm = qnrm; a.order = order; a.nq = nq;
-    a.k = p.k; a.r2max = p.r2; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
+    a.k = p.k; a.r2max = p.r2; a.rmax = p.r; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
     a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
     a.work_counter = nullptr; a.rounds_per_chunk = 1;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;

@@ -9,8 +9,11 @@ that set is evaluated in FP64 (the oracle's radiance_fp64).  Moving one
 photon p changes only the queries whose set contains p or could gain p, and
 their new set is the k nearest among their old k + 1 nearest plus p, so each
 finite difference re-evaluates a few hundred queries exactly instead of the
-whole map.  A sample whose neighbour set (or k-th neighbour) changes inside
-[-h, +h] sits on a kink of L and is excluded; the count is reported.
+whole map.  The loss is evaluated in FP64 with the moved photon at an FP64
+position (exact +-h steps); the neighbour sets are decided on the positions
+rounded to FP32, as the engine sees them.  A sample whose neighbour set (or
+k-th neighbour) changes inside [-h, +h] sits on a kink of L and is excluded;
+the count is reported.
 """
 from __future__ import annotations
 
@@ -18,6 +21,8 @@ from dataclasses import dataclass
 
 import numpy as np
 from scipy.spatial import cKDTree
+
+from tests.np_restate import front
 
 
 def _d2_f32(q: np.ndarray, p: np.ndarray) -> np.ndarray:
@@ -73,11 +78,48 @@ class LossFD:
         cnt = np.minimum(ok.sum(1), k)
         return rows, cnt
 
-    def _loss(self, qsel, rows, cnt, pos):
-        nbr = np.where(rows >= 0, rows, 0).astype(np.uint32)
-        e = self.o.radiance_fp64(pos, self.pw, self.q[qsel], self.n[qsel], nbr, cnt.astype(np.uint32), self.k,
-                                 self.R, self.filt, self.cone_k, self.min_found)
+    def _loss(self, qsel, rows, cnt, p: int = -1, xp=None):
+        """FP64 loss of the queries qsel over fixed neighbour rows, with photon
+        p at the FP64 position xp (None: where it is)."""
+        k = self.k
+        valid = rows >= 0
+        safe = np.where(valid, rows, 0)
+        pts = self.pos[safe, :3].astype(np.float64)
+        if xp is not None:
+            pts[rows == p] = np.asarray(xp, np.float64)
+        dv = pts - self.q[qsel, None, :3].astype(np.float64)
+        d2 = (dv * dv).sum(-1)
+        last = np.take_along_axis(d2, np.maximum(cnt - 1, 0)[:, None], axis=1)[:, 0]
+        R2 = float(np.float64(np.float32(self.R))) ** 2
+        r2 = np.where(cnt == k, last, R2)
+        alive = (cnt > 0) & (cnt >= self.min_found) & (r2 > 0)
+        r2s = np.where(alive, r2, 1.0)[:, None]
+        if self.filt == "cone":
+            w = 1.0 - np.sqrt(d2) / (self.cone_k * np.sqrt(r2s))
+            norm = 1.0 / ((1.0 - 2.0 / (3.0 * self.cone_k)) * np.pi * r2s)
+        elif self.filt == "epanechnikov":
+            w = 1.0 - d2 / r2s
+            norm = 2.0 / (np.pi * r2s)
+        else:
+            w = np.ones_like(d2)
+            norm = 1.0 / (np.pi * r2s)
+        nrm = np.repeat(self.n[qsel], rows.shape[1], axis=0)
+        fr = front(nrm, self.pw[safe.ravel(), 3].view(np.uint32)).reshape(rows.shape)
+        wt = np.where(valid & fr, w, 0.0)
+        e = (wt[..., None] * self.pw[safe, :3].astype(np.float64)).sum(1) * norm
+        e = np.where(alive[:, None], e, 0.0)
         return float(((e - self.t[qsel]) ** 2).sum())
+
+    @staticmethod
+    def _same_set(a, b, cnt_a, cnt_b, k):
+        """Same neighbour sets and the same k-th neighbour (order inside a set
+        does not move the estimate)."""
+        if not np.array_equal(cnt_a, cnt_b):
+            return False
+        if not np.array_equal(np.sort(a, axis=1), np.sort(b, axis=1)):
+            return False
+        full = cnt_a == k
+        return np.array_equal(a[full, k - 1], b[full, k - 1])
 
     def _affected(self, p: int, h: float) -> np.ndarray:
         x = self.pos[p, :3].astype(np.float64)
@@ -89,20 +131,22 @@ class LossFD:
         could_enter = dist - 2 * h < self.rk[near]
         return near[has_p | could_enter]
 
-    def _central(self, p: int, qsel, base_rows, a: int, h: float):
-        """Central difference along axis a with step h, or None if the
-        neighbour sets change inside [-h, +h]."""
-        xp, xm = self.pos[p, :3].copy(), self.pos[p, :3].copy()
-        xp[a] = np.float32(float(self.pos[p, a]) + h)
-        xm[a] = np.float32(float(self.pos[p, a]) - h)
-        rp, cp = self._rows(qsel, p, xp)
-        rm, cm = self._rows(qsel, p, xm)
-        if not (np.array_equal(rp, base_rows) and np.array_equal(rm, base_rows)):
-            return None
-        pp, pm = self.pos.copy(), self.pos.copy()
-        pp[p, :3], pm[p, :3] = xp, xm
-        lp, lm = self._loss(qsel, rp, cp, pp), self._loss(qsel, rm, cm, pm)
-        return (lp - lm) / (float(xp[a]) - float(xm[a]))   # the FP32-rounded step actually taken
+    def _central(self, p: int, qsel, base, a: int, h: float):
+        """FP64 central difference along axis a with step h, or None if a
+        neighbour set (or k-th neighbour) changes inside [-h, +h]; the sets are
+        decided on the FP32-rounded positions, as the engine would see them."""
+        rows0, cnt0 = base
+        x = self.pos[p, :3].astype(np.float64)
+        for sgn in (1.0, -1.0, 0.5, -0.5):
+            y = x.copy()
+            y[a] += sgn * h
+            r, c = self._rows(qsel, p, y.astype(np.float32))
+            if not self._same_set(r, rows0, c, cnt0, self.k):
+                return None
+        xp, xm = x.copy(), x.copy()
+        xp[a] += h
+        xm[a] -= h
+        return (self._loss(qsel, rows0, cnt0, p, xp) - self._loss(qsel, rows0, cnt0, p, xm)) / (2.0 * h)
 
     def position(self, photons, h: float = 1e-4) -> FDResult:
         """dL/dx_p by FP64 central differences with step h and h/2, combined by
@@ -117,10 +161,10 @@ class LossFD:
             if qsel.size == 0:
                 out[s] = plain[s] = 0.0
                 continue
-            base_rows, _ = self._rows(qsel, p, self.pos[p, :3])
+            base = self._rows(qsel, p, self.pos[p, :3])
             for a in range(3):
-                d1 = self._central(p, qsel, base_rows, a, h)
-                d2 = self._central(p, qsel, base_rows, a, h / 2) if d1 is not None else None
+                d1 = self._central(p, qsel, base, a, h)
+                d2 = self._central(p, qsel, base, a, h / 2) if d1 is not None else None
                 if d1 is None or d2 is None:
                     excl[s, a] = True
                     continue
@@ -145,10 +189,10 @@ class LossFD:
                 self.pw = keep.copy()
                 self.pw[p, c] = keep[p, c] + dh
                 up = float(self.pw[p, c])
-                lp = self._loss(qsel, rows, cnt, self.pos)
+                lp = self._loss(qsel, rows, cnt)
                 self.pw[p, c] = keep[p, c] - dh
                 dn = float(self.pw[p, c])
-                lm = self._loss(qsel, rows, cnt, self.pos)
+                lm = self._loss(qsel, rows, cnt)
                 self.pw = keep
                 out[s, c] = (lp - lm) / (up - dn)
         return out
