@@ -165,8 +165,9 @@ PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, con
  * bit, as pm_query on a built map.
  *   - The map must already be built.  The caller passes every input and
  *     output buffer, as for pm_query.
- *   - The query scratch (Morton sort keys and the work counter) lives in one
- *     fixed array of about 6.2 MiB inside this library.  Every GPU that loads
+ *   - The query scratch (Morton sort keys, the list of queries re-evaluated
+ *     with FP64 distances, the work counters) lives in one fixed array of
+ *     about 7.2 MiB inside this library.  Every GPU that loads
  *     the library holds it until the process exits.
  *   - nq > PM_NOALLOC_MAX_QUERIES is rejected with PM_ERR_INVALID; split
  *     larger query sets into several calls.

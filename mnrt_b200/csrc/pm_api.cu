@@ -12,7 +12,7 @@
 #include <new>
 
 #include "pm_internal.h"
-#include "../../include/pmgpu.h"
+#include "pmgpu.h"
 
 using namespace pm;
 
@@ -45,7 +45,7 @@ struct pm_map {
     DevBuf pos, pow, inv, nodes, hdr;
     DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
     // query-sized
-    DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter;
+    DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter, fixq;
     DevBuf stats;           // query counters (profiling level 2)
     // backward (pm_query_backward): pair sort, per-query records, segments,
     // FP64 running sums, and the forward outputs when the kNN is recomputed
@@ -168,6 +168,7 @@ pm_status ensure_query_capacity(pm_map* m, uint32_t nq, cudaStream_t st) {
     ENSURE(qvals1, cap * sizeof(uint32_t));
     ENSURE(qscratch, sort_words((uint32_t)cap) * sizeof(uint32_t));
     ENSURE(counter, 64 * sizeof(uint32_t));
+    ENSURE(fixq, cap * sizeof(uint32_t));
 #undef ENSURE
     m->cap_queries = (uint32_t)cap;
     return PM_OK;
@@ -275,7 +276,7 @@ pm_status pm_destroy(pm_map* m) {
     DevBuf* all[] = {&m->pos, &m->pow, &m->inv, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
-                     &m->qscratch, &m->counter, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
+                     &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad};
     for (DevBuf* b : all) buf_free(m, *b);
@@ -389,7 +390,7 @@ pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, c
     if (prof) cudaEventRecord(m->ev[4], st);
     QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
     nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
-                    P<uint32_t>(m->counter), tuning_of(m), st);
+                    P<uint32_t>(m->counter), P<uint32_t>(m->fixq), tuning_of(m), st);
     if (prof) cudaEventRecord(m->ev[5], st);
     m->have_query_ev = prof;
     m->query_launches = (uint32_t)nl;
@@ -515,7 +516,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
                 QueryTuning t = tuning_of(m);
                 t.stats = nullptr;
                 nl += query_knn(view_of(m), params_of(desc), qp, a.qnrm + q0, order, nqc, out, P<uint32_t>(m->counter),
-                                t, st);
+                                P<uint32_t>(m->fixq), t, st);
             }
             a.nbr = P<uint32_t>(m->rnbr);
             a.count_in = P<uint32_t>(m->rcnt);
@@ -658,14 +659,15 @@ pm_status pm_export_tree(pm_map* m, uint32_t* host_nodes, uint32_t max_nodes, fl
 // host applications hand the engine a fixed memory budget up front and let
 // nothing grow afterwards.  This entry point runs the same kernels as
 // pm_query, but the scratch they need beyond the caller's inputs and outputs
-// (query Morton keys, radix-sort histograms, the work counter) is carved from
+// (query Morton keys, radix-sort histograms, the list of queries re-evaluated
+// with FP64 distances, the work counters) is carved from
 // one file-scope device array of a fixed size.  The map itself must already
 // be built.  Nothing here calls cudaMalloc, cudaFree or any allocating
 // library routine.
 //
 // The array is shared by every call on every handle.  Each call rewrites all
-// of it that it reads (the keys, the histograms) and query_knn clears the
-// work counter on the stream before the kernel starts, so one call's leftovers
+// of it that it reads (the keys, the histograms, the fix list) and query_knn
+// clears the counters on the stream before the kernel starts, so one call's leftovers
 // never leak into the next; calls that overlap on the GPU race.
 namespace {
 
@@ -678,7 +680,8 @@ constexpr size_t kNoallocKeys1 = kNoallocKeys0 + noalloc_round((size_t)kNoallocM
 constexpr size_t kNoallocVals0 = kNoallocKeys1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint64_t));
 constexpr size_t kNoallocVals1 = kNoallocVals0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
 constexpr size_t kNoallocSort = kNoallocVals1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
-constexpr size_t kNoallocCounter = kNoallocSort + noalloc_round(kNoallocSortWords * sizeof(uint32_t));
+constexpr size_t kNoallocFix = kNoallocSort + noalloc_round(kNoallocSortWords * sizeof(uint32_t));
+constexpr size_t kNoallocCounter = kNoallocFix + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
 constexpr size_t kNoallocBytes = kNoallocCounter + kNoallocAlign;
 
 // In host code this name is only a host-side handle for the runtime: its
@@ -746,7 +749,8 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
     t.stats = nullptr;
     QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
     nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
-                    reinterpret_cast<uint32_t*>(base + kNoallocCounter), t, st);
+                    reinterpret_cast<uint32_t*>(base + kNoallocCounter), reinterpret_cast<uint32_t*>(base + kNoallocFix),
+                    t, st);
     m->launches += (uint64_t)nl;
     return check_cuda(m, "pm_query_noalloc");
 }

@@ -82,7 +82,7 @@ struct QueryTuning {
     unsigned long long* stats;   // 8 traversal counters (group layout), nullptr = off
 };
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
-              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
+              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list,
               const QueryTuning& t, cudaStream_t st);
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);

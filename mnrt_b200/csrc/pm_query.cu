@@ -48,6 +48,9 @@ struct KnnArgs {
     float* out_r2;
     uint32_t* out_count;
     uint32_t* work_counter;
+    uint32_t* fix_list;       // group kernel: queries whose estimate needs FP64 distances
+    uint32_t* fix_count;
+    const uint32_t* nq_dev;   // fix pass: query count read on the device
     uint32_t rounds_per_chunk;
     uint32_t cap;             // group kernel: candidate buffer entries per query
     uint32_t smem_per_warp;   // group kernel: shared bytes per warp
@@ -108,22 +111,38 @@ __device__ __forceinline__ double d2_64(double qx, double qy, double qz, const f
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
+// Filter weight of one neighbour, relative error about 1e-7 however close
+// the neighbour is to the edge of the ball: the cancelling difference
+// delta = (k_c r)^2 - d^2 (cone) or r^2 - d^2 (Epanechnikov) is formed in FP64
+// from FP64 distances, the rest in FP32.
+//   cone:          w = 1 - d / (k_c r) = delta / (k_c r (k_c r + d))
+//   Epanechnikov:  w = 1 - d^2 / r^2   = delta / r^2
 struct Filter64 {
     int filter;
     double qx, qy, qz;
-    double inv;   // 1 / (k_c r) for the cone, 1 / r^2 for Epanechnikov
+    double edge2;   // (k_c r)^2 (cone) or r^2 (Epanechnikov), FP64
+    float edge;     // k_c r (cone)
+    float inv;      // 1 / r^2 (Epanechnikov)
     __device__ __forceinline__ void init(int f, float cone_k, float x, float y, float z, double r2) {
         filter = f;
         qx = x; qy = y; qz = z;
-        if (f == 1) inv = __drcp_rn(__dmul_rn((double)cone_k, __dsqrt_rn(r2)));
-        else if (f == 2) inv = __drcp_rn(r2);
-        else inv = 0.0;
+        edge2 = 0.0; edge = 0.0f; inv = 0.0f;
+        if (f == 1) {
+            const double e = __dmul_rn((double)cone_k, __dsqrt_rn(r2));
+            edge2 = __dmul_rn(e, e);
+            edge = __double2float_rn(e);
+        } else if (f == 2) {
+            edge2 = r2;
+            inv = __double2float_rn(__drcp_rn(r2));
+        }
     }
-    __device__ __forceinline__ double weight(const float4& p) const {
-        if (filter == 0) return 1.0;
+    __device__ __forceinline__ float weight(const float4& p) const {
+        if (filter == 0) return 1.0f;
         const double d2 = d2_64(qx, qy, qz, p);
-        if (filter == 1) return __dsub_rn(1.0, __dmul_rn(__dsqrt_rn(d2), inv));
-        return __dsub_rn(1.0, __dmul_rn(d2, inv));
+        const float delta = __double2float_rn(__dsub_rn(edge2, d2));
+        if (filter == 2) return __fmul_rn(delta, inv);
+        const float d = __fsqrt_rn(__double2float_rn(d2));
+        return __fdiv_rn(delta, __fmul_rn(edge, __fadd_rn(edge, d)));
     }
 };
 
@@ -135,15 +154,92 @@ __device__ __forceinline__ double filter_r2(const float4* __restrict__ pos, bool
     return d2_64(qx, qy, qz, __ldg(pos + kth));
 }
 
-__device__ __forceinline__ long long fixed_term(double w, float phi, float scale) {
-    return __double2ll_rn(__dmul_rn(__dmul_rn(w, (double)phi), (double)scale));
-}
-
 __device__ __forceinline__ double filter_norm(int filter, double r2, double cone_k) {
     const double pi = 3.14159265358979323846;
     if (filter == 1) return 1.0 / ((1.0 - 2.0 / (3.0 * cone_k)) * pi * r2);
     if (filter == 2) return 2.0 / (pi * r2);
     return 1.0 / (pi * r2);
+}
+
+__device__ __forceinline__ long long fixed_term(float w, float phi, float scale) {
+    return __float2ll_rn(__fmul_rn(__fmul_rn(w, phi), scale));
+}
+
+// FP32 filter weights (the common path).  Their absolute error is below
+// about 8e-7 (FP32 d^2 against FP64, the reciprocal square root, r), so the
+// estimate's relative error is below 8e-7 * sum(flux) / sum(w * flux) plus
+// about 3e-7 from r^2: the FP32 path is kept when sum(w * flux) is at least
+// sum(flux) / 6 (bound 5.1e-6), decided on the fixed-point sums (identical in
+// every kernel), and the query is re-evaluated with FP64 distances otherwise.
+__device__ __forceinline__ float filter_inv32(int filter, float r2, float cone_k) {
+    if (filter == 1) return __frcp_rn(__fmul_rn(cone_k, __fsqrt_rn(r2)));
+    if (filter == 2) return __frcp_rn(r2);
+    return 0.0f;
+}
+
+__device__ __forceinline__ float filter_weight32(int filter, float d2, float inv) {
+    if (filter == 1) {
+        const float d = d2 > 0.0f ? __fmul_rn(d2, rsqrtf(d2)) : 0.0f;
+        return fmaxf(__fsub_rn(1.0f, __fmul_rn(d, inv)), 0.0f);
+    }
+    if (filter == 2) return fmaxf(__fsub_rn(1.0f, __fmul_rn(d2, inv)), 0.0f);
+    return 1.0f;
+}
+
+struct EstAcc {
+    long long c0, c1, c2;   // weighted flux, fixed point
+    long long f;            // unweighted flux (all channels), fixed point
+};
+
+__device__ __forceinline__ void est_add32(const KnnArgs& a, uint32_t t, float d2, float inv, float nx, float ny,
+                                          float nz, float scale, EstAcc& acc) {
+    const float4 w = __ldg(a.pow + t);
+    if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) return;
+    const float wt = filter_weight32(a.filter, d2, inv);
+    acc.c0 += fixed_term(wt, w.x, scale);
+    acc.c1 += fixed_term(wt, w.y, scale);
+    acc.c2 += fixed_term(wt, w.z, scale);
+    acc.f += fixed_term(1.0f, __fadd_rn(__fadd_rn(w.x, w.y), w.z), scale);
+}
+
+__device__ __forceinline__ void est_add64(const KnnArgs& a, uint32_t t, const Filter64& flt, float nx, float ny,
+                                          float nz, float scale, EstAcc& acc) {
+    const float4 w = __ldg(a.pow + t);
+    if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) return;
+    const float wt = flt.weight(__ldg(a.pos + t));
+    acc.c0 += fixed_term(wt, w.x, scale);
+    acc.c1 += fixed_term(wt, w.y, scale);
+    acc.c2 += fixed_term(wt, w.z, scale);
+}
+
+__device__ __forceinline__ bool est_needs_fp64(int filter, const EstAcc& acc) {
+    return filter != 0 && 6 * (acc.c0 + acc.c1 + acc.c2) < acc.f;
+}
+
+__device__ __forceinline__ float4 est_result(const EstAcc& acc, int filter, double r2, float cone_k, float scale,
+                                             uint32_t n) {
+    float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)n);
+    if (scale > 0.0f) {
+        const double f = filter_norm(filter, r2, (double)cone_k) / (double)scale;
+        rad.x = __double2float_rn((double)acc.c0 * f);
+        rad.y = __double2float_rn((double)acc.c1 * f);
+        rad.z = __double2float_rn((double)acc.c2 * f);
+    }
+    return rad;
+}
+
+
+// The FP64 re-evaluation of one query (rare path).  Returns r^2 in FP64.
+__device__ __forceinline__ double est_fp64_heap(const KnnArgs& a, const uint64_t* h, uint32_t stride, uint32_t hn,
+                                             bool full, uint32_t kth, float qx, float qy, float qz, float nx, float ny,
+                                             float nz, EstAcc& acc) {
+    const double r2d = filter_r2(a.pos, full, kth, qx, qy, qz, a.rmax);
+    const float scale = a.hdr->fix_scale;
+    Filter64 flt;
+    flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
+    acc = EstAcc{0, 0, 0, 0};
+    for (uint32_t j = 0; j < hn; ++j) est_add64(a, (uint32_t)h[j * stride], flt, nx, ny, nz, scale, acc);
+    return r2d;
 }
 
 // Epilogue for one lane: fixed-point filtered flux sum over the heap, optional
@@ -182,27 +278,17 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
             row[j] = (j < hn) ? __float_as_uint(a.pos[(uint32_t)h[j * stride]].w) : kInvalid;
     }
     float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)hn);
-    const double r2d = filter_r2(a.pos, hn == k, kth, qx, qy, qz, a.rmax);
-    if (hn > 0 && hn >= a.min_found && r2d > 0.0) {
+    if (hn > 0 && hn >= a.min_found && r2 > 0.0f) {
         const float scale = a.hdr->fix_scale;
-        Filter64 flt;
-        flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
-        long long acc0 = 0, acc1 = 0, acc2 = 0;
+        const float inv = filter_inv32(a.filter, r2, a.cone_k);
+        EstAcc acc = {0, 0, 0, 0};
         for (uint32_t j = 0; j < hn; ++j) {
-            const uint32_t t = (uint32_t)h[j * stride];
-            const float4 w = a.pow[t];
-            if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
-            const double wt = flt.weight(__ldg(a.pos + t));
-            acc0 += fixed_term(wt, w.x, scale);
-            acc1 += fixed_term(wt, w.y, scale);
-            acc2 += fixed_term(wt, w.z, scale);
+            const uint64_t key = h[j * stride];
+            est_add32(a, (uint32_t)key, __uint_as_float((uint32_t)(key >> 32)), inv, nx, ny, nz, scale, acc);
         }
-        if (scale > 0.0f) {
-            const double f = filter_norm(a.filter, r2d, (double)a.cone_k) / (double)scale;
-            rad.x = __double2float_rn((double)acc0 * f);
-            rad.y = __double2float_rn((double)acc1 * f);
-            rad.z = __double2float_rn((double)acc2 * f);
-        }
+        double r2d = (double)r2;
+        if (est_needs_fp64(a.filter, acc)) r2d = est_fp64_heap(a, h, stride, hn, hn == k, kth, qx, qy, qz, nx, ny, nz, acc);
+        rad = est_result(acc, a.filter, r2d, a.cone_k, scale, hn);
     }
     a.out_rad[qo] = rad;
     if (a.out_r2) a.out_r2[qo] = r2;
@@ -547,57 +633,84 @@ __device__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32
 // Final selection and outputs for one query held by a group of G lanes:
 // keeps the k nearest, writes radiance / r^2 / count / sorted neighbours and
 // returns the r^2 used by the filter.
+// Tree position of the k-th neighbour (the largest exact key (d^2, caller
+// index)) of a full group buffer; caller indices are read only for entries
+// that share the largest d^2.
 template <int G>
+__device__ uint32_t group_kth(const KnnArgs& a, const uint64_t* buf, uint32_t n, uint32_t s, uint32_t gmask) {
+    uint32_t mx = 0;
+    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+    mx = gmax_u32<G>(mx, gmask);
+    uint64_t best = 0;   // exact key + 1; 0 = no entry with the largest d^2 in this lane
+    uint32_t bpos = 0;
+    for (uint32_t e = s; e < n; e += G) {
+        const uint64_t v = buf[e];
+        if ((uint32_t)(v >> 32) != mx) continue;
+        const uint64_t x = exact_key(v, a.pos) + 1ull;
+        if (x > best) { best = x; bpos = (uint32_t)v; }
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+        const uint64_t ob = __shfl_xor_sync(gmask, best, o);
+        const uint32_t op = __shfl_xor_sync(gmask, bpos, o);
+        if (ob > best) { best = ob; bpos = op; }
+    }
+    return bpos;
+}
+
+template <int G>
+__device__ __forceinline__ double est_fp64_group(const KnnArgs& a, const uint64_t* buf, uint32_t n, uint32_t s,
+                                              uint32_t gmask, float qx, float qy, float qz, float nx, float ny,
+                                              float nz, EstAcc& acc) {
+    const bool full = n == a.k;
+    const uint32_t kth = full ? group_kth<G>(a, buf, n, s, gmask) : 0u;
+    const double r2d = filter_r2(a.pos, full, kth, qx, qy, qz, a.rmax);
+    const float scale = a.hdr->fix_scale;
+    Filter64 flt;
+    flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
+    acc = EstAcc{0, 0, 0, 0};
+    for (uint32_t e = s; e < n; e += G) est_add64(a, (uint32_t)buf[e], flt, nx, ny, nz, scale, acc);
+    acc.c0 = gsum_i64<G>(acc.c0, gmask);
+    acc.c1 = gsum_i64<G>(acc.c1, gmask);
+    acc.c2 = gsum_i64<G>(acc.c2, gmask);
+    return r2d;
+}
+
+template <int G, bool kFix>
 __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, uint32_t s,
                               uint32_t gmask, uint32_t lt, uint32_t qo, float qx, float qy, float qz, float nx,
                               float ny, float nz) {
     const uint32_t k = a.k;
     if (n > k) group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
     float rk2 = a.r2max;
-    uint32_t kth = 0;   // tree position of the k-th neighbour (n == k)
-    if (n == k) {       // the largest exact key (d^2, caller index), carried with its tree position
-        uint64_t best = 0;   // exact key + 1; 0 = no entry in this lane
-        uint32_t bpos = 0;
-        for (uint32_t e = s; e < n; e += G) {
-            const uint64_t v = buf[e];
-            const uint64_t x = exact_key(v, a.pos) + 1ull;
-            if (x > best) { best = x; bpos = (uint32_t)v; }
-        }
-#pragma unroll
-        for (int o = G / 2; o; o >>= 1) {
-            const uint64_t ob = __shfl_xor_sync(gmask, best, o);
-            const uint32_t op = __shfl_xor_sync(gmask, bpos, o);
-            if (ob > best) { best = ob; bpos = op; }
-        }
-        rk2 = __uint_as_float((uint32_t)((best - 1ull) >> 32));
-        kth = bpos;
+    if (n == k) {
+        uint32_t mx = 0;
+        for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+        rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
     }
     const float r2 = rk2;
     float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
-    const double r2d = filter_r2(a.pos, n == k, kth, qx, qy, qz, a.rmax);
-    if (n > 0 && n >= a.min_found && r2d > 0.0) {
+    if (n > 0 && n >= a.min_found && r2 > 0.0f) {
         const float scale = a.hdr->fix_scale;
-        Filter64 flt;
-        flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
-        long long acc0 = 0, acc1 = 0, acc2 = 0;
+        const float inv = filter_inv32(a.filter, r2, a.cone_k);
+        EstAcc acc = {0, 0, 0, 0};
         for (uint32_t e = s; e < n; e += G) {
-            const uint32_t t = (uint32_t)buf[e];
-            const float4 w = a.pow[t];
-            if (!front_rn(nx, ny, nz, __float_as_uint(w.w))) continue;
-            const double wt = flt.weight(__ldg(a.pos + t));
-            acc0 += fixed_term(wt, w.x, scale);
-            acc1 += fixed_term(wt, w.y, scale);
-            acc2 += fixed_term(wt, w.z, scale);
+            const uint64_t key = buf[e];
+            est_add32(a, (uint32_t)key, __uint_as_float((uint32_t)(key >> 32)), inv, nx, ny, nz, scale, acc);
         }
-        acc0 = gsum_i64<G>(acc0, gmask);
-        acc1 = gsum_i64<G>(acc1, gmask);
-        acc2 = gsum_i64<G>(acc2, gmask);
-        if (scale > 0.0f) {
-            const double f = filter_norm(a.filter, r2d, (double)a.cone_k) / (double)scale;
-            rad.x = __double2float_rn((double)acc0 * f);
-            rad.y = __double2float_rn((double)acc1 * f);
-            rad.z = __double2float_rn((double)acc2 * f);
+        acc.c0 = gsum_i64<G>(acc.c0, gmask);
+        acc.c1 = gsum_i64<G>(acc.c1, gmask);
+        acc.c2 = gsum_i64<G>(acc.c2, gmask);
+        acc.f = gsum_i64<G>(acc.f, gmask);
+        double r2d = (double)r2;
+        if (est_needs_fp64(a.filter, acc)) {
+            if (kFix) {
+                r2d = est_fp64_group<G>(a, buf, n, s, gmask, qx, qy, qz, nx, ny, nz, acc);
+            } else if (s == 0) {   // re-evaluated by the fix pass (the FP32 result written below is replaced)
+                a.fix_list[atomicAdd(a.fix_count, 1u)] = qo;
+            }
         }
+        rad = est_result(acc, a.filter, r2d, a.cone_k, scale, n);
     }
     if (s == 0) {
         a.out_rad[qo] = rad;
@@ -621,7 +734,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
     return r2;
 }
 
-template <int G>
+template <int G, bool kFix>
 __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
     constexpr int QW = 32 / G;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -638,7 +751,8 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
     uint32_t* stack = reinterpret_cast<uint32_t*>(wb + (size_t)QW * (C * sizeof(uint64_t) + 256 * sizeof(uint32_t)));
     const float r2max = a.r2max;
     const uint32_t chunk_q = a.rounds_per_chunk * QW;
-    const uint32_t nchunks = (a.nq + chunk_q - 1) / chunk_q;
+    const uint32_t nq = kFix ? *a.nq_dev : a.nq;
+    const uint32_t nchunks = (nq + chunk_q - 1) / chunk_q;
 
     for (;;) {
         uint32_t chunk = 0;
@@ -649,7 +763,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
         bool pvalid = false;
         for (uint32_t round = 0; round < a.rounds_per_chunk; ++round) {
             const uint32_t slot_q = chunk * chunk_q + round * QW + g;
-            const bool inrange = slot_q < a.nq;
+            const bool inrange = slot_q < nq;
             if (!__any_sync(kFull, inrange)) break;
             uint32_t qo = 0;
             float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
@@ -795,7 +909,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 atomicAdd(a.stats + kStatPhotons, (unsigned long long)st_photons);
             }
             if (active) {
-                const float r2 = group_finish<G>(a, buf, n, hist, s, gmask, lt, qo, qx, qy, qz, nx, ny, nz);
+                const float r2 = group_finish<G, kFix>(a, buf, n, hist, s, gmask, lt, qo, qx, qy, qz, nx, ny, nz);
                 rk2 = r2;
             } else if (inrange && s == 0) {
                 a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -907,6 +1021,7 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.k = p.k; a.r2max = p.r2; a.rmax = p.r; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
     a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
     a.work_counter = nullptr; a.rounds_per_chunk = 1;
+    a.fix_list = nullptr; a.fix_count = nullptr; a.nq_dev = nullptr;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
     return a;
 }
@@ -932,7 +1047,7 @@ static uint32_t grid_for(K kernel, int threads, int smem, uint32_t work_items, i
 }
 
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
-              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter,
+              const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list,
               const QueryTuning& t, cudaStream_t st) {
     if (!nq) return 0;
     KnnArgs a = make_args(m, p, qpos, qnrm, order, nq, out);
@@ -941,7 +1056,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
     if (t.stats) cudaMemsetAsync(t.stats, 0, kStatCount * sizeof(unsigned long long), st);
     a.rounds_per_chunk = (uint32_t)t.rounds_per_chunk;
     const int threads = 32 * t.warps_per_block;
-    cudaMemsetAsync(work_counter, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(work_counter, 0, 3 * sizeof(uint32_t), st);   // work, fix count, fix work
     if (t.layout == 0) {   // one lane per query, shared-memory heap
         const int smem = query_smem_bytes_per_warp(p.k) * t.warps_per_block;
         const uint32_t nchunks = (nq + 32u * a.rounds_per_chunk - 1) / (32u * a.rounds_per_chunk);
@@ -954,10 +1069,19 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
     a.smem_per_warp = (uint32_t)group_smem_bytes_per_warp(p.k, qpw);
     const int smem = (int)a.smem_per_warp * t.warps_per_block;
     const uint32_t nchunks = (nq + (uint32_t)qpw * a.rounds_per_chunk - 1) / ((uint32_t)qpw * a.rounds_per_chunk);
-#define PM_LAUNCH_GROUP(G)                                                                 \
-    {                                                                                      \
-        const uint32_t grid = grid_for(k_knn_group<G>, threads, smem, nchunks, t.warps_per_block); \
-        k_knn_group<G><<<grid, threads, smem, st>>>(a);                                    \
+    a.fix_list = fix_list;
+    a.fix_count = work_counter + 1;
+    a.nq_dev = nullptr;
+    KnnArgs fx = a;   // fix pass: the listed queries, FP64 distances where needed
+    fx.order = fix_list;
+    fx.nq_dev = work_counter + 1;
+    fx.work_counter = work_counter + 2;
+#define PM_LAUNCH_GROUP(G)                                                                          \
+    {                                                                                               \
+        const uint32_t grid = grid_for(k_knn_group<G, false>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, false><<<grid, threads, smem, st>>>(a);                                      \
+        const uint32_t gfix = grid_for(k_knn_group<G, true>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, true><<<gfix, threads, smem, st>>>(fx);                                      \
     }
     switch (qpw) {
         case 1: PM_LAUNCH_GROUP(32) break;
@@ -966,7 +1090,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         default: PM_LAUNCH_GROUP(4) break;
     }
 #undef PM_LAUNCH_GROUP
-    return 1;
+    return 2;
 }
 
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
