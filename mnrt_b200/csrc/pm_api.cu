@@ -51,6 +51,7 @@ struct pm_map {
     // FP64 running sums, and the forward outputs when the kNN is recomputed
     DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, qr2, qcnt, seg_start, seg_end, acc;
     DevBuf rnbr, rcnt, rr2, rrad;
+    DevBuf gnrm, gest;        // pm_gather_for: flipped normals, estimates
     uint64_t cap_pairs = 0;
     uint32_t cap_bq = 0, cap_bn = 0, cap_rq = 0;
     uint32_t bwd_chunk = 0;   // max queries per backward chunk (0 = automatic)
@@ -278,7 +279,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
-                     &m->rcnt, &m->rr2, &m->rrad};
+                     &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -535,9 +536,43 @@ pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit
                         const float* d_ray_dir4, const float* d_ray_origin4, const float* d_ray_influence4,
                         const float* d_clr_diffuse4, const uint32_t* d_idx_shading, uint32_t n, float* d_io_radiance4,
                         float* d_io_recip_dist, void* stream) {
-    (void)desc; (void)d_hit_pos4; (void)d_hit_nrm4; (void)d_ray_dir4; (void)d_ray_origin4; (void)d_ray_influence4;
-    (void)d_clr_diffuse4; (void)d_idx_shading; (void)n; (void)d_io_radiance4; (void)d_io_recip_dist; (void)stream;
-    return fail(m, PM_ERR_UNSUPPORTED, "pm_gather_for is not available in this build");
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = validate_desc(m, desc, true);
+    if (s != PM_OK) return s;
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (n > 0 && (!d_hit_pos4 || !d_hit_nrm4 || !d_ray_dir4 || !d_ray_influence4 || !d_io_radiance4))
+        return fail(m, PM_ERR_INVALID, "hit positions, normals, ray directions, influences and radiance must be non-NULL");
+    if (n > 0 && d_io_recip_dist && !d_ray_origin4)
+        return fail(m, PM_ERR_INVALID, "ray origins are needed for the reciprocal-distance accumulator");
+    const void* f4[] = {d_hit_pos4, d_hit_nrm4, d_ray_dir4, d_ray_origin4, d_ray_influence4, d_clr_diffuse4, d_io_radiance4};
+    for (const void* p : f4)
+        if (p && !aligned16(p)) return fail(m, PM_ERR_INVALID, "float4 arrays must be 16-byte aligned");
+    if (n == 0 || m->n == 0) return PM_OK;   // nothing to gather (PhotonMap.cpp:239-240)
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    s = ensure_query_capacity(m, n, st);
+    if (s != PM_OK) return s;
+    if (m->gnrm.bytes < (size_t)n * sizeof(float4) || m->gest.bytes < (size_t)n * sizeof(float4)) {
+        if (capturing(st)) return fail(m, PM_ERR_STATE, "gather storage must grow during stream capture");
+        if ((s = buf_ensure(m, m->gnrm, (size_t)n * sizeof(float4), "gnrm")) != PM_OK) return s;
+        if ((s = buf_ensure(m, m->gest, (size_t)n * sizeof(float4), "gest")) != PM_OK) return s;
+    }
+    const float4* hit = reinterpret_cast<const float4*>(d_hit_pos4);
+    int nl = gather_normals(reinterpret_cast<const float4*>(d_hit_nrm4), reinterpret_cast<const float4*>(d_ray_dir4), n,
+                            P<float4>(m->gnrm), st);
+    const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, hit, n, st, &nl) : nullptr;
+    QueryParams qp = params_of(desc);
+    if (!d_clr_diffuse4) qp.min_found = 0;   // photon visualisation keeps every estimate (GPU/photon_knn.cu:515-519)
+    QueryOutputs out{P<float4>(m->gest), nullptr, nullptr, nullptr};
+    QueryTuning t = tuning_of(m);
+    t.stats = nullptr;
+    nl += query_knn(view_of(m), qp, hit, P<float4>(m->gnrm), order, n, out, P<uint32_t>(m->counter),
+                    P<uint32_t>(m->fixq), t, st);
+    nl += gather_accumulate(P<float4>(m->gest), hit, reinterpret_cast<const float4*>(d_ray_origin4),
+                            reinterpret_cast<const float4*>(d_ray_influence4),
+                            reinterpret_cast<const float4*>(d_clr_diffuse4), d_idx_shading, n,
+                            reinterpret_cast<float4*>(d_io_radiance4), d_io_recip_dist, st);
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_gather_for");
 }
 
 pm_status pm_scale_flux(pm_map* m, float scale, void* stream) {

@@ -88,6 +88,12 @@ int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);
 int query_smem_bytes_per_warp(uint32_t k);
 
+// pm_gather.cu
+int gather_normals(const float4* hit_nrm, const float4* ray_dir, uint32_t n, float4* out_nrm, cudaStream_t st);
+int gather_accumulate(const float4* est, const float4* hit_pos, const float4* ray_origin, const float4* influence,
+                      const float4* clr_diffuse, const uint32_t* idx_shading, uint32_t n, float4* io_rad,
+                      float* io_recip, cudaStream_t st);
+
 // pm_backward.cu
 struct BwdArgs {
     const float4* pos;        // tree order

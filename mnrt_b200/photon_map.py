@@ -221,3 +221,34 @@ class PhotonMap:
 
     def set_backward_chunk(self, max_queries: int) -> None:
         L.check(self._lib.pm_set_backward_chunk(self._h, int(max_queries)), self._h)
+
+    # -- reference gather entry points ------------------------------------------------
+    def gather_for(self, sp: ShadingPoints, rays: RayChunk, clr_diff_hit: torch.Tensor | None,
+                   idx_shading_pts: torch.Tensor | None, io_radiance: torch.Tensor,
+                   io_recip_dist: torch.Tensor | None = None, stream=None, **kw) -> None:
+        """PhotonMap::GatherFor (PhotonMap.cpp:234-270): estimate at the gather
+        hits (normal flipped toward the incoming ray) and accumulate
+        clr.w * clr.rgb / pi * E * influence into io_radiance[idx] (and
+        rsqrt(|hit - origin|^2) into io_recip_dist[idx]).  Defaults follow the
+        reference: k = the map's kNN target count, R = its global radius,
+        box filter, estimates from fewer than 8 photons zeroed."""
+        kw.setdefault("filter", "box")
+        kw.setdefault("min_found", 8)
+        d = self.desc(**kw)
+        n = int(sp.pt_inter.shape[0])
+        L.check(self._lib.pm_gather_for(self._h, C.byref(d), _ptr(sp.pt_inter), _ptr(sp.normals_s), _ptr(rays.dirs),
+                                        _ptr(rays.origins), _ptr(rays.influences), _ptr(clr_diff_hit),
+                                        _ptr(idx_shading_pts), n, _ptr(io_radiance), _ptr(io_recip_dist),
+                                        _stream(stream)), self._h)
+
+    def gather(self, sp: ShadingPoints, rays: RayChunk, clr_diff_hit: torch.Tensor, io_radiance: torch.Tensor,
+               stream=None, **kw) -> None:
+        """PhotonMap::Gather (PhotonMap.cpp:195-232): GatherFor with the
+        shading points themselves as targets and no distance accumulator."""
+        self.gather_for(sp, rays, clr_diff_hit, None, io_radiance, None, stream=stream, **kw)
+
+    def visualize(self, sp: ShadingPoints, rays: RayChunk, io_radiance: torch.Tensor, stream=None) -> None:
+        """PhotonMap::Visualize (PhotonMap.cpp:272-285): the nearest photon
+        within 5 % of the global radius, white, no photon-count rule."""
+        self.gather_for(sp, rays, None, None, io_radiance, None, stream=stream, k=1, r_max=0.05 * self.r_max,
+                        min_found=0)
