@@ -227,6 +227,43 @@ PM_API pm_status pm_scale_flux(pm_map* map, float scale, void* stream);
 PM_API pm_status pm_compute_query_radii(pm_map* map, const pm_query_desc* desc, const float* d_qpos4, uint32_t nq,
                                  float* d_radii, void* stream);
 
+/* ---- Batches of photon maps (no counterpart in the reference, which builds
+ * and gathers one map per call).  Many maps of uneven size are built by one
+ * sort and one tree, and queried by one persistent launch over a work queue
+ * of all maps' queries; pm_batch_capture records both in a CUDA graph.
+ *   Photons of map i: elements [photon_offsets[i], photon_offsets[i+1]) of
+ *   d_pos4 / d_pow4 (host array of num_maps + 1 entries, starting at 0).
+ *   Queries of map i: elements [query_offsets[i], query_offsets[i+1]) of
+ *   d_qpos4 / d_qnrm4, answered with descs[i] (exact mode; k, r_max, filter,
+ *   min_found per map).  d_rad4, d_r2, d_count are indexed like the queries;
+ *   the neighbour rows of map i (k_i entries each, photon indices local to
+ *   map i) start at entry sum_{j<i} q_j k_j of d_nbr.
+ * Results are identical, bit for bit, to building and querying every map on
+ * its own with pm_build / pm_query.  At most 65,536 maps and 2^31 - 1
+ * photons per batch.  Batch queries always use one query per warp. */
+typedef struct pm_batch pm_batch;
+PM_API pm_status pm_batch_create(pm_batch** out);
+PM_API pm_status pm_batch_destroy(pm_batch* batch);
+/* Photons per leaf, warps per query block and query rounds per work chunk. */
+PM_API pm_status pm_batch_set_tuning(pm_batch* batch, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk);
+PM_API pm_status pm_batch_build(pm_batch* batch, const float* d_pos4, const float* d_pow4,
+                                const uint32_t* photon_offsets, uint32_t num_maps, int format, void* stream);
+PM_API pm_status pm_batch_query(pm_batch* batch, const pm_query_desc* descs, const float* d_qpos4,
+                                const float* d_qnrm4, const uint32_t* query_offsets, float* d_rad4, uint32_t* d_nbr,
+                                float* d_r2, uint32_t* d_count, void* stream);
+/* Records build + query with these arguments into a CUDA graph kept by the
+ * handle (tables are uploaded and storage sized first; synchronous).
+ * pm_batch_launch replays it on any stream: the graph reads the same device
+ * buffers each time, so new photon and query values in them are picked up. */
+PM_API pm_status pm_batch_capture(pm_batch* batch, const float* d_pos4, const float* d_pow4,
+                                  const uint32_t* photon_offsets, uint32_t num_maps, int format,
+                                  const pm_query_desc* descs, const float* d_qpos4, const float* d_qnrm4,
+                                  const uint32_t* query_offsets, float* d_rad4, uint32_t* d_nbr, float* d_r2,
+                                  uint32_t* d_count);
+PM_API pm_status pm_batch_launch(pm_batch* batch, void* stream);
+PM_API pm_status pm_batch_get_info(pm_batch* batch, pm_map_info* info, void* stream);
+PM_API const char* pm_batch_last_error(const pm_batch* batch);
+
 /* Phase timing with CUDA events recorded on the call's stream (off by
  * default).  pm_last_timings waits for the last recorded events. */
 typedef struct pm_timings {

@@ -69,6 +69,15 @@ SIGNATURES = {
     "pm_query_stats": (_I, [_VP, _VP, _U32]),
     "pm_clear_errors": (_I, [_VP, _VP]),
     "pm_export_tree": (_I, [_VP, _VP, _U32, _VP, _VP, _U32]),
+    "pm_batch_create": (_I, [C.POINTER(C.c_void_p)]),
+    "pm_batch_destroy": (_I, [_VP]),
+    "pm_batch_set_tuning": (_I, [_VP, _U32, _I, _I]),
+    "pm_batch_build": (_I, [_VP, _FP, _FP, _VP, _U32, _I, _VP]),
+    "pm_batch_query": (_I, [_VP, _VP, _FP, _FP, _VP, _FP, _UP, _FP, _UP, _VP]),
+    "pm_batch_capture": (_I, [_VP, _FP, _FP, _VP, _U32, _I, _VP, _FP, _FP, _VP, _FP, _UP, _FP, _UP]),
+    "pm_batch_launch": (_I, [_VP, _VP]),
+    "pm_batch_get_info": (_I, [_VP, C.POINTER(MapInfo), _VP]),
+    "pm_batch_last_error": (C.c_char_p, [_VP]),
     "pm_last_error": (C.c_char_p, [_VP]),
     "pm_status_string": (C.c_char_p, [_I]),
     "pm_abi_version": (_I, []),

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "pm_internal.h"
 #include "pmgpu.h"
@@ -789,3 +790,291 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
     m->launches += (uint64_t)nl;
     return check_cuda(m, "pm_query_noalloc");
 }
+
+// ---------------------------------------------------------------------------
+// Batches of photon maps (no counterpart in the reference, which builds and
+// gathers one map per call).  A batch owns one pm_map for its combined
+// storage plus the per-map tables; see pm_batch.cu for the device side.
+struct pm_batch {
+    pm_map* m = nullptr;
+    uint32_t num_maps = 0;
+    uint32_t total_photons = 0;
+    bool built = false;
+    int format = PM_PHOTONS_PACKED;
+    DevBuf ph_off, q_off, bq, geom, acc;
+    uint32_t cap_maps = 0;
+    std::vector<uint32_t> h_ph_off;   // host copy of the built photon offsets
+    // CUDA graph of build + query
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t query_launches = 0;
+};
+
+namespace {
+
+pm_status batch_fail(pm_batch* b, pm_status s, const char* msg) {
+    if (b && b->m) fail(b->m, s, "%s", msg);
+    return s;
+}
+
+pm_status batch_tables(pm_batch* b, uint32_t maps) {
+    if (maps <= b->cap_maps && b->ph_off.ptr) return PM_OK;
+    pm_map* m = b->m;
+    pm_status s;
+    if ((s = buf_ensure(m, b->ph_off, (maps + 1) * sizeof(uint32_t), "batch photon offsets")) != PM_OK) return s;
+    if ((s = buf_ensure(m, b->q_off, (maps + 1) * sizeof(uint32_t), "batch query offsets")) != PM_OK) return s;
+    if ((s = buf_ensure(m, b->bq, maps * sizeof(BatchQuery), "batch query table")) != PM_OK) return s;
+    if ((s = buf_ensure(m, b->geom, maps * sizeof(BatchGeom), "batch geometry")) != PM_OK) return s;
+    if ((s = buf_ensure(m, b->acc, maps * 8 * sizeof(uint32_t), "batch bounds")) != PM_OK) return s;
+    b->cap_maps = maps;
+    return PM_OK;
+}
+
+// Validates and uploads the photon offsets (synchronously: tables are small
+// and this runs outside any capture).
+pm_status batch_upload_photons(pm_batch* b, const uint32_t* offsets, uint32_t maps) {
+    if (!offsets) return batch_fail(b, PM_ERR_INVALID, "photon offsets are NULL");
+    if (maps == 0 || maps > 65536) return batch_fail(b, PM_ERR_INVALID, "a batch holds 1 to 65536 maps");
+    if (offsets[0] != 0) return batch_fail(b, PM_ERR_INVALID, "photon offsets must start at 0");
+    for (uint32_t i = 0; i < maps; ++i)
+        if (offsets[i + 1] < offsets[i]) return batch_fail(b, PM_ERR_INVALID, "photon offsets must not decrease");
+    if (offsets[maps] > 0x7fffffffu) return batch_fail(b, PM_ERR_UNSUPPORTED, "more than 2^31 - 1 photons in a batch");
+    pm_status s = batch_tables(b, maps);
+    if (s != PM_OK) return s;
+    if (cudaMemcpy(b->ph_off.ptr, offsets, (maps + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        return check_cuda(b->m, "batch photon offsets");
+    b->h_ph_off.assign(offsets, offsets + maps + 1);
+    return PM_OK;
+}
+
+pm_status batch_upload_queries(pm_batch* b, const pm_query_desc* descs, const uint32_t* offsets, uint32_t* kmax_out,
+                               uint64_t* nbr_total) {
+    const uint32_t maps = b->num_maps;
+    if (!descs || !offsets) return batch_fail(b, PM_ERR_INVALID, "query descriptors or offsets are NULL");
+    if (offsets[0] != 0) return batch_fail(b, PM_ERR_INVALID, "query offsets must start at 0");
+    std::vector<BatchQuery> t(maps);
+    uint32_t kmax = 1;
+    uint64_t nbr = 0;
+    for (uint32_t i = 0; i < maps; ++i) {
+        pm_status s = validate_desc(b->m, &descs[i], true);
+        if (s != PM_OK) return s;
+        if (offsets[i + 1] < offsets[i]) return batch_fail(b, PM_ERR_INVALID, "query offsets must not decrease");
+        BatchQuery& q = t[i];
+        q.q_off = offsets[i];
+        q.q_n = offsets[i + 1] - offsets[i];
+        q.ph_off = b->h_ph_off[i];
+        q.ph_n = b->h_ph_off[i + 1] - b->h_ph_off[i];
+        q.nbr_off = nbr;
+        q.k = descs[i].k;
+        q.min_found = descs[i].min_found;
+        q.rmax = descs[i].r_max;
+        q.r2max = descs[i].r_max * descs[i].r_max;
+        q.filter = descs[i].filter;
+        q.cone_k = descs[i].filter == PM_FILTER_CONE ? descs[i].cone_k : 1.0f;
+        nbr += (uint64_t)q.q_n * q.k;
+        kmax = q.k > kmax ? q.k : kmax;
+    }
+    if (cudaMemcpy(b->bq.ptr, t.data(), maps * sizeof(BatchQuery), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->q_off.ptr, offsets, (maps + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        return check_cuda(b->m, "batch query tables");
+    *kmax_out = kmax;
+    *nbr_total = nbr;
+    return PM_OK;
+}
+
+// The device work of a batch build (tables already uploaded, storage sized).
+pm_status batch_build_device(pm_batch* b, const float* d_pos4, const float* d_pow4, int format, cudaStream_t st) {
+    pm_map* m = b->m;
+    const uint32_t n = b->total_photons, maps = b->num_maps;
+    BuildBuffers bb;
+    bb.keys[0] = P<uint64_t>(m->keys0); bb.keys[1] = P<uint64_t>(m->keys1);
+    bb.vals[0] = P<uint32_t>(m->vals0); bb.vals[1] = P<uint32_t>(m->vals1);
+    bb.scratch = P<uint32_t>(m->scratch);
+    bb.kfirst = P<uint32_t>(m->kfirst); bb.klast = P<uint32_t>(m->klast); bb.ksplit = P<uint32_t>(m->ksplit);
+    bb.kkeep = P<uint32_t>(m->kkeep); bb.krank = P<uint32_t>(m->krank);
+    bb.parent = P<uint32_t>(m->parent); bb.arrive = P<uint32_t>(m->arrive); bb.nleaf = P<uint32_t>(m->nleaf);
+    bb.partials = P<uint32_t>(m->partials); bb.num_partials = 1184;
+    const float4* pos = reinterpret_cast<const float4*>(d_pos4);
+    const float4* pw = reinterpret_cast<const float4*>(d_pow4);
+    int nl = batch_bounds_and_keys(pos, pw, P<uint32_t>(b->ph_off), maps, n, P<uint32_t>(b->acc),
+                                   P<BatchGeom>(b->geom), P<MapHeader>(m->hdr), bb.keys[0], bb.vals[0], st);
+    uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
+    uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
+    const int cur = n > 1 ? radix_sort_pairs(keys, vals, n, 48 + map_id_bits(maps), bb.scratch, st, &nl) : 0;
+    nl += build_from_sorted(pos, pw, n, format, m->leaf_size, keys[cur], vals[cur], P<float4>(m->pos),
+                            P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes), P<MapHeader>(m->hdr), bb, st);
+    nl += batch_roots(P<uint32_t>(b->ph_off), maps, n, m->leaf_size, P<float4>(m->pos), P<Node>(m->nodes), bb,
+                      P<BatchGeom>(b->geom), st);
+    m->launches += (uint64_t)nl;
+    m->build_launches = (uint32_t)nl;
+    return check_cuda(m, "pm_batch_build");
+}
+
+pm_status batch_query_device(pm_batch* b, uint32_t kmax, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
+                             float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, cudaStream_t st) {
+    pm_map* m = b->m;
+    if (nq == 0) return PM_OK;
+    const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
+    int nl = batch_query_keys(qpos, P<uint32_t>(b->q_off), b->num_maps, nq, P<BatchGeom>(b->geom),
+                              P<uint64_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
+    uint64_t* keys[2] = {P<uint64_t>(m->qkeys0), P<uint64_t>(m->qkeys1)};
+    uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
+    const int cur = nq > 1 ? radix_sort_pairs(keys, vals, nq, 48 + map_id_bits(b->num_maps), P<uint32_t>(m->qscratch),
+                                              st, &nl)
+                           : 0;
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
+    QueryTuning t = tuning_of(m);
+    t.stats = nullptr;
+    nl += query_knn_batch(view_of(m), P<BatchQuery>(b->bq), P<BatchGeom>(b->geom), kmax, qpos,
+                          reinterpret_cast<const float4*>(d_qnrm4), vals[cur], keys[cur], nq, out, P<uint32_t>(m->counter),
+                          P<uint32_t>(m->fixq), t, st);
+    m->launches += (uint64_t)nl;
+    b->query_launches = (uint32_t)nl;
+    return check_cuda(m, "pm_batch_query");
+}
+
+pm_status batch_check_query_args(pm_batch* b, const uint32_t* offsets, const float* d_qpos4, const float* d_qnrm4,
+                                 float* d_rad4, uint32_t* nq_out) {
+    if (!b->built) return batch_fail(b, PM_ERR_STATE, "the batch has not been built");
+    if (!offsets) return batch_fail(b, PM_ERR_INVALID, "query offsets are NULL");
+    const uint32_t nq = offsets[b->num_maps];
+    if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_rad4))
+        return batch_fail(b, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
+    if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_rad4)))
+        return batch_fail(b, PM_ERR_INVALID, "query and radiance arrays must be 16-byte aligned");
+    *nq_out = nq;
+    return PM_OK;
+}
+
+pm_status batch_prepare_build(pm_batch* b, const float* d_pos4, const float* d_pow4, const uint32_t* photon_offsets,
+                              uint32_t num_maps, int format) {
+    if (format != PM_PHOTONS_REFERENCE && format != PM_PHOTONS_PACKED)
+        return batch_fail(b, PM_ERR_INVALID, "unknown photon format");
+    pm_status s = batch_upload_photons(b, photon_offsets, num_maps);
+    if (s != PM_OK) return s;
+    const uint32_t n = photon_offsets[num_maps];
+    if (n > 0 && (!d_pos4 || !d_pow4)) return batch_fail(b, PM_ERR_INVALID, "photon arrays must be non-NULL");
+    if (n > 0 && (!aligned16(d_pos4) || !aligned16(d_pow4)))
+        return batch_fail(b, PM_ERR_INVALID, "photon arrays must be 16-byte aligned");
+    s = ensure_photon_capacity(b->m, n, nullptr);
+    if (s != PM_OK) return s;
+    b->num_maps = num_maps;
+    b->total_photons = n;
+    b->format = format;
+    return PM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pm_status pm_batch_create(pm_batch** out) {
+    if (!out) return PM_ERR_INVALID;
+    *out = nullptr;
+    pm_batch* b = new (std::nothrow) pm_batch();
+    if (!b) return PM_ERR_OOM;
+    pm_status s = pm_create(&b->m, 0, nullptr, nullptr, 1.0f);
+    if (s != PM_OK) { delete b; return s; }
+    *out = b;
+    return PM_OK;
+}
+
+pm_status pm_batch_destroy(pm_batch* b) {
+    if (!b) return PM_ERR_INVALID;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    DevBuf* all[] = {&b->ph_off, &b->q_off, &b->bq, &b->geom, &b->acc};
+    for (DevBuf* x : all) buf_free(b->m, *x);
+    pm_destroy(b->m);
+    delete b;
+    return PM_OK;
+}
+
+pm_status pm_batch_set_tuning(pm_batch* b, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk) {
+    if (!b) return PM_ERR_INVALID;
+    return pm_set_tuning(b->m, leaf_size, warps_per_block, rounds_per_chunk, 1, PM_KBUF_GROUP);
+}
+
+pm_status pm_batch_build(pm_batch* b, const float* d_pos4, const float* d_pow4, const uint32_t* photon_offsets,
+                         uint32_t num_maps, int format, void* stream) {
+    if (!b) return PM_ERR_INVALID;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return batch_fail(b, PM_ERR_STATE, "use pm_batch_capture to record a batch in a graph");
+    pm_status s = batch_prepare_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format);
+    if (s != PM_OK) return s;
+    s = batch_build_device(b, d_pos4, d_pow4, format, st);
+    if (s != PM_OK) return s;
+    b->m->n = b->total_photons;
+    b->m->built = true;
+    b->built = true;
+    return PM_OK;
+}
+
+pm_status pm_batch_query(pm_batch* b, const pm_query_desc* descs, const float* d_qpos4, const float* d_qnrm4,
+                         const uint32_t* query_offsets, float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count,
+                         void* stream) {
+    if (!b) return PM_ERR_INVALID;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return batch_fail(b, PM_ERR_STATE, "use pm_batch_capture to record a batch in a graph");
+    uint32_t nq = 0, kmax = 1;
+    uint64_t nbr_total = 0;
+    pm_status s = batch_check_query_args(b, query_offsets, d_qpos4, d_qnrm4, d_rad4, &nq);
+    if (s != PM_OK) return s;
+    if ((s = ensure_query_capacity(b->m, nq, st)) != PM_OK) return s;
+    if ((s = batch_upload_queries(b, descs, query_offsets, &kmax, &nbr_total)) != PM_OK) return s;
+    return batch_query_device(b, kmax, d_qpos4, d_qnrm4, nq, d_rad4, d_nbr, d_r2, d_count, st);
+}
+
+pm_status pm_batch_capture(pm_batch* b, const float* d_pos4, const float* d_pow4, const uint32_t* photon_offsets,
+                           uint32_t num_maps, int format, const pm_query_desc* descs, const float* d_qpos4,
+                           const float* d_qnrm4, const uint32_t* query_offsets, float* d_rad4, uint32_t* d_nbr,
+                           float* d_r2, uint32_t* d_count) {
+    if (!b) return PM_ERR_INVALID;
+    pm_status s = batch_prepare_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format);
+    if (s != PM_OK) return s;
+    b->built = true;   // the tables describe the maps the graph will build
+    uint32_t nq = 0, kmax = 1;
+    uint64_t nbr_total = 0;
+    if ((s = batch_check_query_args(b, query_offsets, d_qpos4, d_qnrm4, d_rad4, &nq)) != PM_OK) return s;
+    if ((s = ensure_query_capacity(b->m, nq, nullptr)) != PM_OK) return s;
+    if ((s = batch_upload_queries(b, descs, query_offsets, &kmax, &nbr_total)) != PM_OK) return s;
+    if (!b->cap_stream && cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return check_cuda(b->m, "pm_batch_capture: stream");
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    // kernel attributes are set outside the capture
+    if (cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return check_cuda(b->m, "pm_batch_capture: begin");
+    pm_status sb = batch_build_device(b, d_pos4, d_pow4, format, b->cap_stream);
+    pm_status sq = sb == PM_OK ? batch_query_device(b, kmax, d_qpos4, d_qnrm4, nq, d_rad4, d_nbr, d_r2, d_count,
+                                                    b->cap_stream)
+                               : sb;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    if (sq != PM_OK) { if (g) cudaGraphDestroy(g); return sq; }
+    if (e != cudaSuccess || !g) return check_cuda(b->m, "pm_batch_capture: end");
+    b->graph = g;
+    if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return check_cuda(b->m, "pm_batch_capture: instantiate");
+    b->m->n = b->total_photons;
+    b->m->built = true;
+    return PM_OK;
+}
+
+pm_status pm_batch_launch(pm_batch* b, void* stream) {
+    if (!b) return PM_ERR_INVALID;
+    if (!b->exec) return batch_fail(b, PM_ERR_STATE, "no captured batch; call pm_batch_capture first");
+    if (cudaGraphLaunch(b->exec, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+        return check_cuda(b->m, "pm_batch_launch");
+    return PM_OK;
+}
+
+pm_status pm_batch_get_info(pm_batch* b, pm_map_info* info, void* stream) {
+    if (!b) return PM_ERR_INVALID;
+    return pm_get_info(b->m, info, stream);
+}
+
+const char* pm_batch_last_error(const pm_batch* b) { return b ? pm_last_error(b->m) : "null handle"; }
+
+}  // extern "C"

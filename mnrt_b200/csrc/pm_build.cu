@@ -320,6 +320,32 @@ void scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr, cudaStream_
     k_scale_flux<<<blocks, 256, 0, st>>>(pw, n, scale, hdr);
 }
 
+// Everything after the sort: photons into tree order, radix tree, compaction
+// into 64-byte nodes, refit.  keys/vals are the sorted (code, caller index)
+// pairs; any code whose prefix separates groups (e.g. a map id in the top
+// bits) yields one subtree per group.
+int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
+                      const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st) {
+    const uint32_t tb = 256;
+    if (n > 0) {
+        k_gather<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, in_pow, vals, n, format, out_pos, out_pow, inv);
+        if (n > 1) {
+            const uint32_t ni = n - 1, gi = (ni + tb - 1) / tb;
+            k_radix_tree<<<gi, tb, 0, st>>>(keys, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep);
+            uint32_t* total = bb.scratch + sort_scratch_words(n);
+            const int ns = exclusive_scan(bb.kkeep, bb.krank, ni, total + 1, total, st);
+            k_emit<<<gi, tb, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank,
+                                      total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
+            k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
+            return 5 + ns;
+        }
+    }
+    k_emit<<<1, 32, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank, nullptr,
+                             nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
+    return n > 0 ? 2 : 1;
+}
+
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
               float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
               cudaStream_t st, cudaEvent_t sort_done) {
@@ -330,31 +356,18 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
     cudaMemsetAsync(bb.partials + 8 * bblocks, 0, sizeof(uint32_t), st);
     k_bounds<<<bblocks, kBoundsThreads, 0, st>>>(in_pos, in_pow, n, reinterpret_cast<float*>(bb.partials), hdr);
     ++nl;
+    uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
+    uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
+    int cur = 0;
     if (n > 0) {
-        const uint32_t tb = 256, grid = (n + tb - 1) / tb;
-        k_morton<<<grid, tb, 0, st>>>(in_pos, n, hdr, bb.keys[0], bb.vals[0]);
-        uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
-        uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
-        const int cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl);
-        if (sort_done) cudaEventRecord(sort_done, st);
-        k_gather<<<grid, tb, 0, st>>>(in_pos, in_pow, vals[cur], n, format, out_pos, out_pow, inv);
-        nl += 2;
-        if (n > 1) {
-            const uint32_t ni = n - 1, gi = (ni + tb - 1) / tb;
-            k_radix_tree<<<gi, tb, 0, st>>>(keys[cur], n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep);
-            uint32_t* total = bb.scratch + sort_scratch_words(n);
-            nl += 1 + exclusive_scan(bb.kkeep, bb.krank, ni, total + 1, total, st);
-            k_emit<<<gi, tb, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank,
-                                      total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
-            k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
-            return nl + 2;
-        }
-    } else if (sort_done) {
-        cudaEventRecord(sort_done, st);
+        const uint32_t tb = 256;
+        k_morton<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, n, hdr, bb.keys[0], bb.vals[0]);
+        ++nl;
+        cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl);
     }
-    k_emit<<<1, 32, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank, nullptr,
-                             nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
-    return nl + 1;
+    if (sort_done) cudaEventRecord(sort_done, st);
+    return nl + build_from_sorted(in_pos, in_pow, n, format, leaf_size, keys[cur], vals[cur], out_pos, out_pow, inv,
+                                  nodes, hdr, bb, st);
 }
 
 }  // namespace pm

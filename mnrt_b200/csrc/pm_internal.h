@@ -19,6 +19,25 @@ int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_b
 int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
                        cudaStream_t st, int* launches = nullptr);
 
+// One photon map of a batch: geometry written by the batch build, query
+// parameters uploaded by the host.
+struct __align__(16) BatchGeom {
+    ChildSlot root;        // slot of the map's subtree (empty slot for an empty map)
+    float lo[3];           // photon bounds, lower corner
+    float mscale;          // Morton scale of the map's cubic cell
+    float fix_scale;       // 2^40 / largest flux channel
+    float max_power;
+    uint32_t pad[2];
+};
+struct __align__(16) BatchQuery {
+    uint32_t q_off, q_n;   // queries [q_off, q_off + q_n) of the batch
+    uint32_t ph_off, ph_n; // photons [ph_off, ph_off + ph_n) of the batch
+    uint64_t nbr_off;      // first neighbour slot of the map's rows (rows hold k entries)
+    uint32_t k, min_found;
+    float r2max, rmax, cone_k;
+    int filter;
+};
+
 // Device buffers describing one built map (the build writes them, the
 // query reads them).  Pointers are device addresses.
 struct MapView {
@@ -54,6 +73,9 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
               float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
               cudaStream_t st, cudaEvent_t sort_done = nullptr);
 void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st);
+int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
+                      const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st);
 
 // pm_query.cu
 struct QueryParams {
@@ -87,6 +109,21 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);
 int query_smem_bytes_per_warp(uint32_t k);
+
+int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
+                    const float4* qnrm, const uint32_t* order, const uint64_t* qkeys, uint32_t nq,
+                    const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list, const QueryTuning& t,
+                    cudaStream_t st);
+
+// pm_batch.cu
+int batch_bounds_and_keys(const float4* pos, const float4* pw, const uint32_t* ph_off, uint32_t m, uint32_t n,
+                          uint32_t* acc, BatchGeom* geom, MapHeader* hdr, uint64_t* keys, uint32_t* vals,
+                          cudaStream_t st);
+int batch_query_keys(const float4* qpos, const uint32_t* q_off, uint32_t m, uint32_t nq, const BatchGeom* geom,
+                     uint64_t* keys, uint32_t* vals, cudaStream_t st);
+int batch_roots(const uint32_t* ph_off, uint32_t m, uint32_t n, uint32_t leaf_size, const float4* pos,
+                const Node* nodes, const BuildBuffers& bb, BatchGeom* geom, cudaStream_t st);
+int map_id_bits(uint32_t m);
 
 // pm_gather.cu
 int gather_normals(const float4* hit_nrm, const float4* ray_dir, uint32_t n, float4* out_nrm, cudaStream_t st);

@@ -48,13 +48,22 @@ struct KnnArgs {
     float* out_r2;
     uint32_t* out_count;
     uint32_t* work_counter;
-    uint32_t* fix_list;       // group kernel: queries whose estimate needs FP64 distances
+    uint32_t* fix_list;       // group kernel: sorted slots of queries whose estimate needs FP64 distances
+    const uint32_t* fix_in;   // fix pass: the list it works through
     uint32_t* fix_count;
     const uint32_t* nq_dev;   // fix pass: query count read on the device
     uint32_t rounds_per_chunk;
     uint32_t cap;             // group kernel: candidate buffer entries per query
     uint32_t smem_per_warp;   // group kernel: shared bytes per warp
     unsigned long long* stats;   // optional traversal counters (kStat*), nullptr = off
+    const float* scale_ptr;   // fixed-point scale of the flux sums (map header or batch map)
+    const ChildSlot* root;    // slot the traversal starts from
+    uint64_t nbr_off;         // batch: first neighbour slot of the map's rows
+    uint32_t q_off;           // batch: first query of the map
+    uint32_t ph_off;          // batch: first photon of the map (caller indices are batch-global)
+    const uint64_t* qkeys;    // batch: sorted query keys, map id in bits 48..63
+    const BatchGeom* bgeom;   // batch: per-map geometry (built)
+    const BatchQuery* bq;     // batch: per-map query parameters
 };
 
 // Counters of the group kernel, accumulated when KnnArgs::stats is set.
@@ -234,7 +243,7 @@ __device__ __forceinline__ double est_fp64_heap(const KnnArgs& a, const uint64_t
                                              bool full, uint32_t kth, float qx, float qy, float qz, float nx, float ny,
                                              float nz, EstAcc& acc) {
     const double r2d = filter_r2(a.pos, full, kth, qx, qy, qz, a.rmax);
-    const float scale = a.hdr->fix_scale;
+    const float scale = *a.scale_ptr;
     Filter64 flt;
     flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
     acc = EstAcc{0, 0, 0, 0};
@@ -279,7 +288,7 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
     }
     float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)hn);
     if (hn > 0 && hn >= a.min_found && r2 > 0.0f) {
-        const float scale = a.hdr->fix_scale;
+        const float scale = *a.scale_ptr;
         const float inv = filter_inv32(a.filter, r2, a.cone_k);
         EstAcc acc = {0, 0, 0, 0};
         for (uint32_t j = 0; j < hn; ++j) {
@@ -298,6 +307,13 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
 __device__ __forceinline__ void load_slot(const Node* nodes, uint32_t node, uint32_t side, float* lo, float* hi,
                                           uint32_t& ref, uint32_t& cnt) {
     const float4* p = reinterpret_cast<const float4*>(&nodes[node].c[side]);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    lo[0] = a.x; lo[1] = a.y; lo[2] = a.z; hi[0] = a.w;
+    hi[1] = b.x; hi[2] = b.y; ref = __float_as_uint(b.z); cnt = __float_as_uint(b.w);
+}
+
+__device__ __forceinline__ void load_root(const ChildSlot* slot, float* lo, float* hi, uint32_t& ref, uint32_t& cnt) {
+    const float4* p = reinterpret_cast<const float4*>(slot);
     const float4 a = __ldg(p), b = __ldg(p + 1);
     lo[0] = a.x; lo[1] = a.y; lo[2] = a.z; hi[0] = a.w;
     hi[1] = b.x; hi[2] = b.y; ref = __float_as_uint(b.z); cnt = __float_as_uint(b.w);
@@ -665,7 +681,7 @@ __device__ __forceinline__ double est_fp64_group(const KnnArgs& a, const uint64_
     const bool full = n == a.k;
     const uint32_t kth = full ? group_kth<G>(a, buf, n, s, gmask) : 0u;
     const double r2d = filter_r2(a.pos, full, kth, qx, qy, qz, a.rmax);
-    const float scale = a.hdr->fix_scale;
+    const float scale = *a.scale_ptr;
     Filter64 flt;
     flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
     acc = EstAcc{0, 0, 0, 0};
@@ -678,8 +694,8 @@ __device__ __forceinline__ double est_fp64_group(const KnnArgs& a, const uint64_
 
 template <int G, bool kFix>
 __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, uint32_t s,
-                              uint32_t gmask, uint32_t lt, uint32_t qo, float qx, float qy, float qz, float nx,
-                              float ny, float nz) {
+                              uint32_t gmask, uint32_t lt, uint32_t qo, uint32_t slot, float qx, float qy, float qz,
+                              float nx, float ny, float nz) {
     const uint32_t k = a.k;
     if (n > k) group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
     float rk2 = a.r2max;
@@ -691,7 +707,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
     const float r2 = rk2;
     float4 rad = make_float4(0.f, 0.f, 0.f, (float)n);
     if (n > 0 && n >= a.min_found && r2 > 0.0f) {
-        const float scale = a.hdr->fix_scale;
+        const float scale = *a.scale_ptr;
         const float inv = filter_inv32(a.filter, r2, a.cone_k);
         EstAcc acc = {0, 0, 0, 0};
         for (uint32_t e = s; e < n; e += G) {
@@ -707,7 +723,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
             if (kFix) {
                 r2d = est_fp64_group<G>(a, buf, n, s, gmask, qx, qy, qz, nx, ny, nz, acc);
             } else if (s == 0) {   // re-evaluated by the fix pass (the FP32 result written below is replaced)
-                a.fix_list[atomicAdd(a.fix_count, 1u)] = qo;
+                a.fix_list[atomicAdd(a.fix_count, 1u)] = slot;
             }
         }
         rad = est_result(acc, a.filter, r2d, a.cone_k, scale, n);
@@ -721,12 +737,12 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
         // rank sort by exact (d^2, caller index)
         for (uint32_t e = s; e < n; e += G) buf[e] = exact_key(buf[e], a.pos);
         __syncwarp(gmask);
-        uint32_t* row = a.out_nbr + (size_t)qo * k;
+        uint32_t* row = a.out_nbr + a.nbr_off + (size_t)(qo - a.q_off) * k;
         for (uint32_t e = s; e < n; e += G) {
             const uint64_t v = buf[e];
             uint32_t rank = 0;
             for (uint32_t f = 0; f < n; ++f) rank += buf[f] < v ? 1u : 0u;
-            row[rank] = (uint32_t)v;
+            row[rank] = (uint32_t)v - a.ph_off;
         }
         for (uint32_t j = n + s; j < k; j += G) row[j] = kInvalid;
         __syncwarp(gmask);
@@ -734,8 +750,8 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
     return r2;
 }
 
-template <int G, bool kFix>
-__global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
+template <int G, bool kFix, bool kBatch>
+__global__ void __launch_bounds__(256) k_knn_group(KnnArgs a0) {
     constexpr int QW = 32 / G;
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = lane_id();
@@ -744,32 +760,50 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
     const uint32_t gbase = g * G;
     const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
     const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t k = a.k, C = a.cap;
-    unsigned char* wb = smem + (size_t)warp * a.smem_per_warp;
+    const uint32_t C = a0.cap;
+    unsigned char* wb = smem + (size_t)warp * a0.smem_per_warp;
     uint64_t* buf = reinterpret_cast<uint64_t*>(wb) + (size_t)g * C;
     uint32_t* hist = reinterpret_cast<uint32_t*>(wb + (size_t)QW * C * sizeof(uint64_t)) + g * 256;
     uint32_t* stack = reinterpret_cast<uint32_t*>(wb + (size_t)QW * (C * sizeof(uint64_t) + 256 * sizeof(uint32_t)));
-    const float r2max = a.r2max;
-    const uint32_t chunk_q = a.rounds_per_chunk * QW;
-    const uint32_t nq = kFix ? *a.nq_dev : a.nq;
+    const uint32_t chunk_q = a0.rounds_per_chunk * QW;
+    const uint32_t nq = kFix ? *a0.nq_dev : a0.nq;
     const uint32_t nchunks = (nq + chunk_q - 1) / chunk_q;
 
     for (;;) {
         uint32_t chunk = 0;
-        if (lane == 0) chunk = atomicAdd(a.work_counter, 1u);
+        if (lane == 0) chunk = atomicAdd(a0.work_counter, 1u);
         chunk = __shfl_sync(kFull, chunk, 0);
         if (chunk >= nchunks) break;
         float pqx = 0.f, pqy = 0.f, pqz = 0.f, pr = 0.f;
         bool pvalid = false;
-        for (uint32_t round = 0; round < a.rounds_per_chunk; ++round) {
+        uint32_t pmap = 0;   // batch: map of the previous round's query
+        for (uint32_t round = 0; round < a0.rounds_per_chunk; ++round) {
             const uint32_t slot_q = chunk * chunk_q + round * QW + g;
             const bool inrange = slot_q < nq;
             if (!__any_sync(kFull, inrange)) break;
+            // per-query arguments: the launch's, or (batch) those of the query's map
+            KnnArgs a = a0;
+            uint32_t map = 0;
+            const uint32_t slot_main = (kFix && inrange) ? a0.fix_in[slot_q] : slot_q;   // slot of the sorted launch
+            if (kBatch && inrange) {
+                map = (uint32_t)(a0.qkeys[slot_main] >> 48);
+                const BatchQuery bq = a0.bq[map];
+                a.k = bq.k; a.r2max = bq.r2max; a.rmax = bq.rmax; a.filter = bq.filter; a.cone_k = bq.cone_k;
+                a.min_found = bq.min_found; a.nbr_off = bq.nbr_off; a.q_off = bq.q_off; a.ph_off = bq.ph_off;
+                a.scale_ptr = &a0.bgeom[map].fix_scale;
+                a.root = &a0.bgeom[map].root;
+            }
+            const uint32_t k = a.k;
+            const float r2max = a.r2max;
+            if (kBatch) {   // a radius bound only carries over within one map
+                if (map != pmap) pvalid = false;
+                pmap = map;
+            }
             uint32_t qo = 0;
             float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
             bool active = false;
             if (inrange) {
-                qo = a.order ? a.order[slot_q] : slot_q;
+                qo = a.order ? a.order[slot_main] : slot_main;
                 const float4 q = a.qpos[qo];
                 const float4 nn = a.qnrm[qo];
                 qx = q.x; qy = q.y; qz = q.z; nx = nn.x; ny = nn.y; nz = nn.z;
@@ -801,7 +835,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 int sp = 0;
                 float lo[3], hi[3];
                 uint32_t ref, cnt;
-                load_slot(a.nodes, 0, 0, lo, hi, ref, cnt);
+                load_root(a.root, lo, hi, ref, cnt);
                 bool have;
                 {
                     const float lb = box_lb(qx, qy, qz, lo, hi);
@@ -909,7 +943,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 atomicAdd(a.stats + kStatPhotons, (unsigned long long)st_photons);
             }
             if (active) {
-                const float r2 = group_finish<G, kFix>(a, buf, n, hist, s, gmask, lt, qo, qx, qy, qz, nx, ny, nz);
+                const float r2 = group_finish<G, kFix>(a, buf, n, hist, s, gmask, lt, qo, slot_main, qx, qy, qz, nx, ny, nz);
                 rk2 = r2;
             } else if (inrange && s == 0) {
                 a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -917,7 +951,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a) {
                 if (a.out_count) a.out_count[qo] = 0;
             }
             if (inrange && !active && a.out_nbr)
-                for (uint32_t j = s; j < k; j += G) a.out_nbr[(size_t)qo * k + j] = kInvalid;
+                for (uint32_t j = s; j < k; j += G) a.out_nbr[a.nbr_off + (size_t)(qo - a.q_off) * k + j] = kInvalid;
             __syncwarp();
             pqx = qx; pqy = qy; pqz = qz;
             pvalid = active && n == k;
@@ -1021,7 +1055,11 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.k = p.k; a.r2max = p.r2; a.rmax = p.r; a.filter = p.filter; a.cone_k = p.cone_k; a.min_found = p.min_found;
     a.out_rad = out.rad; a.out_nbr = out.nbr; a.out_r2 = out.r2; a.out_count = out.count;
     a.work_counter = nullptr; a.rounds_per_chunk = 1;
-    a.fix_list = nullptr; a.fix_count = nullptr; a.nq_dev = nullptr;
+    a.fix_list = nullptr; a.fix_count = nullptr; a.nq_dev = nullptr; a.fix_in = nullptr;
+    a.scale_ptr = &m.hdr->fix_scale;
+    a.root = &m.nodes[0].c[0];
+    a.nbr_off = 0; a.q_off = 0; a.ph_off = 0;
+    a.qkeys = nullptr; a.bgeom = nullptr; a.bq = nullptr;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
     return a;
 }
@@ -1073,15 +1111,15 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
     a.fix_count = work_counter + 1;
     a.nq_dev = nullptr;
     KnnArgs fx = a;   // fix pass: the listed queries, FP64 distances where needed
-    fx.order = fix_list;
+    fx.fix_in = fix_list;
     fx.nq_dev = work_counter + 1;
     fx.work_counter = work_counter + 2;
 #define PM_LAUNCH_GROUP(G)                                                                          \
     {                                                                                               \
-        const uint32_t grid = grid_for(k_knn_group<G, false>, threads, smem, nchunks, t.warps_per_block); \
-        k_knn_group<G, false><<<grid, threads, smem, st>>>(a);                                      \
-        const uint32_t gfix = grid_for(k_knn_group<G, true>, threads, smem, nchunks, t.warps_per_block); \
-        k_knn_group<G, true><<<gfix, threads, smem, st>>>(fx);                                      \
+        const uint32_t grid = grid_for(k_knn_group<G, false, false>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, false, false><<<grid, threads, smem, st>>>(a);                                      \
+        const uint32_t gfix = grid_for(k_knn_group<G, true, false>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, true, false><<<gfix, threads, smem, st>>>(fx);                                      \
     }
     switch (qpw) {
         case 1: PM_LAUNCH_GROUP(32) break;
@@ -1090,6 +1128,41 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         default: PM_LAUNCH_GROUP(4) break;
     }
 #undef PM_LAUNCH_GROUP
+    return 2;
+}
+
+// One persistent launch over the queries of many maps (one query per warp):
+// the sorted query keys carry each query's map id, whose root slot and
+// parameters the kernel reads; kmax sizes the candidate buffers.
+int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
+                    const float4* qnrm, const uint32_t* order, const uint64_t* qkeys, uint32_t nq,
+                    const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list, const QueryTuning& t,
+                    cudaStream_t st) {
+    if (!nq) return 0;
+    QueryParams p;
+    p.k = kmax; p.r = 0.0f; p.r2 = 0.0f; p.filter = 0; p.cone_k = 1.0f; p.min_found = 0;
+    KnnArgs a = make_args(m, p, qpos, qnrm, order, nq, out);
+    a.work_counter = work_counter;
+    a.rounds_per_chunk = (uint32_t)t.rounds_per_chunk;
+    a.qkeys = qkeys;
+    a.bgeom = bg;
+    a.bq = bq;
+    a.cap = group_capacity(kmax);
+    a.smem_per_warp = (uint32_t)group_smem_bytes_per_warp(kmax, 1);
+    a.fix_list = fix_list;
+    a.fix_count = work_counter + 1;
+    const int threads = 32 * t.warps_per_block;
+    const int smem = (int)a.smem_per_warp * t.warps_per_block;
+    cudaMemsetAsync(work_counter, 0, 3 * sizeof(uint32_t), st);
+    const uint32_t nchunks = (nq + a.rounds_per_chunk - 1) / a.rounds_per_chunk;
+    const uint32_t grid = grid_for(k_knn_group<32, false, true>, threads, smem, nchunks, t.warps_per_block);
+    k_knn_group<32, false, true><<<grid, threads, smem, st>>>(a);
+    KnnArgs fx = a;   // queries whose estimate needs FP64 distances
+    fx.fix_in = fix_list;
+    fx.nq_dev = work_counter + 1;
+    fx.work_counter = work_counter + 2;
+    const uint32_t gfix = grid_for(k_knn_group<32, true, true>, threads, smem, nchunks, t.warps_per_block);
+    k_knn_group<32, true, true><<<gfix, threads, smem, st>>>(fx);
     return 2;
 }
 

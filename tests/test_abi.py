@@ -116,3 +116,19 @@ def test_backward_validation_without_gpu(engine_lib):
     assert lib.pm_set_backward_chunk(h, 1000) == L.PM_OK
     assert lib.pm_set_backward_chunk(None, 1000) == L.PM_ERR_INVALID
     lib.pm_destroy(h)
+
+
+def test_batch_validation_without_gpu(engine_lib):
+    import numpy as np
+    lib = engine_lib
+    h = C.c_void_p()
+    assert lib.pm_batch_create(C.byref(h)) == L.PM_OK
+    bad_start = np.array([1, 5], np.uint32)
+    assert lib.pm_batch_build(h, 16, 32, bad_start.ctypes.data, 1, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID
+    decreasing = np.array([0, 5, 3], np.uint32)
+    assert lib.pm_batch_build(h, 16, 32, decreasing.ctypes.data, 2, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID
+    assert b"must not decrease" in lib.pm_batch_last_error(h)
+    assert lib.pm_batch_build(h, 16, 32, None, 2, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID
+    assert lib.pm_batch_launch(h, None) == L.PM_ERR_STATE
+    assert lib.pm_batch_set_tuning(h, 0, 4, 8) == L.PM_ERR_INVALID
+    assert lib.pm_batch_destroy(h) == L.PM_OK
