@@ -430,13 +430,94 @@ def run_diff(args, cfg) -> dict:
     }
 
 
+def run_batch(args) -> dict:
+    """Config 3: 64 photon maps (photon counts log-uniform in [1e4, 2e6], query
+    counts log-uniform in [1e3, 1e6], k from {16, 32, 64, 128}, R = 0.05),
+    built and queried as one batch (eager and CUDA-graph replay) against 64
+    sequential per-map build + query calls."""
+    import torch
+    from mnrt_b200 import gen
+    from mnrt_b200.batch import PhotonMapBatch, make_desc
+    from mnrt_b200.photon_map import PhotonMap
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    spec = gen.batch_spec(args.maps, seed=777)
+    phs = [gen.photons(n, seed=sd, caustic_frac=0.2) for n, sd in zip(spec.n, spec.seeds)]
+    qs = [gen.queries(nq, seed=sd + 500) for nq, sd in zip(spec.nq, spec.seeds)]
+    descs = [dict(k=k, r_max=0.05, filter="cone") for k in spec.k]
+    poff = np.concatenate([[0], np.cumsum(spec.n)]).astype(np.uint32)
+    qoff = np.concatenate([[0], np.cumsum(spec.nq)]).astype(np.uint32)
+    N, Q = int(poff[-1]), int(qoff[-1])
+    d_pos = torch.from_numpy(np.concatenate([p.pos for p in phs])).to(dev)
+    d_pw = torch.from_numpy(np.concatenate([p.pow for p in phs])).to(dev)
+    d_qp = torch.from_numpy(np.concatenate([q.pos for q in qs])).to(dev)
+    d_qn = torch.from_numpy(np.concatenate([q.nrm for q in qs])).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ts = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0.record(); fn(); e1.record(); e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.mean(ts))
+
+    # 64 sequential plain-form calls (storage reserved beforehand)
+    maps = []
+    for i, (ph, q) in enumerate(zip(phs, qs)):
+        pm = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=spec.k[i])
+        pm.reserve(ph.n, q.n)
+        a, b = int(poff[i]), int(poff[i + 1])
+        c, d = int(qoff[i]), int(qoff[i + 1])
+        out = {"rad": torch.empty((q.n, 4), dtype=torch.float32, device=dev)}
+        maps.append((pm, d_pos[a:b], d_pw[a:b], d_qp[c:d], d_qn[c:d], out, descs[i]))
+
+    def sequential():
+        for pm, p, w, qp, qn, out, dsc in maps:
+            pm.build(p, w)
+            pm.query(qp, qn, out=out, **dsc)
+
+    seq_ms = timed(sequential)
+    for m in maps:
+        m[0].close()
+    batch = PhotonMapBatch()
+    out = batch.outputs(descs, qoff, dev)
+
+    def eager():
+        batch.build(d_pos, d_pw, poff)
+        batch.query(descs, d_qp, d_qn, qoff, out=out)
+
+    eager_ms = timed(eager)
+    batch.capture(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
+    graph_ms = timed(lambda: batch.launch())
+    info = batch.info()
+    batch.close()
+    clocks = None
+    return {
+        "metric": "batched photon maps: kNN radiance estimates/s (build + query of all maps per step)",
+        "value": Q / (graph_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batch: {args.maps} maps, {N:,} photons, {Q:,} queries (log-uniform sizes, "
+                               f"seed 777), k in {{16,32,64,128}}, R=0.05, cone filter",
+                   "maps": args.maps, "photons": N, "queries": Q, "l2": "flushed between steps (256 MiB write, untimed)"},
+        "batched_graph_ms": graph_ms, "batched_eager_ms": eager_ms, "sequential_per_map_ms": seq_ms,
+        "sequential_queries_per_s": Q / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q / (eager_ms / 1000.0),
+        "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": info.device_errors,
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff"])
+    ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff", "batch"])
+    ap.add_argument("--maps", type=int, default=64, help="maps of the batch workload")
     ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gd-steps", type=int, default=200, help="gradient-descent steps of the diff workload")
@@ -448,11 +529,14 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    cfg = workload_config(args.config)
+    cfg = workload_config(args.config) if args.config != "batch" else None
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
         print(json.dumps(run_reference(args, cfg)), flush=True)
+        return 0
+    if args.config == "batch":
+        print(json.dumps(run_batch(args)), flush=True)
         return 0
     if args.config == "diff":
         print(json.dumps(run_diff(args, cfg)), flush=True)
