@@ -213,9 +213,16 @@ def run_ours(args, cfg) -> dict | None:
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
 
     pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
+    tuning = "defaults"
     if args.leaf or args.wpb or args.rounds or args.qpw or args.layout >= 0:
         pm.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 32,
                       queries_per_warp=args.qpw or 1, kbuf_layout=args.layout if args.layout >= 0 else 1)
+        tuning = "set by flags"
+    elif not args.no_autotune:   # untimed: picks the kernel setting on a query sample
+        t = pm.autotune(d_pos, d_pow, d_qpos, d_qnrm, max_sample=0, k=k, r_max=R, filter=cfg["filter"])
+        tuning = {"leaf_size": t.leaf_size, "warps_per_block": t.warps_per_block,
+                  "rounds_per_chunk": t.rounds_per_chunk, "queries_per_warp": t.queries_per_warp,
+                  "kbuf_layout": t.kbuf_layout, "chosen_by": "pm_autotune over all queries"}
     pm.reserve(N, Q)
     pm.set_profiling(True)
     out = {"rad": d_rad}
@@ -297,7 +304,7 @@ def run_ours(args, cfg) -> dict | None:
         "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R,
                    "filter": cfg["filter"], "query_order": "as given" if args.unsorted else "Morton-sorted",
                    "l2": "flushed between steps (256 MiB write, untimed)",
-                   "parallelism": f"{world} independent replica(s), one per GPU"},
+                   "parallelism": f"{world} independent replica(s), one per GPU", "tuning": tuning},
         "build_ms": build_ms, "query_ms": float(np.mean(queries)), "query_sort_ms": float(np.mean(sorts)),
         "query_kernel_ms": kern_ms, "query_only_mqueries_per_s": Q / (float(np.mean(queries)) / 1000.0) / 1e6,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -486,6 +493,7 @@ def run_batch(args) -> dict:
         m[0].close()
     batch = PhotonMapBatch()
     out = batch.outputs(descs, qoff, dev)
+    bt = batch.autotune(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
 
     def eager():
         batch.build(d_pos, d_pw, poff)
@@ -507,6 +515,8 @@ def run_batch(args) -> dict:
         "batched_graph_ms": graph_ms, "batched_eager_ms": eager_ms, "sequential_per_map_ms": seq_ms,
         "sequential_queries_per_s": Q / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q / (eager_ms / 1000.0),
         "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": info.device_errors,
+        "batch_tuning": {"leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block,
+                         "rounds_per_chunk": bt.rounds_per_chunk, "chosen_by": "pm_batch_autotune"},
     }
 
 
@@ -520,6 +530,7 @@ def main(argv=None) -> int:
     ap.add_argument("--maps", type=int, default=64, help="maps of the batch workload")
     ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel setting")
     ap.add_argument("--gd-steps", type=int, default=200, help="gradient-descent steps of the diff workload")
     ap.add_argument("--leaf", type=int, default=0)
     ap.add_argument("--wpb", type=int, default=0)

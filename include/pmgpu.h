@@ -123,6 +123,28 @@ enum { PM_KBUF_HEAP = 0,   /* one lane per query, max-heap in shared memory */
 PM_API pm_status pm_set_tuning(pm_map* map, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk,
                                int queries_per_warp, int kbuf_layout);
 
+/* The autotuner's choice (no counterpart in the reference). */
+typedef struct pm_tuning {
+    uint32_t leaf_size;
+    int warps_per_block;
+    int rounds_per_chunk;
+    int queries_per_warp;
+    int kbuf_layout;
+    float build_ms;          /* timed build of the chosen setting */
+    float query_ms;          /* timed query of the sample, scaled to all nq queries */
+} pm_tuning;
+
+/* Times build + query over a grid of tuning candidates (leaf size, warps per
+ * block, rounds per chunk, queries per warp, k-buffer layout) on a strided
+ * sample of at most max_sample queries (0 = all), applies the fastest to the
+ * map, writes it to *best and leaves the map built with it.  Synchronous.
+ * A sample is sparser than the full set, which weakens the reuse of the
+ * previous query's radius bound between Morton neighbours: tune on all
+ * queries (or a dense spatial subset) when the setting matters. */
+PM_API pm_status pm_autotune(pm_map* map, const float* d_pos4, const float* d_pow4, uint32_t n, int format,
+                             const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
+                             uint32_t max_sample, pm_tuning* best, void* stream);
+
 /* Reserves storage for up to max_photons photons and max_queries queries so
  * that later builds and queries allocate nothing (needed for stream capture). */
 PM_API pm_status pm_reserve(pm_map* map, uint32_t max_photons, uint32_t max_queries);
@@ -263,6 +285,13 @@ PM_API pm_status pm_batch_capture(pm_batch* batch, const float* d_pos4, const fl
 PM_API pm_status pm_batch_launch(pm_batch* batch, void* stream);
 PM_API pm_status pm_batch_get_info(pm_batch* batch, pm_map_info* info, void* stream);
 PM_API const char* pm_batch_last_error(const pm_batch* batch);
+/* Times batch build + query over a grid of leaf sizes, warps per block and
+ * rounds per chunk, applies the fastest, writes it to *best and leaves the
+ * batch built with it.  Synchronous. */
+PM_API pm_status pm_batch_autotune(pm_batch* batch, const float* d_pos4, const float* d_pow4,
+                                   const uint32_t* photon_offsets, uint32_t num_maps, int format,
+                                   const pm_query_desc* descs, const float* d_qpos4, const float* d_qnrm4,
+                                   const uint32_t* query_offsets, float* d_rad4, pm_tuning* best, void* stream);
 
 /* Phase timing with CUDA events recorded on the call's stream (off by
  * default).  pm_last_timings waits for the last recorded events. */

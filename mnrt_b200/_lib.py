@@ -35,6 +35,12 @@ class MapInfo(C.Structure):
                 ("max_power", C.c_float), ("launches", C.c_uint64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("leaf_size", C.c_uint32), ("warps_per_block", C.c_int), ("rounds_per_chunk", C.c_int),
+                ("queries_per_warp", C.c_int), ("kbuf_layout", C.c_int), ("build_ms", C.c_float),
+                ("query_ms", C.c_float)]
+
+
 class Timings(C.Structure):
     _fields_ = [("build_ms", C.c_float), ("build_sort_ms", C.c_float), ("query_ms", C.c_float),
                 ("query_sort_ms", C.c_float), ("query_kernel_ms", C.c_float), ("build_launches", C.c_uint32),
@@ -54,6 +60,7 @@ SIGNATURES = {
     "pm_set_allocator": (_I, [_VP, ALLOC_FN, FREE_FN, _VP]),
     "pm_set_tuning": (_I, [_VP, _U32, _I, _I, _I, _I]),
     "pm_reserve": (_I, [_VP, _U32, _U32]),
+    "pm_autotune": (_I, [_VP, _FP, _FP, _U32, _I, C.POINTER(QueryDesc), _FP, _FP, _U32, _U32, C.POINTER(Tuning), _VP]),
     "pm_build": (_I, [_VP, _FP, _FP, _U32, _I, _VP]),
     "pm_query": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_bruteforce": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
@@ -78,6 +85,7 @@ SIGNATURES = {
     "pm_batch_launch": (_I, [_VP, _VP]),
     "pm_batch_get_info": (_I, [_VP, C.POINTER(MapInfo), _VP]),
     "pm_batch_last_error": (C.c_char_p, [_VP]),
+    "pm_batch_autotune": (_I, [_VP, _FP, _FP, _VP, _U32, _I, _VP, _FP, _FP, _VP, _FP, C.POINTER(Tuning), _VP]),
     "pm_last_error": (C.c_char_p, [_VP]),
     "pm_status_string": (C.c_char_p, [_I]),
     "pm_abi_version": (_I, []),

@@ -100,6 +100,19 @@ class PhotonMapBatch:
                                                _ptr(qpos), _ptr(qnrm), qoff.ctypes.data, _ptr(out["rad"]),
                                                _ptr(out.get("nbr")), _ptr(out.get("r2")), _ptr(out.get("count"))))
 
+    def autotune(self, pos, pw, photon_offsets, descs, qpos, qnrm, query_offsets, out: dict, packed: bool = True,
+                 stream=None) -> L.Tuning:
+        """Times build + query over leaf sizes, warps per block and rounds per
+        chunk; keeps the fastest and leaves the batch built with it."""
+        poff, qoff = _offsets(photon_offsets), _offsets(query_offsets)
+        arr = self._descs(descs)
+        best = L.Tuning()
+        fmt = L.PM_PHOTONS_PACKED if packed else L.PM_PHOTONS_REFERENCE
+        self._check(self._lib.pm_batch_autotune(self._h, _ptr(pos), _ptr(pw), poff.ctypes.data, poff.size - 1, fmt, arr,
+                                                _ptr(qpos), _ptr(qnrm), qoff.ctypes.data, _ptr(out["rad"]),
+                                                C.byref(best), _stream(stream)))
+        return best
+
     def launch(self, stream=None) -> None:
         self._check(self._lib.pm_batch_launch(self._h, _stream(stream)))
 

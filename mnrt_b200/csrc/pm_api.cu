@@ -1078,3 +1078,158 @@ pm_status pm_batch_get_info(pm_batch* b, pm_map_info* info, void* stream) {
 const char* pm_batch_last_error(const pm_batch* b) { return b ? pm_last_error(b->m) : "null handle"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: times build + query for a grid of tuning candidates on a strided
+// sample of the caller's queries and keeps the fastest (build time plus query
+// time scaled to all queries).  Leaf size changes the build, so every
+// candidate rebuilds the map.
+namespace {
+
+struct TuneCand {
+    uint32_t leaf;
+    int wpb, rounds, qpw, layout;
+};
+
+std::vector<TuneCand> tune_candidates(uint32_t k) {
+    std::vector<TuneCand> c;
+    const uint32_t leaves[] = {16, 24, 32};
+    const int wpbs[] = {2, 4, 8};
+    const int rounds[] = {8, 32};
+    for (uint32_t l : leaves)
+        for (int w : wpbs)
+            for (int r : rounds) {
+                c.push_back({l, w, r, 1, PM_KBUF_GROUP});
+                c.push_back({l, w, r, 2, PM_KBUF_GROUP});
+            }
+    if (k <= 64) c.push_back({16, 4, 8, 1, PM_KBUF_HEAP});   // one lane per query suits small k
+    return c;
+}
+
+}  // namespace
+
+extern "C" pm_status pm_autotune(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t n, int format,
+                                 const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
+                                 uint32_t max_sample, pm_tuning* best, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!best) return fail(m, PM_ERR_INVALID, "best is NULL");
+    pm_status s = validate_desc(m, desc, true);
+    if (s != PM_OK) return s;
+    if (nq == 0 || n == 0) return fail(m, PM_ERR_INVALID, "autotuning needs photons and queries");
+    if (!d_qpos4 || !d_qnrm4 || !aligned16(d_qpos4) || !aligned16(d_qnrm4))
+        return fail(m, PM_ERR_INVALID, "query arrays must be non-NULL and 16-byte aligned");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return fail(m, PM_ERR_STATE, "pm_autotune cannot run inside a stream capture");
+    const uint32_t sample = max_sample == 0 || max_sample > nq ? nq : max_sample;
+    const uint32_t stride = nq / sample;
+    if ((s = ensure_query_capacity(m, sample, st)) != PM_OK) return s;
+    if ((s = buf_ensure(m, m->gnrm, (size_t)sample * sizeof(float4), "tune normals")) != PM_OK) return s;
+    if ((s = buf_ensure(m, m->gest, (size_t)sample * sizeof(float4), "tune estimates")) != PM_OK) return s;
+    DevBuf spos;
+    if ((s = buf_ensure(m, spos, (size_t)sample * sizeof(float4), "tune positions")) != PM_OK) return s;
+    // strided sample: every stride-th query (one 16-byte record per row)
+    if (cudaMemcpy2DAsync(spos.ptr, sizeof(float4), d_qpos4, (size_t)stride * sizeof(float4), sizeof(float4), sample,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpy2DAsync(m->gnrm.ptr, sizeof(float4), d_qnrm4, (size_t)stride * sizeof(float4), sizeof(float4), sample,
+                          cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+        buf_free(m, spos);
+        return check_cuda(m, "pm_autotune: sample");
+    }
+    cudaEvent_t ev[3];
+    for (cudaEvent_t& e : ev) cudaEventCreate(&e);
+    const uint32_t saved_leaf = m->leaf_size;
+    const int saved[4] = {m->warps_per_block, m->rounds_per_chunk, m->queries_per_warp, m->kbuf_layout};
+    float best_score = INFINITY;
+    TuneCand best_c{saved_leaf, saved[0], saved[1], saved[2], saved[3]};
+    float best_b = 0, best_q = 0;
+    const double scale = (double)nq / (double)sample;
+    for (const TuneCand& c : tune_candidates(desc->k)) {
+        m->leaf_size = c.leaf; m->warps_per_block = c.wpb; m->rounds_per_chunk = c.rounds;
+        m->queries_per_warp = c.qpw; m->kbuf_layout = c.layout;
+        float tb = 0, tq = 0;
+        for (int rep = 0; rep < 2; ++rep) {   // the second run is timed
+            cudaEventRecord(ev[0], st);
+            s = pm_build(m, d_pos4, d_pow4, n, format, stream);
+            cudaEventRecord(ev[1], st);
+            if (s == PM_OK)
+                s = pm_query(m, desc, static_cast<const float*>(spos.ptr), static_cast<const float*>(m->gnrm.ptr), sample,
+                             static_cast<float*>(m->gest.ptr), nullptr, nullptr, nullptr, stream);
+            cudaEventRecord(ev[2], st);
+            if (s != PM_OK) break;
+            cudaEventSynchronize(ev[2]);
+            cudaEventElapsedTime(&tb, ev[0], ev[1]);
+            cudaEventElapsedTime(&tq, ev[1], ev[2]);
+        }
+        if (s != PM_OK) break;
+        const float score = tb + (float)(tq * scale);
+        if (score < best_score) { best_score = score; best_c = c; best_b = tb; best_q = (float)(tq * scale); }
+    }
+    for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+    buf_free(m, spos);
+    if (s != PM_OK) {
+        m->leaf_size = saved_leaf; m->warps_per_block = saved[0]; m->rounds_per_chunk = saved[1];
+        m->queries_per_warp = saved[2]; m->kbuf_layout = saved[3];
+        return s;
+    }
+    m->leaf_size = best_c.leaf; m->warps_per_block = best_c.wpb; m->rounds_per_chunk = best_c.rounds;
+    m->queries_per_warp = best_c.qpw; m->kbuf_layout = best_c.layout;
+    best->leaf_size = best_c.leaf; best->warps_per_block = best_c.wpb; best->rounds_per_chunk = best_c.rounds;
+    best->queries_per_warp = best_c.qpw; best->kbuf_layout = best_c.layout;
+    best->build_ms = best_b; best->query_ms = best_q;
+    // leave the map built with the chosen leaf size
+    return pm_build(m, d_pos4, d_pow4, n, format, stream);
+}
+
+extern "C" pm_status pm_batch_autotune(pm_batch* b, const float* d_pos4, const float* d_pow4,
+                                       const uint32_t* photon_offsets, uint32_t num_maps, int format,
+                                       const pm_query_desc* descs, const float* d_qpos4, const float* d_qnrm4,
+                                       const uint32_t* query_offsets, float* d_rad4, pm_tuning* best, void* stream) {
+    if (!b) return PM_ERR_INVALID;
+    if (!best) return batch_fail(b, PM_ERR_INVALID, "best is NULL");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return batch_fail(b, PM_ERR_STATE, "pm_batch_autotune cannot run inside a stream capture");
+    pm_map* m = b->m;
+    cudaEvent_t ev[3];
+    for (cudaEvent_t& e : ev) cudaEventCreate(&e);
+    const uint32_t saved_leaf = m->leaf_size;
+    const int saved_wpb = m->warps_per_block, saved_rounds = m->rounds_per_chunk;
+    float best_score = INFINITY, best_b = 0, best_q = 0;
+    uint32_t bl = saved_leaf;
+    int bw = saved_wpb, br = saved_rounds;
+    pm_status s = PM_OK;
+    const uint32_t leaves[] = {16, 24, 32};
+    const int wpbs[] = {2, 4, 8};
+    const int rounds[] = {8, 32};
+    for (uint32_t l : leaves)
+        for (int w : wpbs)
+            for (int r : rounds) {
+                m->leaf_size = l; m->warps_per_block = w; m->rounds_per_chunk = r;
+                m->queries_per_warp = 1; m->kbuf_layout = PM_KBUF_GROUP;
+                float tb = 0, tq = 0;
+                for (int rep = 0; rep < 2 && s == PM_OK; ++rep) {
+                    cudaEventRecord(ev[0], st);
+                    s = pm_batch_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format, stream);
+                    cudaEventRecord(ev[1], st);
+                    if (s == PM_OK)
+                        s = pm_batch_query(b, descs, d_qpos4, d_qnrm4, query_offsets, d_rad4, nullptr, nullptr, nullptr,
+                                           stream);
+                    cudaEventRecord(ev[2], st);
+                    cudaEventSynchronize(ev[2]);
+                    cudaEventElapsedTime(&tb, ev[0], ev[1]);
+                    cudaEventElapsedTime(&tq, ev[1], ev[2]);
+                }
+                if (s != PM_OK) break;
+                if (tb + tq < best_score) { best_score = tb + tq; bl = l; bw = w; br = r; best_b = tb; best_q = tq; }
+            }
+    for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+    m->leaf_size = s == PM_OK ? bl : saved_leaf;
+    m->warps_per_block = s == PM_OK ? bw : saved_wpb;
+    m->rounds_per_chunk = s == PM_OK ? br : saved_rounds;
+    m->queries_per_warp = 1;
+    m->kbuf_layout = PM_KBUF_GROUP;
+    if (s != PM_OK) return s;
+    best->leaf_size = bl; best->warps_per_block = bw; best->rounds_per_chunk = br;
+    best->queries_per_warp = 1; best->kbuf_layout = PM_KBUF_GROUP;
+    best->build_ms = best_b; best->query_ms = best_q;
+    return pm_batch_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format, stream);
+}

@@ -111,6 +111,21 @@ class PhotonMap:
         L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk, queries_per_warp,
                                         kbuf_layout), self._h)
 
+    def autotune(self, positions: torch.Tensor, powers: torch.Tensor, qpos: torch.Tensor, qnrm: torch.Tensor,
+                 max_sample: int = 0, packed: bool = True, stream=None, **kw) -> L.Tuning:
+        """Picks leaf size, warps per block, rounds per chunk, queries per warp
+        and k-buffer layout by timing build + query on a sample of the queries;
+        the map is left built with the choice."""
+        d = self.desc(**kw)
+        best = L.Tuning()
+        n = int(positions.shape[0])
+        fmt = L.PM_PHOTONS_PACKED if packed else L.PM_PHOTONS_REFERENCE
+        L.check(self._lib.pm_autotune(self._h, _ptr(positions), _ptr(powers), n, fmt, C.byref(d), _ptr(qpos),
+                                      _ptr(qnrm), int(qpos.shape[0]), int(max_sample), C.byref(best),
+                                      _stream(stream)), self._h)
+        self.num_photons = n
+        return best
+
     def reserve(self, max_photons: int, max_queries: int) -> None:
         L.check(self._lib.pm_reserve(self._h, int(max_photons), int(max_queries)), self._h)
 

@@ -239,3 +239,19 @@ def test_engine_reproduces_ingest_golden(cuda):
     _, tpos, tpow = pm.export_tree()
     order = tpos[:, 3].view(np.uint32)
     assert np.array_equal(tpow[:, 3].view(np.uint32), bits[order])
+
+
+def test_autotune_keeps_results_exact(cuda, oracle_mod):
+    """pm_autotune picks a setting from its grid, leaves the map built with it,
+    and the query results stay bit-exact against the oracle."""
+    ph = gen.photons(80000, seed=140, caustic_frac=0.2)
+    q = gen.queries(20000, seed=141)
+    pm = PhotonMap(ph.n, global_q_radius_max=0.05)
+    d_pos, d_pow, d_qp, d_qn = (to_dev(x, cuda) for x in (ph.pos, ph.pow, q.pos, q.nrm))
+    t = pm.autotune(d_pos, d_pow, d_qp, d_qn, max_sample=4096, k=64, r_max=0.05, filter="cone")
+    assert t.leaf_size in (16, 24, 32) and t.warps_per_block in (2, 4, 8) and t.rounds_per_chunk in (8, 32)
+    assert t.queries_per_warp in (1, 2) and t.kbuf_layout in (0, 1) and t.query_ms > 0
+    out = pm.query(d_qp, d_qn, want_nbr=True, k=64, r_max=0.05, filter="cone")
+    torch.cuda.synchronize()
+    res = {kk: v.cpu().numpy() for kk, v in out.items()}
+    check_against_oracle(oracle_mod, ph, q, res, 64, 0.05, "cone")
