@@ -53,6 +53,12 @@ struct pm_map {
     DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, qr2, qcnt, seg_start, seg_end, acc;
     DevBuf rnbr, rcnt, rr2, rrad;
     DevBuf gnrm, gest;        // pm_gather_for: flipped normals, estimates
+    // PM_MODE_ZHOU_COMPAT: node radius estimates of the current tree, kept
+    // for one (k, R, refinement rounds) until the next build
+    DevBuf compat_est;
+    uint64_t build_gen = 0, compat_gen = ~0ull;
+    uint32_t compat_k = 0, compat_iters = 0;
+    float compat_r = 0.0f;
     uint64_t cap_pairs = 0;
     uint32_t cap_bq = 0, cap_bn = 0, cap_rq = 0;
     uint32_t bwd_chunk = 0;   // max queries per backward chunk (0 = automatic)
@@ -280,7 +286,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
-                     &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest};
+                     &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -358,6 +364,7 @@ pm_status pm_build(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t
     if (s != PM_OK) return s;
     m->n = n;
     m->built = true;
+    ++m->build_gen;
     return PM_OK;
 }
 
@@ -374,14 +381,40 @@ static pm_status query_common(pm_map* m, const pm_query_desc* desc, const float*
     return PM_OK;
 }
 
+static pm_status compat_run(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                            uint32_t nq, float* d_radius, float* d_rad4, float* d_r2, uint32_t* d_count, cudaStream_t st) {
+    if (nq == 0) return PM_OK;
+    const uint32_t iters = desc->refine_iters;
+    if (iters > 64) return fail(m, PM_ERR_INVALID, "refine_iters must be at most 64");
+    const uint32_t max_slots = 2 * (m->cap_photons + 1);
+    if (m->compat_gen != m->build_gen || m->compat_k != desc->k || m->compat_r != desc->r_max ||
+        m->compat_iters != iters) {
+        if (m->compat_est.bytes < (size_t)max_slots * sizeof(float)) {
+            if (capturing(st)) return fail(m, PM_ERR_STATE, "compat storage must grow during stream capture");
+            pm_status s = buf_ensure(m, m->compat_est, (size_t)max_slots * sizeof(float), "compat node estimates");
+            if (s != PM_OK) return s;
+        }
+        m->launches += (uint64_t)compat_node_estimates(view_of(m), max_slots, desc->r_max, desc->k, iters,
+                                                       P<float>(m->compat_est), st);
+        m->compat_gen = m->build_gen; m->compat_k = desc->k; m->compat_r = desc->r_max; m->compat_iters = iters;
+    }
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), nullptr, d_r2, d_count};
+    m->launches += (uint64_t)compat_query(view_of(m), P<float>(m->compat_est), params_of(desc), iters,
+                                          reinterpret_cast<const float4*>(d_qpos4),
+                                          reinterpret_cast<const float4*>(d_qnrm4), nq, d_radius, out, st);
+    return check_cuda(m, "PM_MODE_ZHOU_COMPAT");
+}
+
 pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
                    float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, void* stream) {
     pm_status s = query_common(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, false);
     if (s != PM_OK) return s;
-    if (desc->mode == PM_MODE_ZHOU_COMPAT)
-        return fail(m, PM_ERR_UNSUPPORTED, "PM_MODE_ZHOU_COMPAT is not available in this build");
-    if (nq == 0) return PM_OK;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (desc->mode == PM_MODE_ZHOU_COMPAT) {
+        if (d_nbr) return fail(m, PM_ERR_INVALID, "PM_MODE_ZHOU_COMPAT returns no neighbour lists (d_nbr must be NULL)");
+        return compat_run(m, desc, d_qpos4, d_qnrm4, nq, nullptr, d_rad4, d_r2, d_count, st);
+    }
+    if (nq == 0) return PM_OK;
     s = ensure_query_capacity(m, nq, st);
     if (s != PM_OK) return s;
     const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
@@ -587,8 +620,14 @@ pm_status pm_scale_flux(pm_map* m, float scale, void* stream) {
 
 pm_status pm_compute_query_radii(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, uint32_t nq,
                                  float* d_radii, void* stream) {
-    (void)desc; (void)d_qpos4; (void)nq; (void)d_radii; (void)stream;
-    return fail(m, PM_ERR_UNSUPPORTED, "pm_compute_query_radii is not available in this build");
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = validate_desc(m, desc, false);
+    if (s != PM_OK) return s;
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (nq > 0 && (!d_qpos4 || !d_radii)) return fail(m, PM_ERR_INVALID, "query positions and radii must be non-NULL");
+    if (nq > 0 && !aligned16(d_qpos4)) return fail(m, PM_ERR_INVALID, "query positions must be 16-byte aligned");
+    return compat_run(m, desc, d_qpos4, d_qpos4, nq, d_radii, nullptr, nullptr, nullptr,
+                      reinterpret_cast<cudaStream_t>(stream));
 }
 
 pm_status pm_get_info(pm_map* m, pm_map_info* info, void* stream) {

@@ -125,6 +125,12 @@ int batch_roots(const uint32_t* ph_off, uint32_t m, uint32_t n, uint32_t leaf_si
                 const Node* nodes, const BuildBuffers& bb, BatchGeom* geom, cudaStream_t st);
 int map_id_bits(uint32_t m);
 
+// pm_compat.cu
+int compat_node_estimates(const MapView& m, uint32_t max_slots, float rmax, uint32_t k, uint32_t iters, float* est,
+                          cudaStream_t st);
+int compat_query(const MapView& m, const float* est, const QueryParams& p, uint32_t iters, const float4* qpos,
+                 const float4* qnrm, uint32_t nq, float* out_radius, const QueryOutputs& out, cudaStream_t st);
+
 // pm_gather.cu
 int gather_normals(const float4* hit_nrm, const float4* ray_dir, uint32_t n, float4* out_nrm, cudaStream_t st);
 int gather_accumulate(const float4* est, const float4* hit_pos, const float4* ray_origin, const float4* influence,

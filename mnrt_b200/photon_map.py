@@ -267,3 +267,16 @@ class PhotonMap:
         within 5 % of the global radius, white, no photon-count rule."""
         self.gather_for(sp, rays, None, None, io_radiance, None, stream=stream, k=1, r_max=0.05 * self.r_max,
                         min_found=0)
+
+    def compute_query_radii(self, qpos: torch.Tensor, out: torch.Tensor | None = None, stream=None,
+                            **kw) -> torch.Tensor:
+        """KDTreePoint::ComputeQueryRadii (KDTreePoint.cpp:229-248): the
+        reference's histogram-refined query radius per point (ZHOU_COMPAT)."""
+        kw.setdefault("mode", L.PM_MODE_ZHOU_COMPAT)
+        d = self.desc(**kw)
+        nq = int(qpos.shape[0])
+        if out is None:
+            out = torch.empty((nq,), dtype=torch.float32, device=qpos.device)
+        L.check(self._lib.pm_compute_query_radii(self._h, C.byref(d), _ptr(qpos), nq, _ptr(out), _stream(stream)),
+                self._h)
+        return out

@@ -50,6 +50,7 @@ def load() -> C.CDLL:
         "orc_kdtree_free": (None, [P]),
         "orc_knn_kdtree": (None, [P, P, u32, u32, f32, P, P, P, P, i32]),
         "orc_radiance_fp64": (None, [P, P, P, P, u32, P, P, u32, f32, i32, f32, u32, P, i32]),
+        "orc_compat": (None, [P, u32, P, P, P, P, u32, u32, f32, u32, i32, f32, u32, P, P, P, P, i32]),
         "orc_backward_fp64": (None, [P, P, P, P, u32, u32, P, P, u32, f32, i32, f32, u32, P, P, P]),
     }
     for name, (res, args) in sig.items():
@@ -145,6 +146,23 @@ def backward_fp64(pos4, pow4, q4, n4, nbr, count, k: int, r_max: float, grad, fi
                           count.ctypes.data, k, r_max, FILTER_IDS[filt], cone_k, min_found, grad.ctypes.data,
                           gp.ctypes.data, gx.ctypes.data)
     return gp, gx
+
+
+def compat(nodes, tpos4, tpow4, q4, n4, k: int, r_max: float, iters: int = 2, filt: str = "box",
+           cone_k: float = 1.0, min_found: int = 0, threads: int = 0):
+    """ZHOU_COMPAT answer on an exported tree: (radius, count, r2_used, rad (nq, 3) FP64)."""
+    lib = load()
+    nodes = _c(nodes, np.uint32)
+    tpos4, tpow4, q4, n4 = (_c(a, np.float32) for a in (tpos4, tpow4, q4, n4))
+    nq = q4.shape[0]
+    radius = np.empty(nq, np.float32)
+    count = np.empty(nq, np.uint32)
+    r2 = np.empty(nq, np.float32)
+    rad = np.empty((nq, 3), np.float64)
+    lib.orc_compat(nodes.ctypes.data, nodes.shape[0] - 1, tpos4.ctypes.data, tpow4.ctypes.data, q4.ctypes.data,
+                   n4.ctypes.data, nq, k, r_max, iters, FILTER_IDS[filt], cone_k, min_found, radius.ctypes.data,
+                   count.ctypes.data, r2.ctypes.data, rad.ctypes.data, threads)
+    return radius, count, r2, rad
 
 
 def threads_available() -> int:

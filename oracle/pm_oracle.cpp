@@ -485,3 +485,174 @@ void orc_backward_fp64(const float* pos4, const float* pow4, const float* q4, co
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ ZHOU_COMPAT mode --
+// The reference's radius pipeline restated on the engine's exported tree
+// (nodes: 16 uint32 each = two slots {lo[3], hi[3], ref, cnt}; tree-order
+// photons).  Follows KDTreePoint::PrecomputeQueryRadii / ComputeQueryRadii
+// (KDTreePoint.cpp:187-248), dev_RefineQueryRadiusZhou / dev_RangeSearchHist
+// (GPU/kdtree_point.cu:118-267), kernel_QREEstimateRadii (:453-504) and the
+// gather of dev_RangeSearch (GPU/photon_knn.cu:113-235), with the engine's
+// stated choices: slots are the tree nodes, the root-to-leaf path follows the
+// nearer child box, FP32 steps in a fixed order, histogram index clamped to 31.
+namespace {
+
+struct CSlot { float lo[3], hi[3]; uint32_t ref, cnt; };
+
+struct CompatTree {
+    const uint32_t* nodes; uint32_t m;   // internal nodes 1..m, node 0 = super-root
+    const float* pos; const float* pow;
+    CSlot slot(uint32_t sid) const {
+        const uint32_t* w = nodes + 16 * (size_t)(sid >> 1) + 8 * (sid & 1u);
+        CSlot s;
+        for (int a = 0; a < 3; ++a) { s.lo[a] = u2f(w[a]); s.hi[a] = u2f(w[3 + a]); }
+        s.ref = w[6]; s.cnt = w[7];
+        return s;
+    }
+};
+
+inline float box_lb_f32(float qx, float qy, float qz, const float* lo, const float* hi) {
+    const float q[3] = {qx, qy, qz};
+    float g[3];
+    for (int a = 0; a < 3; ++a) {
+        float x = std::max(lo[a] - q[a], q[a] - hi[a]);
+        g[a] = std::max(x, 0.0f);
+    }
+    float s = g[0] * g[0] + g[1] * g[1];
+    return s + g[2] * g[2];
+}
+
+template <class F>
+void compat_range(const CompatTree& t, float qx, float qy, float qz, float r2, F&& f) {
+    std::vector<uint32_t> stack;
+    stack.push_back(0u);
+    while (!stack.empty()) {
+        const uint32_t sid = stack.back();
+        stack.pop_back();
+        const CSlot s = t.slot(sid);
+        if (s.ref == 0xffffffffu) continue;
+        if (!(box_lb_f32(qx, qy, qz, s.lo, s.hi) < r2)) continue;
+        if (s.cnt > 0) {
+            for (uint32_t j = 0; j < s.cnt; ++j) {
+                const float* p = t.pos + 4 * (size_t)(s.ref + j);
+                const float d2 = d2_f32(qx, qy, qz, p[0], p[1], p[2]);
+                if (d2 < r2) f(s.ref + j, d2);
+            }
+        } else {
+            stack.push_back((s.ref << 1) | 1u);
+            stack.push_back(s.ref << 1);
+        }
+    }
+}
+
+float compat_refine(const CompatTree& t, float qx, float qy, float qz, float radius_max, uint32_t k, uint32_t iters) {
+    float r_min = 0.0f, r_max = radius_max;
+    for (uint32_t it = 0; it < iters; ++it) {
+        const float r = r_max;
+        const float delta = r_max - r_min;
+        if (!(delta > 0.0f)) break;
+        uint32_t hist[32] = {0};
+        compat_range(t, qx, qy, qz, r * r, [&](uint32_t, float d2) {
+            const float d = std::sqrt(d2);
+            const float fi = (std::max(d - r_min, 0.0f) * 32.0f) / delta;
+            uint32_t idx = (uint32_t)fi;
+            if (idx > 31) idx = 31;
+            if (hist[idx] < 0xfffeu) ++hist[idx];
+        });
+        uint32_t m = 31, sum = 0;
+        for (uint32_t j = 0; j < 32; ++j) {
+            sum += hist[j];
+            if (sum >= k) { m = j; break; }
+        }
+        const float inv = 1.0f / 32.0f;
+        const float old = r_min;
+        r_min = old + ((float)m * delta) * inv;
+        r_max = old + ((float)(m + 1) * delta) * inv;
+    }
+    return r_max;
+}
+
+void compat_extent(const CSlot& s, float* c, float& rad) {
+    float d2 = 0.0f;
+    for (int a = 0; a < 3; ++a) {
+        c[a] = (s.lo[a] + s.hi[a]) * 0.5f;
+        const float e = s.hi[a] - s.lo[a];
+        d2 = a == 0 ? e * e : d2 + e * e;
+    }
+    rad = std::sqrt(d2) * 0.5f;
+}
+
+}  // namespace
+
+extern "C" {
+
+// radius (nq), count (nq), r2_used (nq), rad (3 nq doubles; NULL = radii only)
+void orc_compat(const uint32_t* nodes, uint32_t m, const float* tpos4, const float* tpow4, const float* q4,
+                const float* n4, uint32_t nq, uint32_t k, float R, uint32_t iters, int filter, float cone_k,
+                uint32_t min_found, float* out_radius, uint32_t* out_count, float* out_r2, double* out_rad,
+                int nthreads) {
+    CompatTree t{nodes, m, tpos4, tpow4};
+    const uint32_t nslots = 2 * (m + 1);
+    std::vector<float> est(nslots, INFINITY);
+    const bool enabled = 2 * m + 1 >= 1000;
+    parallel_for_blocks(nslots, 64, nthreads, [&](int64_t b, int64_t e) {
+        for (int64_t sid = b; sid < e; ++sid) {
+            const CSlot s = t.slot((uint32_t)sid);
+            if (!enabled || s.ref == 0xffffffffu) continue;
+            float c[3], rad;
+            compat_extent(s, c, rad);
+            if (rad <= 0.5f * R) est[sid] = compat_refine(t, c[0], c[1], c[2], R, k, iters);
+        }
+    });
+    parallel_for_blocks(nq, 64, nthreads, [&](int64_t b, int64_t e) {
+        for (int64_t q = b; q < e; ++q) {
+            const float qx = q4[4 * q], qy = q4[4 * q + 1], qz = q4[4 * q + 2];
+            float est_q = R;
+            uint32_t sid = 0;
+            for (int depth = 0; depth < 4096; ++depth) {
+                const CSlot s = t.slot(sid);
+                if (s.ref == 0xffffffffu) break;
+                float c[3], rad;
+                compat_extent(s, c, rad);
+                const float len = std::sqrt(d2_f32(qx, qy, qz, c[0], c[1], c[2]));
+                est_q = std::min(est_q, len + est[sid]);
+                if (s.cnt > 0) break;
+                const CSlot s0 = t.slot(s.ref << 1), s1 = t.slot((s.ref << 1) | 1u);
+                const float b0 = s0.ref == 0xffffffffu ? INFINITY : box_lb_f32(qx, qy, qz, s0.lo, s0.hi);
+                const float b1 = s1.ref == 0xffffffffu ? INFINITY : box_lb_f32(qx, qy, qz, s1.lo, s1.hi);
+                sid = (s.ref << 1) | (b1 < b0 ? 1u : 0u);
+            }
+            const float r = compat_refine(t, qx, qy, qz, est_q, k, iters);
+            out_radius[q] = r;
+            if (!out_rad) continue;
+            const float r2 = r * r;
+            uint32_t count = 0;
+            float maxd2 = 0.0f;
+            compat_range(t, qx, qy, qz, r2, [&](uint32_t, float d2) { ++count; maxd2 = std::max(maxd2, d2); });
+            const float r2u = count >= k ? maxd2 : r2;
+            out_count[q] = count;
+            out_r2[q] = r2u;
+            double acc[3] = {0, 0, 0};
+            if (count > 0 && count >= min_found && r2u > 0.0f) {
+                const double r2d = r2u, kc = cone_k;
+                compat_range(t, qx, qy, qz, r2, [&](uint32_t i, float) {
+                    if (!front_f32(n4[4 * q], n4[4 * q + 1], n4[4 * q + 2], f2u(tpow4[4 * (size_t)i + 3]))) return;
+                    const double dx = (double)tpos4[4 * (size_t)i] - qx, dy = (double)tpos4[4 * (size_t)i + 1] - qy,
+                                 dz = (double)tpos4[4 * (size_t)i + 2] - qz;
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    double w = 1.0;
+                    if (filter == 1) w = 1.0 - std::sqrt(d2) / (kc * std::sqrt(r2d));
+                    else if (filter == 2) w = 1.0 - d2 / r2d;
+                    for (int c = 0; c < 3; ++c) acc[c] += w * (double)tpow4[4 * (size_t)i + c];
+                });
+                double norm = 1.0 / (kPi * r2d);
+                if (filter == 1) norm = 1.0 / ((1.0 - 2.0 / (3.0 * kc)) * kPi * r2d);
+                else if (filter == 2) norm = 2.0 / (kPi * r2d);
+                for (int c = 0; c < 3; ++c) acc[c] *= norm;
+            }
+            for (int c = 0; c < 3; ++c) out_rad[3 * q + c] = acc[c];
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+"""PM_MODE_ZHOU_COMPAT and pm_compute_query_radii against the oracle's
+restatement of the reference's radius pipeline on the same (exported) tree:
+radii, photon counts and r^2 bit-exact; radiance within 1e-5 of FP64."""
+import numpy as np
+import pytest
+import torch
+
+from mnrt_b200 import gen
+from mnrt_b200 import _lib as L
+from mnrt_b200.photon_map import PhotonMap
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+@pytest.mark.parametrize("n,nq,k,r,iters,filt,leaf", [
+    (3000, 800, 20, 0.2, 2, "box", 16),          # small tree: node estimates skipped (< 1000 slots)
+    (60000, 3000, 50, 0.1, 2, "box", 16),        # node estimates on
+    (60000, 3000, 100, 0.05, 3, "cone", 32),
+    (30000, 2000, 16, 0.05, 1, "epanechnikov", 8),
+])
+def test_compat_matches_oracle(cuda, oracle_mod, n, nq, k, r, iters, filt, leaf):
+    ph = gen.photons(n, seed=500 + n, caustic_frac=0.2)
+    q = gen.queries(nq, seed=501)
+    pm = PhotonMap(n, global_q_radius_max=r, knn_target_count=k)
+    pm.set_tuning(leaf_size=leaf)
+    pm.build(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda))
+    qp, qn = to_dev(q.pos, cuda), to_dev(q.nrm, cuda)
+    out = pm.query(qp, qn, mode=L.PM_MODE_ZHOU_COMPAT, refine_iters=iters, filter=filt, min_found=8)
+    radii = pm.compute_query_radii(qp, refine_iters=iters)
+    torch.cuda.synchronize()
+    nodes, tpos, tpow = pm.export_tree()
+    o_radius, o_count, o_r2, o_rad = oracle_mod.compat(nodes, tpos, tpow, q.pos, q.nrm, k, r, iters, filt, 1.0, 8)
+    assert np.array_equal(radii.cpu().numpy(), o_radius)
+    assert np.array_equal(out["count"].cpu().numpy().view(np.uint32), o_count)
+    assert np.array_equal(out["r2"].cpu().numpy(), o_r2)
+    got = out["rad"].cpu().numpy()
+    floor = 1e-6 * max(np.abs(o_rad).mean(), 1e-30)
+    rel = np.abs(got[:, :3] - o_rad) / np.maximum(np.abs(o_rad), floor)
+    assert rel.max() <= 1e-5, rel.max()
+    assert (o_count >= 0).all() and (o_radius <= np.float32(r)).all()
+    assert pm.info().device_errors == 0
+    # roughly k photons inside the refined radius (the reference's intent)
+    med = np.median(o_count)
+    assert 0.5 * k <= med <= 3 * k, med
+
+
+def test_compat_rejects_neighbour_lists(cuda):
+    ph = gen.photons(2000, seed=1)
+    q = gen.queries(10, seed=2)
+    pm = PhotonMap(ph.n, global_q_radius_max=0.1)
+    pm.build(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda))
+    with pytest.raises(L.PMError):
+        pm.query(to_dev(q.pos, cuda), to_dev(q.nrm, cuda), want_nbr=True, mode=L.PM_MODE_ZHOU_COMPAT)
