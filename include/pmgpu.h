@@ -156,6 +156,20 @@ PM_API pm_status pm_reserve(pm_map* map, uint32_t max_photons, uint32_t max_quer
 PM_API pm_status pm_build(pm_map* map, const float* d_pos4, const float* d_pow4, uint32_t n, int format,
                    void* stream);
 
+/* PhotonMap::Merge (PhotonMap.cpp:181-184, PhotonData::Merge
+ * KernelDefs.cpp:363-384): appends the photons i with d_is_valid[i] != 0
+ * (NULL = all) to the map's merged photon store, in order; *merged gets the
+ * count.  Synchronous, like the reference (it returns the count).  Exceeding
+ * max_photons is an error (the reference aborts). */
+PM_API pm_status pm_merge(pm_map* map, const float* d_pos4, const float* d_pow4, const uint32_t* d_is_valid, uint32_t n,
+                          uint32_t* merged, void* stream);
+/* PhotonMap::BuildMap (PhotonMap.cpp:157) over the merged store (pm_build
+ * of those photons). */
+PM_API pm_status pm_build_merged(pm_map* map, int format, void* stream);
+/* PhotonData::Clear (KernelDefs.cpp:333-337): empties the merged store. */
+PM_API pm_status pm_clear_merged(pm_map* map);
+PM_API pm_status pm_merged_count(const pm_map* map, uint32_t* count);
+
 /* Exact-kNN radiance estimate (the kernel_PhotonGather / dev_RangeSearch path,
  * GPU/photon_knn.cu:113-235,487-552, with exact k-nearest semantics).
  *   d_qpos4, d_qnrm4: query positions and normals (float4, w ignored), nq each.
@@ -241,7 +255,8 @@ PM_API pm_status pm_gather_for(pm_map* map, const pm_query_desc* desc, const flo
                         uint32_t n, float* d_io_radiance4, float* d_io_recip_dist, void* stream);
 
 /* PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): scales the RGB flux of the
- * built map in place (direction bits untouched). */
+ * photons the map holds -- the built tree and the merged store -- in place
+ * (direction bits untouched). */
 PM_API pm_status pm_scale_flux(pm_map* map, float scale, void* stream);
 
 /* KDTreePoint::ComputeQueryRadii (KDTreePoint.cpp:229-248) in ZHOU_COMPAT

@@ -69,6 +69,10 @@ SIGNATURES = {
     "pm_set_backward_chunk": (_I, [_VP, _U32]),
     "pm_gather_for": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _FP, _FP, _FP, _FP, _UP, _U32, _FP, _FP, _VP]),
     "pm_scale_flux": (_I, [_VP, _F, _VP]),
+    "pm_merge": (_I, [_VP, _FP, _FP, _UP, _U32, C.POINTER(C.c_uint32), _VP]),
+    "pm_build_merged": (_I, [_VP, _I, _VP]),
+    "pm_clear_merged": (_I, [_VP]),
+    "pm_merged_count": (_I, [_VP, C.POINTER(C.c_uint32)]),
     "pm_compute_query_radii": (_I, [_VP, C.POINTER(QueryDesc), _FP, _U32, _FP, _VP]),
     "pm_get_info": (_I, [_VP, C.POINTER(MapInfo), _VP]),
     "pm_set_profiling": (_I, [_VP, _I]),

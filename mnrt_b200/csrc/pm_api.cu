@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -56,6 +57,9 @@ struct pm_map {
     // PM_MODE_ZHOU_COMPAT: node radius estimates of the current tree, kept
     // for one (k, R, refinement rounds) until the next build
     DevBuf compat_est;
+    // photons merged by pm_merge, built by pm_build_merged (PhotonData of the reference)
+    DevBuf mpos, mpow, mflags, mrank, mscan;
+    uint32_t merged_n = 0, cap_merged = 0;
     uint64_t build_gen = 0, compat_gen = ~0ull;
     uint32_t compat_k = 0, compat_iters = 0;
     float compat_r = 0.0f;
@@ -286,7 +290,8 @@ pm_status pm_destroy(pm_map* m) {
                      &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
-                     &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est};
+                     &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
+                     &m->mrank, &m->mscan};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -612,9 +617,14 @@ pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit
 pm_status pm_scale_flux(pm_map* m, float scale, void* stream) {
     if (!m) return PM_ERR_INVALID;
     if (!std::isfinite(scale)) return fail(m, PM_ERR_INVALID, "scale must be finite");
-    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (!m->built && m->merged_n == 0) return fail(m, PM_ERR_STATE, "no photons to scale (nothing merged or built)");
+    if (!m->built) {
+        m->launches += (uint64_t)scale_rgb(P<float4>(m->mpow), m->merged_n, scale, reinterpret_cast<cudaStream_t>(stream));
+        return check_cuda(m, "pm_scale_flux");
+    }
     scale_flux(P<float4>(m->pow), m->n, scale, P<MapHeader>(m->hdr), reinterpret_cast<cudaStream_t>(stream));
     m->launches += 1;
+    m->launches += (uint64_t)scale_rgb(P<float4>(m->mpow), m->merged_n, scale, reinterpret_cast<cudaStream_t>(stream));
     return check_cuda(m, "pm_scale_flux");
 }
 
@@ -1271,4 +1281,75 @@ extern "C" pm_status pm_batch_autotune(pm_batch* b, const float* d_pos4, const f
     best->queries_per_warp = 1; best->kbuf_layout = PM_KBUF_GROUP;
     best->build_ms = best_b; best->query_ms = best_q;
     return pm_batch_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Photon ingest: PhotonMap::Merge (PhotonMap.cpp:181-184) over
+// PhotonData::Merge (KernelDefs.cpp:363-384).
+extern "C" pm_status pm_merge(pm_map* m, const float* d_pos4, const float* d_pow4, const uint32_t* d_is_valid,
+                              uint32_t n, uint32_t* merged, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (merged) *merged = 0;
+    if (n == 0) return PM_OK;
+    if (!d_pos4 || !d_pow4) return fail(m, PM_ERR_INVALID, "photon arrays must be non-NULL");
+    if (!aligned16(d_pos4) || !aligned16(d_pow4)) return fail(m, PM_ERR_INVALID, "photon arrays must be 16-byte aligned");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return fail(m, PM_ERR_STATE, "pm_merge is synchronous and cannot be captured");
+    pm_status s;
+    if ((s = buf_ensure(m, m->mflags, (size_t)n * sizeof(uint32_t), "merge flags")) != PM_OK) return s;
+    if ((s = buf_ensure(m, m->mrank, (size_t)n * sizeof(uint32_t), "merge ranks")) != PM_OK) return s;
+    if ((s = buf_ensure(m, m->mscan, (scan_scratch_words(n) + 1) * sizeof(uint32_t), "merge scan")) != PM_OK) return s;
+    uint32_t* total = P<uint32_t>(m->mscan);
+    int nl = merge_ranks(d_is_valid, n, P<uint32_t>(m->mflags), P<uint32_t>(m->mrank), total + 1, total, st);
+    uint32_t count = 0;
+    if (cudaMemcpyAsync(&count, total, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return check_cuda(m, "pm_merge");
+    const uint64_t need = (uint64_t)m->merged_n + count;
+    if (m->max_photons && need > m->max_photons)
+        return fail(m, PM_ERR_INVALID, "merging %u photons exceeds the map's max_photons = %u", count, m->max_photons);
+    if (need > 0x7fffffffull) return fail(m, PM_ERR_UNSUPPORTED, "more than 2^31 - 1 photons");
+    if (need > m->cap_merged) {   // grow, keeping what is merged already
+        const uint32_t cap = (uint32_t)std::max<uint64_t>(need, m->max_photons ? m->max_photons : need);
+        DevBuf np, nw;
+        if ((s = buf_ensure(m, np, (size_t)cap * sizeof(float4), "merged positions")) != PM_OK) return s;
+        if ((s = buf_ensure(m, nw, (size_t)cap * sizeof(float4), "merged powers")) != PM_OK) { buf_free(m, np); return s; }
+        if (m->merged_n) {
+            cudaMemcpyAsync(np.ptr, m->mpos.ptr, (size_t)m->merged_n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(nw.ptr, m->mpow.ptr, (size_t)m->merged_n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+            cudaStreamSynchronize(st);
+        }
+        buf_free(m, m->mpos);
+        buf_free(m, m->mpow);
+        m->mpos = np;
+        m->mpow = nw;
+        m->cap_merged = cap;
+    }
+    if (count) {
+        nl += merge_scatter(reinterpret_cast<const float4*>(d_pos4), reinterpret_cast<const float4*>(d_pow4),
+                            P<uint32_t>(m->mflags), P<uint32_t>(m->mrank), n, P<float4>(m->mpos) + m->merged_n,
+                            P<float4>(m->mpow) + m->merged_n, st);
+    }
+    m->merged_n += count;
+    m->launches += (uint64_t)nl;
+    if (merged) *merged = count;
+    return check_cuda(m, "pm_merge");
+}
+
+extern "C" pm_status pm_build_merged(pm_map* m, int format, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    return pm_build(m, m->merged_n ? static_cast<const float*>(m->mpos.ptr) : nullptr,
+                    m->merged_n ? static_cast<const float*>(m->mpow.ptr) : nullptr, m->merged_n, format, stream);
+}
+
+extern "C" pm_status pm_clear_merged(pm_map* m) {
+    if (!m) return PM_ERR_INVALID;
+    m->merged_n = 0;
+    return PM_OK;
+}
+
+extern "C" pm_status pm_merged_count(const pm_map* m, uint32_t* count) {
+    if (!m || !count) return PM_ERR_INVALID;
+    *count = m->merged_n;
+    return PM_OK;
 }

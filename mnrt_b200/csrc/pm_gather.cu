@@ -74,3 +74,56 @@ int gather_accumulate(const float4* est, const float4* hit_pos, const float4* ra
 }
 
 }  // namespace pm
+
+// ---- photon ingest: PhotonData::Merge (KernelDefs.cpp:363-384) ----------
+namespace pm {
+
+namespace {
+
+__global__ void k_valid_flags(const uint32_t* __restrict__ is_valid, uint32_t n, uint32_t* __restrict__ flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = (is_valid == nullptr || is_valid[i] != 0u) ? 1u : 0u;
+}
+
+__global__ void k_merge_scatter(const float4* __restrict__ pos, const float4* __restrict__ pw,
+                                const uint32_t* __restrict__ flags, const uint32_t* __restrict__ rank, uint32_t n,
+                                float4* __restrict__ dst_pos, float4* __restrict__ dst_pow) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flags[i]) return;
+    const uint32_t d = rank[i];
+    dst_pos[d] = pos[i];
+    dst_pow[d] = pw[i];
+}
+
+__global__ void k_scale_rgb(float4* __restrict__ pw, uint32_t n, float scale) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 w = pw[i];
+    w.x = __fmul_rn(w.x, scale);
+    w.y = __fmul_rn(w.y, scale);
+    w.z = __fmul_rn(w.z, scale);
+    pw[i] = w;
+}
+
+}  // namespace
+
+// Flags -> exclusive ranks (rank[n] is not written; *total gets the count).
+int merge_ranks(const uint32_t* is_valid, uint32_t n, uint32_t* flags, uint32_t* rank, uint32_t* scan_scratch,
+                uint32_t* total, cudaStream_t st) {
+    k_valid_flags<<<(n + 255) / 256, 256, 0, st>>>(is_valid, n, flags);
+    return 1 + exclusive_scan(flags, rank, n, scan_scratch, total, st);
+}
+
+int merge_scatter(const float4* pos, const float4* pw, const uint32_t* flags, const uint32_t* rank, uint32_t n,
+                  float4* dst_pos, float4* dst_pow, cudaStream_t st) {
+    k_merge_scatter<<<(n + 255) / 256, 256, 0, st>>>(pos, pw, flags, rank, n, dst_pos, dst_pow);
+    return 1;
+}
+
+int scale_rgb(float4* pw, uint32_t n, float scale, cudaStream_t st) {
+    if (!n) return 0;
+    k_scale_rgb<<<(n + 255) / 256, 256, 0, st>>>(pw, n, scale);
+    return 1;
+}
+
+}  // namespace pm

@@ -137,6 +137,12 @@ int gather_accumulate(const float4* est, const float4* hit_pos, const float4* ra
                       const float4* clr_diffuse, const uint32_t* idx_shading, uint32_t n, float4* io_rad,
                       float* io_recip, cudaStream_t st);
 
+int merge_ranks(const uint32_t* is_valid, uint32_t n, uint32_t* flags, uint32_t* rank, uint32_t* scan_scratch,
+                uint32_t* total, cudaStream_t st);
+int merge_scatter(const float4* pos, const float4* pw, const uint32_t* flags, const uint32_t* rank, uint32_t n,
+                  float4* dst_pos, float4* dst_pow, cudaStream_t st);
+int scale_rgb(float4* pw, uint32_t n, float scale, cudaStream_t st);
+
 // pm_backward.cu
 struct BwdArgs {
     const float4* pos;        // tree order

@@ -206,8 +206,11 @@ class PhotonMap:
         return nodes, pos[: self.num_photons], pw[: self.num_photons]
 
     def scale_flux(self, scale: float, stream=None) -> None:
-        """PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): RGB flux only."""
-        if self.num_photons == 0:
+        """PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): RGB flux of the photons
+        held (merged and built), direction bits untouched."""
+        n = C.c_uint32(0)
+        L.check(self._lib.pm_merged_count(self._h, C.byref(n)), self._h)
+        if self.num_photons == 0 and n.value == 0:
             return
         L.check(self._lib.pm_scale_flux(self._h, float(scale), _stream(stream)), self._h)
 
@@ -236,6 +239,30 @@ class PhotonMap:
 
     def set_backward_chunk(self, max_queries: int) -> None:
         L.check(self._lib.pm_set_backward_chunk(self._h, int(max_queries)), self._h)
+
+    # -- reference build entry points ------------------------------------------------
+    def merge(self, other: PhotonData, d_is_valid: torch.Tensor | None = None, stream=None) -> int:
+        """PhotonMap::Merge (PhotonMap.cpp:181): appends the photons of other
+        whose d_is_valid flag is non-zero (all when None); returns the count."""
+        n = other.num_photons
+        merged = C.c_uint32(0)
+        L.check(self._lib.pm_merge(self._h, _ptr(other.positions) if n else None, _ptr(other.powers) if n else None,
+                                   _ptr(d_is_valid), n, C.byref(merged), _stream(stream)), self._h)
+        self._packed = other.packed
+        return int(merged.value)
+
+    def build_map(self, stream=None) -> bool:
+        """PhotonMap::BuildMap (PhotonMap.cpp:157): the tree over the merged photons."""
+        fmt = L.PM_PHOTONS_PACKED if getattr(self, "_packed", False) else L.PM_PHOTONS_REFERENCE
+        L.check(self._lib.pm_build_merged(self._h, fmt, _stream(stream)), self._h)
+        n = C.c_uint32(0)
+        L.check(self._lib.pm_merged_count(self._h, C.byref(n)), self._h)
+        self.num_photons = int(n.value)
+        return True
+
+    def clear(self) -> None:
+        """PhotonData::Clear: drops the merged photons."""
+        L.check(self._lib.pm_clear_merged(self._h), self._h)
 
     # -- reference gather entry points ------------------------------------------------
     def gather_for(self, sp: ShadingPoints, rays: RayChunk, clr_diff_hit: torch.Tensor | None,

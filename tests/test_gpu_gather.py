@@ -116,3 +116,35 @@ def test_gather_normal_flip_and_min_found(cuda, oracle_mod):
     exp_rad, _ = expected(oracle_mod, ph, q, dirs, origins, infl, clr, k, r, 8, "box", io_rad, None,
                           np.arange(q.n))
     assert np.allclose(d_rad.cpu().numpy(), exp_rad, rtol=1e-5, atol=1e-9)
+
+
+def test_merge_scale_build_pipeline(cuda, oracle_mod):
+    """PhotonMap.merge -> scale_flux -> build_map (the reference's build
+    sequence, RTCore.cpp:526-620 -> PhotonMap.cpp:157-193) equals building the
+    valid photons, scaled, directly: same tree order and bit-identical query."""
+    from mnrt_b200.photon_map import PhotonData
+    ph = gen.photons(30000, seed=150, caustic_frac=0.2, layout="reference")
+    valid = (np.arange(ph.n) % 4 != 1).astype(np.uint32) * 3
+    half = ph.n // 2
+    pm = PhotonMap(ph.n, global_q_radius_max=0.06, knn_target_count=40)
+    total = 0
+    for a, b in ((0, half), (half, ph.n)):     # two tracing passes merged in turn
+        total += pm.merge(PhotonData(to_dev(ph.pos[a:b], cuda), to_dev(ph.pow[a:b], cuda)),
+                          to_dev(valid[a:b].view(np.int32), cuda))
+    assert total == int((valid != 0).sum())
+    pm.scale_flux(0.25)
+    pm.build_map()
+    keep = valid != 0
+    ref_pos, ref_pow = ph.pos[keep].copy(), ph.pow[keep].copy()
+    ref_pow[:, :3] *= np.float32(0.25)
+    pm2 = PhotonMap(ph.n, global_q_radius_max=0.06)
+    pm2.build(to_dev(ref_pos, cuda), to_dev(ref_pow, cuda), packed=False)
+    q = gen.queries(3000, seed=151)
+    a = pm.query(to_dev(q.pos, cuda), to_dev(q.nrm, cuda), want_nbr=True, k=40, r_max=0.06, filter="cone")
+    b = pm2.query(to_dev(q.pos, cuda), to_dev(q.nrm, cuda), want_nbr=True, k=40, r_max=0.06, filter="cone")
+    torch.cuda.synchronize()
+    for key in ("rad", "nbr", "r2", "count"):
+        assert torch.equal(a[key], b[key]), key
+    pm.clear()
+    pm.build_map()
+    assert pm.info().num_photons == 0
