@@ -115,7 +115,8 @@ PM_API pm_status pm_set_allocator(pm_map* map, pm_alloc_fn alloc, pm_free_fn fre
 
 /* k-buffer layouts of the query kernel. */
 enum { PM_KBUF_HEAP = 0,   /* one lane per query, max-heap in shared memory */
-       PM_KBUF_GROUP = 1   /* a group of lanes per query, candidate buffer + exact selection */ };
+       PM_KBUF_GROUP = 1,  /* a group of lanes per query, candidate buffer + exact selection */
+       PM_KBUF_WIDE = 2    /* one query per warp over the 32-wide tree, candidate buffer + exact selection */ };
 
 /* Tuning knobs (chosen by the autotuner): photons per leaf (1..32), warps per
  * query block (1..8), query rounds per work chunk (1..4096), queries per warp
@@ -281,8 +282,10 @@ PM_API pm_status pm_compute_query_radii(pm_map* map, const pm_query_desc* desc, 
 typedef struct pm_batch pm_batch;
 PM_API pm_status pm_batch_create(pm_batch** out);
 PM_API pm_status pm_batch_destroy(pm_batch* batch);
-/* Photons per leaf, warps per query block and query rounds per work chunk. */
-PM_API pm_status pm_batch_set_tuning(pm_batch* batch, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk);
+/* Photons per leaf, warps per query block, query rounds per work chunk, and
+ * whether the query traverses the 32-wide tree (wide != 0) or the binary one. */
+PM_API pm_status pm_batch_set_tuning(pm_batch* batch, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk,
+                                     int wide);
 PM_API pm_status pm_batch_build(pm_batch* batch, const float* d_pos4, const float* d_pow4,
                                 const uint32_t* photon_offsets, uint32_t num_maps, int format, void* stream);
 PM_API pm_status pm_batch_query(pm_batch* batch, const pm_query_desc* descs, const float* d_qpos4,
@@ -300,8 +303,8 @@ PM_API pm_status pm_batch_capture(pm_batch* batch, const float* d_pos4, const fl
 PM_API pm_status pm_batch_launch(pm_batch* batch, void* stream);
 PM_API pm_status pm_batch_get_info(pm_batch* batch, pm_map_info* info, void* stream);
 PM_API const char* pm_batch_last_error(const pm_batch* batch);
-/* Times batch build + query over a grid of leaf sizes, warps per block and
- * rounds per chunk, applies the fastest, writes it to *best and leaves the
+/* Times batch build + query over a grid of leaf sizes, warps per block,
+ * rounds per chunk and tree width, applies the fastest, writes it to *best and leaves the
  * batch built with it.  Synchronous. */
 PM_API pm_status pm_batch_autotune(pm_batch* batch, const float* d_pos4, const float* d_pow4,
                                    const uint32_t* photon_offsets, uint32_t num_maps, int format,

@@ -19,7 +19,7 @@ PM_ORDER_SORTED, PM_ORDER_AS_GIVEN = 0, 1
 PM_MAX_K = 128
 PM_NOALLOC_MAX_QUERIES = 262144
 PM_DEVERR_STACK, PM_DEVERR_NONFINITE, PM_DEVERR_QNONFINITE = 0x1, 0x2, 0x4
-PM_KBUF_HEAP, PM_KBUF_GROUP = 0, 1
+PM_KBUF_HEAP, PM_KBUF_GROUP, PM_KBUF_WIDE = 0, 1, 2
 
 FILTERS = {"box": PM_FILTER_BOX, "cone": PM_FILTER_CONE, "epanechnikov": PM_FILTER_EPANECHNIKOV}
 
@@ -82,7 +82,7 @@ SIGNATURES = {
     "pm_export_tree": (_I, [_VP, _VP, _U32, _VP, _VP, _U32]),
     "pm_batch_create": (_I, [C.POINTER(C.c_void_p)]),
     "pm_batch_destroy": (_I, [_VP]),
-    "pm_batch_set_tuning": (_I, [_VP, _U32, _I, _I]),
+    "pm_batch_set_tuning": (_I, [_VP, _U32, _I, _I, _I]),
     "pm_batch_build": (_I, [_VP, _FP, _FP, _VP, _U32, _I, _VP]),
     "pm_batch_query": (_I, [_VP, _VP, _FP, _FP, _VP, _FP, _UP, _FP, _UP, _VP]),
     "pm_batch_capture": (_I, [_VP, _FP, _FP, _VP, _U32, _I, _VP, _FP, _FP, _VP, _FP, _UP, _FP, _UP]),

@@ -46,6 +46,7 @@ struct pm_map {
     // photon-sized
     DevBuf pos, pow, inv, nodes, hdr;
     DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
+    DevBuf wflag, wrank, wcnt, wfirst, wchild, wroot, wscan, rootmark;   // 32-wide tree
     // query-sized
     DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter, fixq;
     DevBuf stats;           // query counters (profiling level 2)
@@ -162,6 +163,14 @@ pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
     ENSURE(arrive, (cap + 1) * sizeof(uint32_t));
     ENSURE(nleaf, (cap + 1) * sizeof(uint32_t));
     ENSURE(partials, (8 * 1184 + 16) * sizeof(uint32_t));
+    ENSURE(wflag, cap * sizeof(uint32_t));
+    ENSURE(wrank, cap * sizeof(uint32_t));
+    ENSURE(wcnt, cap * sizeof(uint32_t));
+    ENSURE(wfirst, cap * sizeof(uint32_t));
+    ENSURE(wchild, (cap + 1) * 2 * sizeof(ChildSlot));
+    ENSURE(wroot, sizeof(ChildSlot));
+    ENSURE(wscan, (scan_scratch_words((uint32_t)cap) + 2) * sizeof(uint32_t));
+    ENSURE(rootmark, (cap + 1) * sizeof(uint32_t));
 #undef ENSURE
     m->cap_photons = (uint32_t)cap;
     return PM_OK;
@@ -210,10 +219,20 @@ MapView view_of(pm_map* m) {
     v.pos = P<float4>(m->pos);
     v.pow = P<float4>(m->pow);
     v.inv = P<uint32_t>(m->inv);
+    v.wchild = P<ChildSlot>(m->wchild);
+    v.wroot = P<ChildSlot>(m->wroot);
     v.nodes = P<Node>(m->nodes);
     v.hdr = P<MapHeader>(m->hdr);
     v.n = m->n;
     return v;
+}
+
+WideBuffers wide_of(pm_map* m) {
+    WideBuffers w;
+    w.wflag = P<uint32_t>(m->wflag); w.wrank = P<uint32_t>(m->wrank); w.wcnt = P<uint32_t>(m->wcnt);
+    w.wfirst = P<uint32_t>(m->wfirst); w.wchild = P<ChildSlot>(m->wchild); w.wroot = P<ChildSlot>(m->wroot);
+    w.scratch = P<uint32_t>(m->wscan);
+    return w;
 }
 
 QueryTuning tuning_of(const pm_map* m) {
@@ -287,7 +306,8 @@ pm_status pm_destroy(pm_map* m) {
     if (!m) return PM_ERR_INVALID;
     DevBuf* all[] = {&m->pos, &m->pow, &m->inv, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
-                     &m->arrive, &m->nleaf, &m->partials, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
+                     &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wrank, &m->wcnt, &m->wfirst,
+                     &m->wchild, &m->wroot, &m->wscan, &m->rootmark, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
@@ -318,7 +338,7 @@ pm_status pm_set_tuning(pm_map* m, uint32_t leaf_size, int warps_per_block, int 
     if (rounds_per_chunk < 1 || rounds_per_chunk > 4096) return fail(m, PM_ERR_INVALID, "rounds_per_chunk must be in [1, 4096]");
     if (queries_per_warp != 1 && queries_per_warp != 2 && queries_per_warp != 4 && queries_per_warp != 8)
         return fail(m, PM_ERR_INVALID, "queries_per_warp must be 1, 2, 4 or 8");
-    if (kbuf_layout != PM_KBUF_HEAP && kbuf_layout != PM_KBUF_GROUP)
+    if (kbuf_layout != PM_KBUF_HEAP && kbuf_layout != PM_KBUF_GROUP && kbuf_layout != PM_KBUF_WIDE)
         return fail(m, PM_ERR_INVALID, "unknown k-buffer layout %d", kbuf_layout);
     m->leaf_size = leaf_size;
     m->warps_per_block = warps_per_block;
@@ -361,10 +381,11 @@ pm_status pm_build(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t
     const int nl = build_map(reinterpret_cast<const float4*>(d_pos4), reinterpret_cast<const float4*>(d_pow4), n,
                              format, m->leaf_size, P<float4>(m->pos), P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes),
                              P<MapHeader>(m->hdr), bb, st, prof ? m->ev[1] : nullptr);
+    const int nw = build_wide(n, P<Node>(m->nodes), P<uint32_t>(m->parent), nullptr, P<MapHeader>(m->hdr), wide_of(m), st);
     if (prof) cudaEventRecord(m->ev[2], st);
     m->have_build_ev = prof;
-    m->build_launches = (uint32_t)nl;
-    m->launches += (uint64_t)nl;
+    m->build_launches = (uint32_t)(nl + nw);
+    m->launches += (uint64_t)(nl + nw);
     s = check_cuda(m, "pm_build");
     if (s != PM_OK) return s;
     m->n = n;
@@ -955,6 +976,8 @@ pm_status batch_build_device(pm_batch* b, const float* d_pos4, const float* d_po
                             P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes), P<MapHeader>(m->hdr), bb, st);
     nl += batch_roots(P<uint32_t>(b->ph_off), maps, n, m->leaf_size, P<float4>(m->pos), P<Node>(m->nodes), bb,
                       P<BatchGeom>(b->geom), st);
+    nl += batch_wide(n, maps, P<Node>(m->nodes), P<uint32_t>(m->parent), P<MapHeader>(m->hdr), P<uint32_t>(m->rootmark),
+                     wide_of(m), P<BatchGeom>(b->geom), st);
     m->launches += (uint64_t)nl;
     m->build_launches = (uint32_t)nl;
     return check_cuda(m, "pm_batch_build");
@@ -1041,9 +1064,9 @@ pm_status pm_batch_destroy(pm_batch* b) {
     return PM_OK;
 }
 
-pm_status pm_batch_set_tuning(pm_batch* b, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk) {
+pm_status pm_batch_set_tuning(pm_batch* b, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk, int wide) {
     if (!b) return PM_ERR_INVALID;
-    return pm_set_tuning(b->m, leaf_size, warps_per_block, rounds_per_chunk, 1, PM_KBUF_GROUP);
+    return pm_set_tuning(b->m, leaf_size, warps_per_block, rounds_per_chunk, 1, wide ? PM_KBUF_WIDE : PM_KBUF_GROUP);
 }
 
 pm_status pm_batch_build(pm_batch* b, const float* d_pos4, const float* d_pow4, const uint32_t* photon_offsets,
@@ -1150,6 +1173,7 @@ std::vector<TuneCand> tune_candidates(uint32_t k) {
             for (int r : rounds) {
                 c.push_back({l, w, r, 1, PM_KBUF_GROUP});
                 c.push_back({l, w, r, 2, PM_KBUF_GROUP});
+                c.push_back({l, w, r, 1, PM_KBUF_WIDE});
             }
     if (k <= 64) c.push_back({16, 4, 8, 1, PM_KBUF_HEAP});   // one lane per query suits small k
     return c;
@@ -1249,11 +1273,14 @@ extern "C" pm_status pm_batch_autotune(pm_batch* b, const float* d_pos4, const f
     const uint32_t leaves[] = {16, 24, 32};
     const int wpbs[] = {2, 4, 8};
     const int rounds[] = {8, 32};
+    const int layouts[] = {PM_KBUF_GROUP, PM_KBUF_WIDE};
+    int blay = PM_KBUF_WIDE;
     for (uint32_t l : leaves)
         for (int w : wpbs)
-            for (int r : rounds) {
+            for (int r : rounds)
+              for (int lay : layouts) {
                 m->leaf_size = l; m->warps_per_block = w; m->rounds_per_chunk = r;
-                m->queries_per_warp = 1; m->kbuf_layout = PM_KBUF_GROUP;
+                m->queries_per_warp = 1; m->kbuf_layout = lay;
                 float tb = 0, tq = 0;
                 for (int rep = 0; rep < 2 && s == PM_OK; ++rep) {
                     cudaEventRecord(ev[0], st);
@@ -1268,17 +1295,19 @@ extern "C" pm_status pm_batch_autotune(pm_batch* b, const float* d_pos4, const f
                     cudaEventElapsedTime(&tq, ev[1], ev[2]);
                 }
                 if (s != PM_OK) break;
-                if (tb + tq < best_score) { best_score = tb + tq; bl = l; bw = w; br = r; best_b = tb; best_q = tq; }
-            }
+                if (tb + tq < best_score) {
+                    best_score = tb + tq; bl = l; bw = w; br = r; blay = lay; best_b = tb; best_q = tq;
+                }
+              }
     for (cudaEvent_t& e : ev) cudaEventDestroy(e);
     m->leaf_size = s == PM_OK ? bl : saved_leaf;
     m->warps_per_block = s == PM_OK ? bw : saved_wpb;
     m->rounds_per_chunk = s == PM_OK ? br : saved_rounds;
     m->queries_per_warp = 1;
-    m->kbuf_layout = PM_KBUF_GROUP;
+    m->kbuf_layout = s == PM_OK ? blay : PM_KBUF_GROUP;
     if (s != PM_OK) return s;
     best->leaf_size = bl; best->warps_per_block = bw; best->rounds_per_chunk = br;
-    best->queries_per_warp = 1; best->kbuf_layout = PM_KBUF_GROUP;
+    best->queries_per_warp = 1; best->kbuf_layout = blay;
     best->build_ms = best_b; best->query_ms = best_q;
     return pm_batch_build(b, d_pos4, d_pow4, photon_offsets, num_maps, format, stream);
 }

@@ -170,7 +170,39 @@ __global__ void k_batch_roots(const uint32_t* __restrict__ off, uint32_t m, uint
     geom[i].root = slot;
 }
 
+// Marks every map's root node (internal) so that the wide tree starts a wide
+// node there.
+__global__ void k_batch_rootmark(const BatchGeom* __restrict__ geom, uint32_t m, uint32_t* __restrict__ rootmark) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const ChildSlot& s = geom[i].root;
+    if (s.ref != kInvalid && s.cnt == 0) rootmark[s.ref] = 1u;
+}
+
+// Every map's start slot in the wide tree.
+__global__ void k_batch_wroots(const uint32_t* __restrict__ wcnt, const uint32_t* __restrict__ wfirst, uint32_t m,
+                               BatchGeom* __restrict__ geom) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    ChildSlot s = geom[i].root;
+    if (s.ref != kInvalid && s.cnt == 0) {
+        const uint32_t t = s.ref - 1;
+        s.ref = wfirst[t];
+        s.cnt = kWideFlag | wcnt[t];
+    }
+    geom[i].wroot = s;
+}
+
 }  // namespace
+
+int batch_wide(uint32_t n, uint32_t m, const Node* nodes, const uint32_t* parent, MapHeader* hdr, uint32_t* rootmark,
+               const WideBuffers& wb, BatchGeom* geom, cudaStream_t st) {
+    cudaMemsetAsync(rootmark, 0, (size_t)(n + 1) * sizeof(uint32_t), st);
+    k_batch_rootmark<<<(m + 127) / 128, 128, 0, st>>>(geom, m, rootmark);
+    int nl = 1 + build_wide(n, nodes, parent, rootmark, hdr, wb, st);
+    k_batch_wroots<<<(m + 127) / 128, 128, 0, st>>>(wb.wcnt, wb.wfirst, m, geom);
+    return nl + 1;
+}
 
 int batch_bounds_and_keys(const float4* pos, const float4* pw, const uint32_t* ph_off, uint32_t m, uint32_t n,
                           uint32_t* acc, BatchGeom* geom, MapHeader* hdr, uint64_t* keys, uint32_t* vals,

@@ -370,4 +370,104 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
                                   nodes, hdr, bb, st);
 }
 
+
+// ---------------------------------------------------------------- wide tree --
+
+__device__ __forceinline__ bool is_marked_root(const uint32_t* rootmark, uint32_t id) {
+    return id == 1 || (rootmark && rootmark[id]);
+}
+
+// wflag[t] = 1 when compacted node t + 1 lies a multiple of kWideLevels below
+// its root (node 1, or a node marked in rootmark).
+__global__ void k_wide_flags(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ rootmark,
+                             const MapHeader* __restrict__ hdr, uint32_t bound, uint32_t* __restrict__ wflag) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bound) return;
+    const uint32_t m = hdr->num_nodes;
+    uint32_t f = 0;
+    if (t < m) {
+        uint32_t c = t + 1, d = 0;
+        while (!is_marked_root(rootmark, c) && d < 4096) { c = parent[c] >> 1; ++d; }
+        f = (d % kWideLevels == 0) ? 1u : 0u;
+    }
+    wflag[t] = f;
+}
+
+// Walks the kWideLevels-level expansion of wide node `id`, calling f(slot, is_wide_child) for
+// every child slot in depth-first, left-to-right order.
+template <class F>
+__device__ void wide_expand(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark, uint32_t id, F&& f) {
+    uint32_t st_node[2 * kWideLevels + 2];
+    uint8_t st_side[2 * kWideLevels + 2], st_lvl[2 * kWideLevels + 2];
+    int sp = 0;
+    st_node[sp] = id; st_side[sp] = 1; st_lvl[sp] = 1; ++sp;
+    st_node[sp] = id; st_side[sp] = 0; st_lvl[sp] = 1; ++sp;
+    while (sp > 0) {
+        --sp;
+        const uint32_t nd = st_node[sp], side = st_side[sp], lvl = st_lvl[sp];
+        const ChildSlot s = nodes[nd].c[side];
+        if (s.ref == kInvalid) continue;
+        if (s.cnt > 0) { f(s, false); continue; }
+        if (lvl == kWideLevels || is_marked_root(rootmark, s.ref)) { f(s, true); continue; }
+        st_node[sp] = s.ref; st_side[sp] = 1; st_lvl[sp] = (uint8_t)(lvl + 1); ++sp;
+        st_node[sp] = s.ref; st_side[sp] = 0; st_lvl[sp] = (uint8_t)(lvl + 1); ++sp;
+    }
+}
+
+__global__ void k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
+                             const uint32_t* __restrict__ wflag, const MapHeader* __restrict__ hdr, uint32_t bound,
+                             uint32_t* __restrict__ wcnt) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bound) return;
+    uint32_t c = 0;
+    if (t < hdr->num_nodes && wflag[t]) wide_expand(nodes, rootmark, t + 1, [&](const ChildSlot&, bool) { ++c; });
+    wcnt[t] = c;
+}
+
+__global__ void k_wide_emit(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
+                            const uint32_t* __restrict__ wflag, const uint32_t* __restrict__ wcnt,
+                            const uint32_t* __restrict__ wfirst, const MapHeader* __restrict__ hdr, uint32_t bound,
+                            ChildSlot* __restrict__ wchild) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bound || t >= hdr->num_nodes || !wflag[t]) return;
+    ChildSlot* out = wchild + wfirst[t];
+    uint32_t j = 0;
+    wide_expand(nodes, rootmark, t + 1, [&](const ChildSlot& s, bool wide) {
+        ChildSlot c = s;
+        if (wide) {
+            c.ref = wfirst[s.ref - 1];
+            c.cnt = kWideFlag | wcnt[s.ref - 1];
+        }
+        out[j++] = c;
+    });
+}
+
+// The traversal's start slot: the super-root's slot, pointing at the wide node.
+__global__ void k_wide_root(const Node* __restrict__ nodes, const uint32_t* __restrict__ wcnt,
+                            const uint32_t* __restrict__ wfirst, ChildSlot* __restrict__ wroot) {
+    ChildSlot s = nodes[0].c[0];
+    if (s.ref != kInvalid && s.cnt == 0) {
+        s.ref = wfirst[0];
+        s.cnt = kWideFlag | wcnt[0];
+    }
+    *wroot = s;
+}
+
+int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint32_t* rootmark, MapHeader* hdr,
+               const WideBuffers& wb, cudaStream_t st) {
+    int nl = 0;
+    const uint32_t bound = n > 1 ? n - 1 : 1;   // internal nodes are at most n - 1
+    const uint32_t tb = 128, grid = (bound + tb - 1) / tb;
+    if (n > 1) {
+        k_wide_flags<<<grid, tb, 0, st>>>(parent, rootmark, hdr, bound, wb.wflag);
+        nl += 1 + exclusive_scan(wb.wflag, wb.wrank, bound, wb.scratch + 1, wb.scratch, st);
+        k_wide_count<<<grid, tb, 0, st>>>(nodes, rootmark, wb.wflag, hdr, bound, wb.wcnt);
+        nl += 1 + exclusive_scan(wb.wcnt, wb.wfirst, bound, wb.scratch + 1, wb.scratch, st);
+        k_wide_emit<<<grid, tb, 0, st>>>(nodes, rootmark, wb.wflag, wb.wcnt, wb.wfirst, hdr, bound, wb.wchild);
+        ++nl;
+    }
+    k_wide_root<<<1, 1, 0, st>>>(nodes, wb.wcnt, wb.wfirst, wb.wroot);
+    return nl + 1;
+}
+
 }  // namespace pm

@@ -35,6 +35,15 @@ struct __align__(16) Node {
 static_assert(sizeof(ChildSlot) == 32, "slot is two 16-byte words");
 static_assert(sizeof(Node) == 64, "node is four 16-byte words");
 
+// 32-wide tree over the binary one: every binary node whose depth below its
+// root is a multiple of kWideLevels is a wide node; its children are the slots
+// reached by expanding kWideLevels binary levels (at most 32), stored
+// contiguously.  A child slot with cnt & kWideFlag references a wide node:
+// ref = index of its first child slot, cnt & kWideCount = its child count.
+constexpr int kWideLevels = 5;
+constexpr uint32_t kWideFlag = 0x80000000u;
+constexpr uint32_t kWideCount = 0x3fu;
+
 // Per-map header kept in device memory (written by the build).
 struct MapHeader {
     float lo[3];

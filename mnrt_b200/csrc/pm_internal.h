@@ -23,6 +23,7 @@ int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key
 // parameters uploaded by the host.
 struct __align__(16) BatchGeom {
     ChildSlot root;        // slot of the map's subtree (empty slot for an empty map)
+    ChildSlot wroot;       // the same subtree in the 32-wide tree
     float lo[3];           // photon bounds, lower corner
     float mscale;          // Morton scale of the map's cubic cell
     float fix_scale;       // 2^40 / largest flux channel
@@ -45,6 +46,8 @@ struct MapView {
     const float4* pow;      // tree order: rgb, w = octahedral direction bits
     const uint32_t* inv;    // caller index -> tree position
     const Node* nodes;      // [0] = super-root, internal nodes from 1
+    const ChildSlot* wchild;   // 32-wide tree: child slots
+    const ChildSlot* wroot;    // 32-wide tree: start slot
     MapHeader* hdr;
     uint32_t n;             // photon count (host copy)
 };
@@ -65,6 +68,16 @@ struct BuildBuffers {
     uint32_t num_partials;
 };
 
+struct WideBuffers {
+    uint32_t* wflag;       // per compacted node: is a wide node
+    uint32_t* wrank;       // scan of wflag
+    uint32_t* wcnt;        // per wide node: child count
+    uint32_t* wfirst;      // scan of wcnt: first child slot
+    ChildSlot* wchild;     // child slots of all wide nodes
+    ChildSlot* wroot;      // start slot of the wide traversal
+    uint32_t* scratch;     // scan scratch (total at [0])
+};
+
 // pm_build.cu
 size_t build_bytes_needed(uint32_t n);
 // Returns the number of kernels launched; sort_done (if set) is recorded on
@@ -73,6 +86,8 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
               float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
               cudaStream_t st, cudaEvent_t sort_done = nullptr);
 void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st);
+int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint32_t* rootmark, MapHeader* hdr,
+               const WideBuffers& wb, cudaStream_t st);
 int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
                       const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
                       Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st);
@@ -124,6 +139,8 @@ int batch_query_keys(const float4* qpos, const uint32_t* q_off, uint32_t m, uint
 int batch_roots(const uint32_t* ph_off, uint32_t m, uint32_t n, uint32_t leaf_size, const float4* pos,
                 const Node* nodes, const BuildBuffers& bb, BatchGeom* geom, cudaStream_t st);
 int map_id_bits(uint32_t m);
+int batch_wide(uint32_t n, uint32_t m, const Node* nodes, const uint32_t* parent, MapHeader* hdr, uint32_t* rootmark,
+               const WideBuffers& wb, BatchGeom* geom, cudaStream_t st);
 
 // pm_compat.cu
 int compat_node_estimates(const MapView& m, uint32_t max_slots, float rmax, uint32_t k, uint32_t iters, float* est,

@@ -58,6 +58,7 @@ struct KnnArgs {
     unsigned long long* stats;   // optional traversal counters (kStat*), nullptr = off
     const float* scale_ptr;   // fixed-point scale of the flux sums (map header or batch map)
     const ChildSlot* root;    // slot the traversal starts from
+    const ChildSlot* wchild;  // wide-tree child slots
     uint64_t nbr_off;         // batch: first neighbour slot of the map's rows
     uint32_t q_off;           // batch: first query of the map
     uint32_t ph_off;          // batch: first photon of the map (caller indices are batch-global)
@@ -750,8 +751,123 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
     return r2;
 }
 
-template <int G, bool kFix, bool kBatch>
-__global__ void __launch_bounds__(256) k_knn_group(KnnArgs a0) {
+// ------------------------------------------------------------------------
+// 32-wide tree traversal for one query held by a whole warp (G = 32): lane i
+// tests child i of a wide node, passing internal children are pushed with the
+// nearest on top, passing leaves are scanned nearest first (one photon per
+// lane).  Candidates go to buf as in the binary traversal.
+constexpr int kWideStack = 192;   // entries of 3 words: first child, child count, lower bound
+
+__device__ __forceinline__ void scan_leaf32(const KnnArgs& a, uint32_t ref, uint32_t cnt, float qx, float qy, float qz,
+                                            uint32_t k, uint32_t C, uint64_t* buf, uint32_t& n, bool& selected,
+                                            float& thr, uint32_t* hist, uint32_t lane, uint32_t lt) {
+    float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lane < cnt) mine = __ldg(a.pos + ref + lane);
+    if (n + 32 > C) {   // make room: keep the k nearest, tighten the threshold
+        const uint64_t T = group_select<32>(buf, n, k, hist, a.pos, lane, kFull, lt);
+        selected = true;
+        thr = __uint_as_float((uint32_t)(T >> 32));
+    }
+    bool acc = false;
+    float d2 = 0.0f;
+    if (lane < cnt) {
+        d2 = d2_rn(qx, qy, qz, mine.x, mine.y, mine.z);
+        acc = selected ? (d2 <= thr) : (d2 < thr);
+    }
+    const uint32_t bal = __ballot_sync(kFull, acc);
+    if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | (ref + lane);
+    n += __popc(bal);
+    __syncwarp();
+}
+
+// Lane holding the smallest v among the lanes in mask (ties: lowest lane).
+__device__ __forceinline__ uint32_t warp_argmin(float v, uint32_t mask, uint32_t lane) {
+    float bv = ((mask >> lane) & 1u) ? v : INFINITY;
+    uint32_t bl = ((mask >> lane) & 1u) ? lane : 32u;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, o);
+        const uint32_t ol = __shfl_xor_sync(kFull, bl, o);
+        if (ov < bv || (ov == bv && ol < bl)) { bv = ov; bl = ol; }
+    }
+    return bl;
+}
+
+__device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float qy, float qz, uint32_t k, uint32_t C, uint64_t* buf,
+                              uint32_t& n, bool& selected, float& thr, uint32_t* hist, uint32_t* stack, uint32_t lane,
+                              uint32_t lt) {
+    int sp = 0;
+    {
+        float lo[3], hi[3];
+        uint32_t ref, cnt;
+        load_root(a.root, lo, hi, ref, cnt);
+        if (ref == kInvalid) return;
+        const float lb = box_lb(qx, qy, qz, lo, hi);
+        if (!(selected ? lb <= thr : lb < thr)) return;
+        if (cnt & kWideFlag) {
+            if (lane == 0) { stack[0] = ref; stack[1] = cnt & kWideCount; stack[2] = __float_as_uint(lb); }
+            sp = 1;
+            __syncwarp();
+        } else if (cnt > 0) {
+            scan_leaf32(a, ref, cnt, qx, qy, qz, k, C, buf, n, selected, thr, hist, lane, lt);
+            return;
+        }
+    }
+    while (sp > 0) {
+        --sp;
+        const uint32_t first = stack[3 * sp], kids = stack[3 * sp + 1];
+        const float plb = __uint_as_float(stack[3 * sp + 2]);
+        __syncwarp();
+        if (!(selected ? plb <= thr : plb < thr)) continue;
+        float lo[3], hi[3];
+        uint32_t ref = kInvalid, cnt = 0;
+        if (lane < kids) load_root(a.wchild + first + lane, lo, hi, ref, cnt);
+        float lb = INFINITY;
+        bool pass = false;
+        if (ref != kInvalid) {
+            lb = box_lb(qx, qy, qz, lo, hi);
+            pass = selected ? lb <= thr : lb < thr;
+        }
+        const bool is_wide = (cnt & kWideFlag) != 0;
+        const uint32_t intm = __ballot_sync(kFull, pass && is_wide);
+        const uint32_t leafm = __ballot_sync(kFull, pass && !is_wide);
+        if (intm) {
+            const uint32_t np = __popc(intm);
+            if (sp + (int)np > kWideStack) {
+                if (lane == 0) atomicOr(&a.hdr->errors, kErrStack);
+            } else {
+                const uint32_t near = warp_argmin(lb, intm, lane);
+                const uint32_t others = intm & ~(1u << near);
+                if ((intm >> lane) & 1u) {
+                    const uint32_t at = (uint32_t)sp + (lane == near ? np - 1 : __popc(others & lt));
+                    stack[3 * at] = ref;
+                    stack[3 * at + 1] = cnt & kWideCount;
+                    stack[3 * at + 2] = __float_as_uint(lb);
+                }
+                sp += (int)np;
+                __syncwarp();
+            }
+        }
+        uint32_t rest = leafm;
+        if (rest) {
+            uint32_t b = warp_argmin(lb, rest, lane);   // nearest leaf first, then in tree order
+            for (;;) {
+                const uint32_t lref = __shfl_sync(kFull, ref, b), lcnt = __shfl_sync(kFull, cnt, b);
+                const float llb = __shfl_sync(kFull, lb, b);
+                if (selected ? llb <= thr : llb < thr)
+                    scan_leaf32(a, lref, lcnt, qx, qy, qz, k, C, buf, n, selected, thr, hist, lane, lt);
+                rest &= ~(1u << b);
+                if (!rest) break;
+                b = __ffs(rest) - 1;
+            }
+        }
+    }
+}
+
+// The wide instances get a minimum of two blocks per SM: without it ptxas
+// holds them to 48 registers and spills.
+template <int G, bool kFix, bool kBatch, bool kWide>
+__global__ void __launch_bounds__(256, kWide ? 2 : 0) k_knn_group(KnnArgs a0) {
     constexpr int QW = 32 / G;
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = lane_id();
@@ -791,7 +907,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a0) {
                 a.k = bq.k; a.r2max = bq.r2max; a.rmax = bq.rmax; a.filter = bq.filter; a.cone_k = bq.cone_k;
                 a.min_found = bq.min_found; a.nbr_off = bq.nbr_off; a.q_off = bq.q_off; a.ph_off = bq.ph_off;
                 a.scale_ptr = &a0.bgeom[map].fix_scale;
-                a.root = &a0.bgeom[map].root;
+                a.root = kWide ? &a0.bgeom[map].wroot : &a0.bgeom[map].root;
             }
             const uint32_t k = a.k;
             const float r2max = a.r2max;
@@ -832,6 +948,9 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a0) {
             while (__any_sync(kFull, todo)) {
                 const bool live = todo;
                 if (live) { n = 0; selected = false; thr = tau0; }
+                if constexpr (kWide) {
+                    if (live) wide_traverse(a, qx, qy, qz, k, C, buf, n, selected, thr, hist, stack, lane, lt);
+                } else {
                 int sp = 0;
                 float lo[3], hi[3];
                 uint32_t ref, cnt;
@@ -922,6 +1041,7 @@ __global__ void __launch_bounds__(256) k_knn_group(KnnArgs a0) {
                     }
                     if (!found) break;
                     have = true;
+                }
                 }
                 // the bound admitted fewer than k photons: redo this query with R
                 todo = live && n < k && tau0 < r2max;
@@ -1058,6 +1178,7 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.fix_list = nullptr; a.fix_count = nullptr; a.nq_dev = nullptr; a.fix_in = nullptr;
     a.scale_ptr = &m.hdr->fix_scale;
     a.root = &m.nodes[0].c[0];
+    a.wchild = m.wchild;
     a.nbr_off = 0; a.q_off = 0; a.ph_off = 0;
     a.qkeys = nullptr; a.bgeom = nullptr; a.bq = nullptr;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
@@ -1065,6 +1186,10 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
 }
 
 uint32_t group_capacity(uint32_t k) { return ((k + 31u) & ~31u) + 64u; }
+
+int wide_smem_bytes_per_warp(uint32_t k) {
+    return (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) + 3 * kWideStack * (int)sizeof(uint32_t);
+}
 
 int group_smem_bytes_per_warp(uint32_t k, int qpw) {
     return qpw * (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) +
@@ -1102,6 +1227,24 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         k_knn_tree<<<grid, threads, smem, st>>>(a);
         return 1;
     }
+    if (t.layout == 2) {   // one query per warp over the 32-wide tree
+        a.cap = group_capacity(p.k);
+        a.smem_per_warp = (uint32_t)wide_smem_bytes_per_warp(p.k);
+        a.root = m.wroot;
+        a.fix_list = fix_list;
+        a.fix_count = work_counter + 1;
+        const int smem = (int)a.smem_per_warp * t.warps_per_block;
+        const uint32_t nchunks = (nq + a.rounds_per_chunk - 1) / a.rounds_per_chunk;
+        KnnArgs fx = a;
+        fx.fix_in = fix_list;
+        fx.nq_dev = work_counter + 1;
+        fx.work_counter = work_counter + 2;
+        const uint32_t grid = grid_for(k_knn_group<32, false, false, true>, threads, smem, nchunks, t.warps_per_block);
+        k_knn_group<32, false, false, true><<<grid, threads, smem, st>>>(a);
+        const uint32_t gfix = grid_for(k_knn_group<32, true, false, true>, threads, smem, nchunks, t.warps_per_block);
+        k_knn_group<32, true, false, true><<<gfix, threads, smem, st>>>(fx);
+        return 2;
+    }
     const int qpw = t.queries_per_warp;
     a.cap = group_capacity(p.k);
     a.smem_per_warp = (uint32_t)group_smem_bytes_per_warp(p.k, qpw);
@@ -1116,10 +1259,10 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
     fx.work_counter = work_counter + 2;
 #define PM_LAUNCH_GROUP(G)                                                                          \
     {                                                                                               \
-        const uint32_t grid = grid_for(k_knn_group<G, false, false>, threads, smem, nchunks, t.warps_per_block); \
-        k_knn_group<G, false, false><<<grid, threads, smem, st>>>(a);                                      \
-        const uint32_t gfix = grid_for(k_knn_group<G, true, false>, threads, smem, nchunks, t.warps_per_block); \
-        k_knn_group<G, true, false><<<gfix, threads, smem, st>>>(fx);                                      \
+        const uint32_t grid = grid_for(k_knn_group<G, false, false, false>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, false, false, false><<<grid, threads, smem, st>>>(a);                                      \
+        const uint32_t gfix = grid_for(k_knn_group<G, true, false, false>, threads, smem, nchunks, t.warps_per_block); \
+        k_knn_group<G, true, false, false><<<gfix, threads, smem, st>>>(fx);                                      \
     }
     switch (qpw) {
         case 1: PM_LAUNCH_GROUP(32) break;
@@ -1134,7 +1277,8 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
 // One persistent launch over the queries of many maps (one query per warp):
 // the sorted query keys carry each query's map id, whose root slot and
 // parameters the kernel reads; kmax sizes the candidate buffers.
-int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
+template <bool kW>
+static int launch_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
                     const float4* qnrm, const uint32_t* order, const uint64_t* qkeys, uint32_t nq,
                     const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list, const QueryTuning& t,
                     cudaStream_t st) {
@@ -1148,22 +1292,31 @@ int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg,
     a.bgeom = bg;
     a.bq = bq;
     a.cap = group_capacity(kmax);
-    a.smem_per_warp = (uint32_t)group_smem_bytes_per_warp(kmax, 1);
+    a.smem_per_warp = (uint32_t)(kW ? wide_smem_bytes_per_warp(kmax) : group_smem_bytes_per_warp(kmax, 1));
     a.fix_list = fix_list;
     a.fix_count = work_counter + 1;
     const int threads = 32 * t.warps_per_block;
     const int smem = (int)a.smem_per_warp * t.warps_per_block;
     cudaMemsetAsync(work_counter, 0, 3 * sizeof(uint32_t), st);
     const uint32_t nchunks = (nq + a.rounds_per_chunk - 1) / a.rounds_per_chunk;
-    const uint32_t grid = grid_for(k_knn_group<32, false, true>, threads, smem, nchunks, t.warps_per_block);
-    k_knn_group<32, false, true><<<grid, threads, smem, st>>>(a);
+    const uint32_t grid = grid_for(k_knn_group<32, false, true, kW>, threads, smem, nchunks, t.warps_per_block);
+    k_knn_group<32, false, true, kW><<<grid, threads, smem, st>>>(a);
     KnnArgs fx = a;   // queries whose estimate needs FP64 distances
     fx.fix_in = fix_list;
     fx.nq_dev = work_counter + 1;
     fx.work_counter = work_counter + 2;
-    const uint32_t gfix = grid_for(k_knn_group<32, true, true>, threads, smem, nchunks, t.warps_per_block);
-    k_knn_group<32, true, true><<<gfix, threads, smem, st>>>(fx);
+    const uint32_t gfix = grid_for(k_knn_group<32, true, true, kW>, threads, smem, nchunks, t.warps_per_block);
+    k_knn_group<32, true, true, kW><<<gfix, threads, smem, st>>>(fx);
     return 2;
+}
+
+int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
+                    const float4* qnrm, const uint32_t* order, const uint64_t* qkeys, uint32_t nq,
+                    const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list, const QueryTuning& t,
+                    cudaStream_t st) {
+    if (t.layout == 2)
+        return launch_batch<true>(m, bq, bg, kmax, qpos, qnrm, order, qkeys, nq, out, work_counter, fix_list, t, st);
+    return launch_batch<false>(m, bq, bg, kmax, qpos, qnrm, order, qkeys, nq, out, work_counter, fix_list, t, st);
 }
 
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,

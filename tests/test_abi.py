@@ -72,7 +72,7 @@ def test_build_validation_without_gpu(engine_lib):
     assert lib.pm_set_tuning(h, 33, 4, 8, 4, 1) == L.PM_ERR_INVALID
     assert lib.pm_set_tuning(h, 16, 9, 8, 4, 1) == L.PM_ERR_INVALID
     assert lib.pm_set_tuning(h, 16, 4, 8, 3, 1) == L.PM_ERR_INVALID
-    assert lib.pm_set_tuning(h, 16, 4, 8, 4, 2) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 16, 4, 8, 4, 3) == L.PM_ERR_INVALID
     assert lib.pm_set_tuning(h, 16, 4, 8, 4, 1) == L.PM_OK
     assert lib.pm_scale_flux(h, 2.0, None) == L.PM_ERR_STATE
     lib.pm_destroy(h)
@@ -130,5 +130,5 @@ def test_batch_validation_without_gpu(engine_lib):
     assert b"must not decrease" in lib.pm_batch_last_error(h)
     assert lib.pm_batch_build(h, 16, 32, None, 2, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID
     assert lib.pm_batch_launch(h, None) == L.PM_ERR_STATE
-    assert lib.pm_batch_set_tuning(h, 0, 4, 8) == L.PM_ERR_INVALID
+    assert lib.pm_batch_set_tuning(h, 0, 4, 8, 1) == L.PM_ERR_INVALID
     assert lib.pm_batch_destroy(h) == L.PM_OK

@@ -75,11 +75,12 @@ def compare(out, ref, qoff):
         noff += (b - a) * d["k"]
 
 
-def test_batch_matches_per_map(cuda):
+@pytest.mark.parametrize("wide", [False, True])
+def test_batch_matches_per_map(cuda, wide):
     phs, qs, poff, qoff, pos, pw, qp, qn = make_batch()
     ref = per_map_reference(cuda, phs, qs)
     b = PhotonMapBatch()
-    b.set_tuning(leaf_size=16, warps_per_block=4, rounds_per_chunk=5)
+    b.set_tuning(leaf_size=16, warps_per_block=4, rounds_per_chunk=5, wide=wide)
     b.build(to_dev(pos, cuda), to_dev(pw, cuda), poff)
     out = b.query(DESCS, to_dev(qp, cuda), to_dev(qn, cuda), qoff, want_nbr=True)
     torch.cuda.synchronize()

@@ -69,10 +69,11 @@ def test_small_config_parity(cuda, oracle_mod, filt):
 
 KERNELS = [dict(kbuf_layout=0), dict(kbuf_layout=1, queries_per_warp=1), dict(kbuf_layout=1, queries_per_warp=2),
            dict(kbuf_layout=1, queries_per_warp=4), dict(kbuf_layout=1, queries_per_warp=8),
-           dict(kbuf_layout=1, queries_per_warp=1, rounds_per_chunk=1)]
+           dict(kbuf_layout=1, queries_per_warp=1, rounds_per_chunk=1), dict(kbuf_layout=2),
+           dict(kbuf_layout=2, rounds_per_chunk=1, leaf_size=4)]
 
 
-@pytest.mark.parametrize("kern", KERNELS, ids=["heap", "g32", "g16", "g8", "g4", "g32r1"])
+@pytest.mark.parametrize("kern", KERNELS, ids=["heap", "g32", "g16", "g8", "g4", "g32r1", "wide", "wide_l4"])
 @pytest.mark.parametrize("k,filt", [(100, "cone"), (16, "box"), (128, "epanechnikov")])
 def test_kernel_variants_bitwise_equal(cuda, oracle_mod, kern, k, filt):
     """Every k-buffer layout / queries-per-warp variant gives the same bits."""
@@ -81,7 +82,9 @@ def test_kernel_variants_bitwise_equal(cuda, oracle_mod, kern, k, filt):
     q = gen.queries(6000, seed=32)
     q.pos[:20, :3] = ph.pos[7, :3]
     ref = run(ph, q, cuda, k, 0.05, filt, brute=True)
-    res = run(ph, q, cuda, k, 0.05, filt, tuning={"rounds_per_chunk": 5, **kern})
+    tun = {"rounds_per_chunk": 5, **kern}
+    leaf = tun.pop("leaf_size", 16)
+    res = run(ph, q, cuda, k, 0.05, filt, tuning=tun, leaf=leaf)
     for key in ("nbr", "count", "r2", "rad"):
         assert np.array_equal(res[key], ref[key]), key
     assert res["info"].device_errors == 0
@@ -250,7 +253,7 @@ def test_autotune_keeps_results_exact(cuda, oracle_mod):
     d_pos, d_pow, d_qp, d_qn = (to_dev(x, cuda) for x in (ph.pos, ph.pow, q.pos, q.nrm))
     t = pm.autotune(d_pos, d_pow, d_qp, d_qn, max_sample=4096, k=64, r_max=0.05, filter="cone")
     assert t.leaf_size in (16, 24, 32) and t.warps_per_block in (2, 4, 8) and t.rounds_per_chunk in (8, 32)
-    assert t.queries_per_warp in (1, 2) and t.kbuf_layout in (0, 1) and t.query_ms > 0
+    assert t.queries_per_warp in (1, 2) and t.kbuf_layout in (0, 1, 2) and t.query_ms > 0
     out = pm.query(d_qp, d_qn, want_nbr=True, k=64, r_max=0.05, filter="cone")
     torch.cuda.synchronize()
     res = {kk: v.cpu().numpy() for kk, v in out.items()}
