@@ -216,7 +216,7 @@ def run_ours(args, cfg) -> dict | None:
     tuning = "defaults"
     if args.leaf or args.wpb or args.rounds or args.qpw or args.layout >= 0:
         pm.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 32,
-                      queries_per_warp=args.qpw or 1, kbuf_layout=args.layout if args.layout >= 0 else 1)
+                      queries_per_warp=args.qpw or 1, kbuf_layout=args.layout if args.layout >= 0 else 2)
         tuning = "set by flags"
     elif not args.no_autotune:   # untimed: picks the kernel setting on a query sample
         t = pm.autotune(d_pos, d_pow, d_qpos, d_qnrm, max_sample=0, k=k, r_max=R, filter=cfg["filter"])
@@ -536,7 +536,7 @@ def main(argv=None) -> int:
     ap.add_argument("--wpb", type=int, default=0)
     ap.add_argument("--rounds", type=int, default=0)
     ap.add_argument("--qpw", type=int, default=0, help="queries per warp (group layout)")
-    ap.add_argument("--layout", type=int, default=-1, help="k-buffer layout: 0 heap, 1 group")
+    ap.add_argument("--layout", type=int, default=-1, help="k-buffer layout: 0 heap, 1 group, 2 wide tree")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

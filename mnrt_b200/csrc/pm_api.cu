@@ -34,7 +34,7 @@ struct pm_map {
     int warps_per_block = 4;
     int rounds_per_chunk = 32;
     int queries_per_warp = 1;
-    int kbuf_layout = 1;
+    int kbuf_layout = PM_KBUF_WIDE;
     pm_alloc_fn alloc = nullptr;
     pm_free_fn free_fn = nullptr;
     void* alloc_user = nullptr;

@@ -600,8 +600,10 @@ __device__ uint32_t hist_round(const uint64_t* buf, uint32_t n, float scale, int
 
 // Keeps exactly kk entries of buf[0, n): the kk smallest (d^2, caller index).
 // Returns the exact key (d^2 bits << 32 | caller index) of the kk-th.
+// Out of line: called about once per query, and inlined at both call sites it
+// crowds the hot loop's instructions.
 template <int G>
-__device__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
+__device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
                                  const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt) {
     uint32_t mx = 0;
     for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
@@ -864,10 +866,11 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
     }
 }
 
-// The wide instances get a minimum of two blocks per SM: without it ptxas
-// holds them to 48 registers and spills.
+// The wide instances are held to 64 registers (4 blocks of 256 per SM, 32
+// warps): measured fastest, and without a bound ptxas holds them to 48
+// registers and spills.
 template <int G, bool kFix, bool kBatch, bool kWide>
-__global__ void __launch_bounds__(256, kWide ? 2 : 0) k_knn_group(KnnArgs a0) {
+__global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
     constexpr int QW = 32 / G;
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = lane_id();
