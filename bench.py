@@ -516,7 +516,8 @@ def run_batch(args) -> dict:
         "sequential_queries_per_s": Q / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q / (eager_ms / 1000.0),
         "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": info.device_errors,
         "batch_tuning": {"leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block,
-                         "rounds_per_chunk": bt.rounds_per_chunk, "chosen_by": "pm_batch_autotune"},
+                         "rounds_per_chunk": bt.rounds_per_chunk, "wide_tree": bt.kbuf_layout == 2,
+                         "chosen_by": "pm_batch_autotune"},
     }
 
 
