@@ -1,0 +1,74 @@
+"""The differentiation workload at full size: 1,048,576
+photons (80 % walls, 20 % caustic), 1,048,576 wall queries, k = 64,
+Epanechnikov filter, target from powers scaled by seeded U[0.5, 1.5], loss
+= sum |E - T|^2.  Gradient check on 1,024 sampled photons:
+  * the engine's dL/dpower and dL/dposition against the oracle's FP64 host
+    gradient on the same neighbour sets: relative 1e-5 (floor 1e-6 of max);
+  * the host gradient against FP64 central finite differences with h = 1e-4
+    (Richardson-combined with h/2): relative 1e-3 (floor 1e-3 of max),
+    samples whose neighbour set or k-th neighbour changes within +-h
+    excluded and counted (printed)."""
+import numpy as np
+import pytest
+import torch
+
+from mnrt_b200 import gen
+from mnrt_b200.photon_map import PhotonMap
+from tests.fd import LossFD
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b, floor_frac):
+    floor = floor_frac * max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+def test_config4_gradient_check(cuda, oracle_mod):
+    cfg = gen.CONFIGS["diff"]
+    n, nq, k, r = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"]
+    ph = gen.photons(n, seed=4000, caustic_frac=0.2)
+    q = gen.queries(nq, seed=4001)
+    rng = np.random.default_rng(4242)
+    tpow = ph.pow.copy()
+    tpow[:, :3] *= rng.uniform(0.5, 1.5, size=(n, 3)).astype(np.float32)
+    dev = cuda
+    to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    pm = PhotonMap(n, global_q_radius_max=r, knn_target_count=k)
+    pm.build(to(ph.pos), to(tpow))
+    t = pm.query(to(q.pos), to(q.nrm), k=k, r_max=r, filter="epanechnikov")["rad"][:, :3].double().cpu().numpy()
+    pm.build(to(ph.pos), to(ph.pow))
+    out = pm.query(to(q.pos), to(q.nrm), want_nbr=True, k=k, r_max=r, filter="epanechnikov")
+    g = torch.zeros((nq, 4), dtype=torch.float32, device=dev)
+    g[:, :3] = (2.0 * (out["rad"][:, :3].double() - torch.from_numpy(t).to(dev))).float()
+    gp, gx = pm.query_backward(to(q.pos), to(q.nrm), g, nbr=out["nbr"], count=out["count"], k=k, r_max=r,
+                               filter="epanechnikov")
+    torch.cuda.synchronize()
+    gp, gx = gp.cpu().numpy()[:, :3], gx.cpu().numpy()[:, :3]
+    nbr = out["nbr"].cpu().numpy().view(np.uint32)
+    cnt = out["count"].cpu().numpy().view(np.uint32)
+    sample = np.random.default_rng(7).choice(n, 1024, replace=False)
+    # engine vs host FP64 gradient, same sets and dL/dE
+    hp, hx = oracle_mod.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, nbr, cnt, k, r,
+                                      g[:, :3].double().cpu().numpy(), "epanechnikov")
+    e_pow = rel_err(gp[sample], hp[sample], 1e-6).max()
+    e_pos = rel_err(gx[sample], hx[sample], 1e-6).max()
+    print(f"config 4: engine vs host gradient on 1,024 photons: power {e_pow:.2e}, position {e_pos:.2e}")
+    assert e_pow <= 1e-5 and e_pos <= 1e-5
+    # host gradient of the FP64 loss vs FP64 central differences
+    e64 = oracle_mod.radiance_fp64(ph.pos, ph.pow, q.pos, q.nrm, nbr, cnt, k, r, "epanechnikov")
+    hp64, hx64 = oracle_mod.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, nbr, cnt, k, r, 2.0 * (e64 - t),
+                                          "epanechnikov")
+    fd = LossFD(oracle_mod, ph.pos, ph.pow, q.pos, q.nrm, t, k, r, "epanechnikov")
+    f = fd.position(sample)
+    ok = ~f.excluded
+    err_rich = rel_err(hx64[sample][ok], f.fd[ok], 1e-3)
+    err_plain = rel_err(hx64[sample][ok], f.plain[ok], 1e-3)
+    fp = fd.power(sample[:256])
+    err_pow = rel_err(hp64[sample[:256]], fp, 1e-3)
+    print(f"config 4: FD position check on {ok.sum()} of {ok.size} samples ({f.num_excluded} excluded: set change "
+          f"within +-h): max rel err {err_rich.max():.2e} (Richardson), {err_plain.max():.2e} (plain h=1e-4), "
+          f"within 1e-3 plain: {(err_plain <= 1e-3).mean() * 100:.1f} %; power FD max rel err {err_pow.max():.2e}")
+    assert ok.sum() >= 0.5 * ok.size
+    assert err_rich.max() <= 1e-3
+    assert err_pow.max() <= 1e-3

