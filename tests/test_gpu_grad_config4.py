@@ -69,6 +69,9 @@ def test_config4_gradient_check(cuda, oracle_mod):
     print(f"config 4: FD position check on {ok.sum()} of {ok.size} samples ({f.num_excluded} excluded: set change "
           f"within +-h): max rel err {err_rich.max():.2e} (Richardson), {err_plain.max():.2e} (plain h=1e-4), "
           f"within 1e-3 plain: {(err_plain <= 1e-3).mean() * 100:.1f} %; power FD max rel err {err_pow.max():.2e}")
-    assert ok.sum() >= 0.5 * ok.size
+    # at this density an in-plane move of 1e-4 crosses about 2.8 queries' k-th-neighbour
+    # boundaries on average (query density x 2 pi r_k x 2 h), so about half the samples sit on a
+    # kink and are excluded; the rest must be plentiful
+    assert ok.sum() >= 500
     assert err_rich.max() <= 1e-3
     assert err_pow.max() <= 1e-3
