@@ -598,12 +598,10 @@ __device__ uint32_t hist_round(const uint64_t* buf, uint32_t n, float scale, int
     return digit;
 }
 
-// Keeps exactly kk entries of buf[0, n): the kk smallest (d^2, caller index).
-// Returns the exact key (d^2 bits << 32 | caller index) of the kk-th.
-// Out of line: called about once per query, and inlined at both call sites it
-// crowds the hot loop's instructions.
+// General selection (any distribution of keys): two 8-bit histogram rounds
+// on d^2 quantised to 16 bits, then an exact pass over the boundary bucket.
 template <int G>
-__device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
+__device__ uint64_t group_select_general(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
                                  const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt) {
     uint32_t mx = 0;
     for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
@@ -647,6 +645,86 @@ __device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32
     }
     n = out;
     return T;
+}
+
+// Sorts one 64-bit key per lane of a group of G lanes (bitonic network).
+template <int G>
+__device__ __forceinline__ uint64_t gsort_bitonic(uint64_t v, uint32_t s, uint32_t gmask) {
+#pragma unroll
+    for (int size = 2; size <= G; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint64_t o = __shfl_xor_sync(gmask, v, stride);
+            const bool up = (s & (uint32_t)size) == 0;
+            const bool lower = (s & (uint32_t)stride) == 0;
+            v = (lower == up) ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    }
+    return v;
+}
+
+// Keeps exactly kk entries of buf[0, n): the kk smallest (d^2, caller index),
+// in order of appearance; returns the d^2 bits of the kk-th in the high word.
+// One 8-bit histogram round on d^2 quantised to [0, 255] finds the boundary
+// bucket B.  On a surface d^2 is close to uniform, so B holds one or two
+// entries: when all of B is kept no caller index is read at all, and when
+// part of it is, its entries (at most G) are ranked by one bitonic sort of
+// their exact keys.  Anything else takes group_select_general.
+// Out of line: called about once per query, and inlined at both call sites it
+// crowds the hot loop's instructions.
+template <int G>
+__device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
+                                              const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt) {
+    uint32_t mx = 0;
+    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+    mx = gmax_u32<G>(mx, gmask);
+    const float dmax = __uint_as_float(mx);
+    if (!(dmax > 0.0f)) return group_select_general<G>(buf, n, kk, hist, pos, s, gmask, lt);
+    const float scale = __fdiv_rn(255.0f, dmax);   // q in [0, 255], monotone in d^2
+    uint32_t need = kk;
+    const uint32_t B = hist_round<G>(buf, n, scale, 0, 0, false, need, hist, s, gmask);
+    const uint32_t nb = hist[B];
+    __syncwarp(gmask);
+    const bool all_b = need == nb;
+    if (!all_b && nb > (uint32_t)G) return group_select_general<G>(buf, n, kk, hist, pos, s, gmask, lt);
+    uint64_t T = ~0ull;
+    if (!all_b) {   // rank the boundary bucket's exact keys
+        uint64_t* bl = reinterpret_cast<uint64_t*>(hist);   // 128 slots of this group's histogram space
+        uint32_t got = 0;
+        for (uint32_t base = 0; base < n; base += G) {
+            const uint32_t e = base + s;
+            const bool in_b = e < n && q16((uint32_t)(buf[e] >> 32), scale) == B;
+            const uint32_t bal = __ballot_sync(gmask, in_b);
+            if (in_b) bl[got + __popc(bal & lt)] = buf[e];
+            got += __popc(bal);
+        }
+        __syncwarp(gmask);
+        const uint64_t x = s < nb ? exact_key(bl[s], pos) : ~0ull;
+        const uint64_t sorted = gsort_bitonic<G>(x, s, gmask);
+        T = __shfl_sync(gmask, sorted, (int)(__ffs(gmask) - 1u + need - 1u));   // the need-th of B
+        __syncwarp(gmask);
+    }
+    uint32_t out = 0, kmax = 0;
+    for (uint32_t base = 0; base < n; base += G) {
+        const uint32_t e = base + s;
+        uint64_t v = 0;
+        bool keep = false;
+        if (e < n) {
+            v = buf[e];
+            const uint32_t q = q16((uint32_t)(v >> 32), scale);
+            keep = q < B || (q == B && (all_b || exact_key(v, pos) <= T));
+        }
+        const uint32_t bal = __ballot_sync(gmask, keep);
+        __syncwarp(gmask);
+        if (keep) {
+            buf[out + __popc(bal & lt)] = v;
+            kmax = max(kmax, (uint32_t)(v >> 32));
+        }
+        out += __popc(bal);
+        __syncwarp(gmask);
+    }
+    n = out;
+    return (uint64_t)gmax_u32<G>(kmax, gmask) << 32;
 }
 
 // Final selection and outputs for one query held by a group of G lanes:
