@@ -495,9 +495,8 @@ __global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
 // appended to the group's buffer in shared memory with one ballot per step
 // (no per-candidate dependent chains).  When the buffer fills, an exact
 // selection keeps the k smallest (d^2, caller index) keys and tightens the
-// threshold.  Selection = two 8-bit histogram rounds on d^2 quantised
-// linearly to 16 bits, then an exact pass over the few keys sharing the
-// boundary bucket.
+// threshold (group_select: one 8-bit histogram round finds the boundary
+// bucket, whose few keys are ranked exactly).
 
 template <int G>
 struct GroupCtx {
