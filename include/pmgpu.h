@@ -61,7 +61,8 @@ enum {
 
 enum { PM_PHOTONS_REFERENCE = 0, PM_PHOTONS_PACKED = 1 };
 enum { PM_FILTER_BOX = 0, PM_FILTER_CONE = 1, PM_FILTER_EPANECHNIKOV = 2 };
-enum { PM_MODE_EXACT = 0, PM_MODE_ZHOU_COMPAT = 1 };
+enum { PM_MODE_EXACT = 0, PM_MODE_ZHOU_COMPAT = 1,
+       PM_MODE_ICUT = 2   /* pm_gather_for only: interpolate the map's illumination cut */ };
 enum { PM_ORDER_SORTED = 0, PM_ORDER_AS_GIVEN = 1 };
 
 /* Largest k the query kernels support. */
@@ -79,7 +80,7 @@ typedef struct pm_query_desc {
     float r_max;         /* maximum query radius R (reference: globalQRadiusMax) */
     int filter;          /* PM_FILTER_* */
     float cone_k;        /* cone filter constant k_c >= 1 (Jensen 2001), used by PM_FILTER_CONE */
-    int mode;            /* PM_MODE_EXACT or PM_MODE_ZHOU_COMPAT */
+    int mode;            /* PM_MODE_EXACT or PM_MODE_ZHOU_COMPAT (PM_MODE_ICUT: pm_gather_for only) */
     uint32_t min_found;  /* estimates from fewer photons are zeroed (reference uses 8) */
     int order;           /* PM_ORDER_SORTED: Morton-sort the queries first; AS_GIVEN: keep order */
     uint32_t refine_iters; /* ZHOU_COMPAT only: histogram refinement rounds (reference default 2) */
@@ -249,11 +250,67 @@ PM_API pm_status pm_set_backward_chunk(pm_map* map, uint32_t max_queries);
  * incoming ray, and estimates from fewer than desc->min_found photons zeroed
  * when d_clr_diffuse4 is non-NULL.  NULL d_clr_diffuse4 means white and no
  * min_found rule (the reference's photon visualisation).  Indices must be
- * distinct within one call (the reference accumulates without atomics). */
+ * distinct within one call (the reference accumulates without atomics).
+ * desc->mode == PM_MODE_ICUT takes E from the map's illumination cut
+ * (pm_icut_interpolate with R = desc->r_max and the normal as given;
+ * kernel_InterpolateIrradiance, GPU/photon_knn.cu:598-660) instead of a
+ * photon search, as the reference's GatherFor does with cuts enabled. */
 PM_API pm_status pm_gather_for(pm_map* map, const pm_query_desc* desc, const float* d_hit_pos4,
                         const float* d_hit_nrm4, const float* d_ray_dir4, const float* d_ray_origin4,
                         const float* d_ray_influence4, const float* d_clr_diffuse4, const uint32_t* d_idx_shading,
                         uint32_t n, float* d_io_radiance4, float* d_io_recip_dist, void* stream);
+
+/* ---- Illumination cuts (Wang et al. 2009 as the reference builds them:
+ * PhotonMap::OnFinalNodeList / GenerateFinalIllumCut PhotonMap.cpp:287-452,
+ * GPU/illumcut.cu, and the interpolation of GPU/photon_knn.cu:338-433,
+ * 598-660).  A cut is a set of tree nodes with one on every root-to-leaf
+ * path; irradiance is estimated once per cut node and final-gather queries
+ * interpolate it (pm_gather_for with desc->mode == PM_MODE_ICUT, the
+ * reference's GatherFor when MNRTSettings::GetUseIllumCuts() is set).
+ *
+ * The cut's nodes are the engine tree's slots: slot 0 is the root, slots
+ * 2j and 2j + 1 are the two children of internal node j; slot 1 is unused.
+ * A built map has 2 (num_nodes + 1) slots (pm_map_info.num_nodes). */
+typedef struct pm_icut_desc {
+    int use_leafs;           /* 1: the coarse cut is every leaf (MNRTSettings ICutUseLeafs, default 1) */
+    uint32_t level_emin;     /* tree level whose mean estimate is E_min (ICutLevelEmin, default 12) */
+    uint32_t refine_iters;   /* refinement rounds of the final cut (ICutRefineIters, default 4), <= 64 */
+    float accuracy;          /* required relative accuracy of a cut node (ICutAccuracy, default 0.2) */
+} pm_icut_desc;
+
+/* Builds the cut of the current tree (PhotonMap::BuildMap with illumination
+ * cuts on, PhotonMap.cpp:166-168).  node_query says how the irradiance at a
+ * node centre is estimated (k, r_max, filter, min_found; PM_MODE_EXACT or
+ * PM_MODE_ZHOU_COMPAT -- the reference uses the latter with the box filter
+ * and min_found 8, PhotonMap.cpp:371-384).  d_node_normals4 (optional, one
+ * float4 per slot, w ignored) gives the surface normal at each slot's centre;
+ * the reference derives it from the scene geometry (PhotonMap.cpp:339-364).
+ * Without it the engine uses the normalised sum of the reversed incident
+ * directions of the slot's photons (slots of fewer than 5,000 photons; larger
+ * slots get no normal and no estimate).  Synchronises the stream once (node
+ * count); the rest is asynchronous.  A rebuild of the map drops the cut. */
+PM_API pm_status pm_icut_build(pm_map* map, const pm_icut_desc* cut, const pm_query_desc* node_query,
+                               const float* d_node_normals4, void* stream);
+/* Number of slots of the built tree (synchronous). */
+PM_API pm_status pm_icut_slot_count(pm_map* map, uint32_t* count);
+/* Per slot: box centre (xyz) and largest box side (w), for a caller that
+ * computes normals from its geometry before pm_icut_build.  Empty slots get
+ * zeros. */
+PM_API pm_status pm_icut_node_centers(pm_map* map, float* d_centers4, void* stream);
+/* Irradiance interpolated from the cut at each query (xyz; w = cut nodes
+ * reached): every cut node reached through nodes whose box lies within r_max
+ * of q contributes w = (1 - t^2) max(0, n_node . n_q), t = |centre - q| /
+ * side <= 1; E = sum(w E_node) / sum(w), 0 when the weights sum to 0.  The
+ * normal is used as given (the reference does not flip it here). */
+PM_API pm_status pm_icut_interpolate(pm_map* map, float r_max, const float* d_qpos4, const float* d_qnrm4,
+                                     uint32_t nq, float* d_irr4, void* stream);
+/* Copies the cut for validation (host arrays of max_slots entries; any may be
+ * NULL): coarse and final marks (0/1), levels (0xFFFFFFFF for empty slots),
+ * centres (xyz, side), normals, photon-sum estimates and node-centre
+ * irradiance (float4 each).  Synchronous. */
+PM_API pm_status pm_icut_export(pm_map* map, uint32_t max_slots, uint32_t* h_coarse, uint32_t* h_final,
+                                uint32_t* h_level, float* h_center4, float* h_normal4, float* h_est4,
+                                float* h_exact4);
 
 /* PhotonMap::ScaleFlux (PhotonMap.cpp:186-193): scales the RGB flux of the
  * photons the map holds -- the built tree and the merged store -- in place

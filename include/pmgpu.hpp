@@ -88,23 +88,37 @@ public:
         if (n == 0 && !m_built) return;   /* nothing to do, as the reference */
         check(pm_scale_flux(m_map, scale, m_stream), m_map);
     }
-    /* BuildMap (PhotonMap.cpp:157): the point kd-tree over the merged photons. */
+    /* BuildMap (PhotonMap.cpp:157-171): the point kd-tree over the merged
+     * photons, then the illumination cut when cuts are enabled. */
     bool BuildMap() {
         check(pm_build_merged(m_map, m_format, m_stream), m_map);
         m_built = true;
+        uint n = 0;
+        pm_merged_count(m_map, &n);
+        if (m_useICut && n > 0) {
+            pm_query_desc d = Desc(m_k, m_rMax);
+            check(pm_icut_build(m_map, &m_icut, &d, nullptr, m_stream), m_map);
+        }
         return true;
     }
     /* Clears the merged photons (PhotonData::Clear). */
     void Clear() { check(pm_clear_merged(m_map), m_map); }
 
-    /* Gather (PhotonMap.cpp:195): estimate at the shading points themselves. */
+    /* Gather (PhotonMap.cpp:195): estimate at the shading points themselves
+     * (never from the illumination cut, :206-224). */
     void Gather(const ShadingPoints& sp, const RayChunk& rayChunk, float4* d_clrDiffHit, float4* d_ioRadiance) {
-        GatherFor(sp, rayChunk, d_clrDiffHit, nullptr, d_ioRadiance, nullptr);
+        pm_query_desc d = Desc(m_k, m_rMax);
+        check(pm_gather_for(m_map, &d, F(sp.d_ptInter), F(sp.d_normalsS), F(rayChunk.d_dirs), F(rayChunk.d_origins),
+                            F(rayChunk.d_influences), F(d_clrDiffHit), nullptr, sp.numPoints,
+                            reinterpret_cast<float*>(d_ioRadiance), nullptr, m_stream),
+              m_map);
     }
-    /* GatherFor (PhotonMap.cpp:234): final-gather accumulation. */
+    /* GatherFor (PhotonMap.cpp:234): final-gather accumulation, from the
+     * illumination cut when cuts are enabled (:244-257). */
     void GatherFor(const ShadingPoints& sp, const RayChunk& rayChunk, float4* d_clrDiffHit, uint* d_idxShadingPts,
                    float4* d_ioRadiance, float* d_ioReciDistAccu) {
         pm_query_desc d = Desc(m_k, m_rMax);
+        if (m_useICut) d.mode = PM_MODE_ICUT;
         check(pm_gather_for(m_map, &d, F(sp.d_ptInter), F(sp.d_normalsS), F(rayChunk.d_dirs), F(rayChunk.d_origins),
                             F(rayChunk.d_influences), F(d_clrDiffHit), d_idxShadingPts, sp.numPoints,
                             reinterpret_cast<float*>(d_ioRadiance), d_ioReciDistAccu, m_stream),
@@ -130,6 +144,14 @@ public:
     }
     void SetStream(cudaStream_t s) { m_stream = s; }
     void SetModeCompat(bool on) { m_mode = on ? PM_MODE_ZHOU_COMPAT : PM_MODE_EXACT; }
+    /* MNRTSettings::SetUseIllumCuts and the ICut* settings (MNRTSettings.h:491-523). */
+    void SetUseIllumCuts(bool on) { m_useICut = on; }
+    void SetICutParams(bool useLeafs, uint levelEmin, uint refineIters, float accuracy) {
+        m_icut.use_leafs = useLeafs ? 1 : 0;
+        m_icut.level_emin = levelEmin;
+        m_icut.refine_iters = refineIters;
+        m_icut.accuracy = accuracy;
+    }
     void SetFilter(int filter, float coneK = 1.0f) { m_filter = filter; m_coneK = coneK; }
     pm_map* Handle() const { return m_map; }
 
@@ -151,6 +173,8 @@ private:
     int m_filter = PM_FILTER_BOX;    /* the reference's filter */
     float m_coneK = 1.0f;
     bool m_built = false;
+    bool m_useICut = false;
+    pm_icut_desc m_icut = {1, 12, 4, 0.2f};   /* MNRTSettings defaults */
     cudaStream_t m_stream = nullptr;
 };
 

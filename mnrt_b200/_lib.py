@@ -14,7 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libpmgpu.so"
 PM_OK, PM_ERR_INVALID, PM_ERR_CUDA, PM_ERR_OOM, PM_ERR_STATE, PM_ERR_DEVICE, PM_ERR_UNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
 PM_PHOTONS_REFERENCE, PM_PHOTONS_PACKED = 0, 1
 PM_FILTER_BOX, PM_FILTER_CONE, PM_FILTER_EPANECHNIKOV = 0, 1, 2
-PM_MODE_EXACT, PM_MODE_ZHOU_COMPAT = 0, 1
+PM_MODE_EXACT, PM_MODE_ZHOU_COMPAT, PM_MODE_ICUT = 0, 1, 2
 PM_ORDER_SORTED, PM_ORDER_AS_GIVEN = 0, 1
 PM_MAX_K = 128
 PM_NOALLOC_MAX_QUERIES = 262144
@@ -27,6 +27,11 @@ FILTERS = {"box": PM_FILTER_BOX, "cone": PM_FILTER_CONE, "epanechnikov": PM_FILT
 class QueryDesc(C.Structure):
     _fields_ = [("k", C.c_uint32), ("r_max", C.c_float), ("filter", C.c_int), ("cone_k", C.c_float),
                 ("mode", C.c_int), ("min_found", C.c_uint32), ("order", C.c_int), ("refine_iters", C.c_uint32)]
+
+
+class IcutDesc(C.Structure):
+    _fields_ = [("use_leafs", C.c_int), ("level_emin", C.c_uint32), ("refine_iters", C.c_uint32),
+                ("accuracy", C.c_float)]
 
 
 class MapInfo(C.Structure):
@@ -80,6 +85,11 @@ SIGNATURES = {
     "pm_query_stats": (_I, [_VP, _VP, _U32]),
     "pm_clear_errors": (_I, [_VP, _VP]),
     "pm_export_tree": (_I, [_VP, _VP, _U32, _VP, _VP, _U32]),
+    "pm_icut_build": (_I, [_VP, C.POINTER(IcutDesc), C.POINTER(QueryDesc), _FP, _VP]),
+    "pm_icut_slot_count": (_I, [_VP, C.POINTER(C.c_uint32)]),
+    "pm_icut_node_centers": (_I, [_VP, _FP, _VP]),
+    "pm_icut_interpolate": (_I, [_VP, _F, _FP, _FP, _U32, _FP, _VP]),
+    "pm_icut_export": (_I, [_VP, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pm_batch_create": (_I, [C.POINTER(C.c_void_p)]),
     "pm_batch_destroy": (_I, [_VP]),
     "pm_batch_set_tuning": (_I, [_VP, _U32, _I, _I, _I]),

@@ -21,7 +21,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libpmgpu.so"
 SOURCES = ["pm_api.cu", "pm_build.cu", "pm_query.cu", "pm_sort.cu", "pm_backward.cu", "pm_gather.cu", "pm_batch.cu",
-           "pm_compat.cu"]
+           "pm_compat.cu", "pm_icut.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

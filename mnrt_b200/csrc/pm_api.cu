@@ -61,6 +61,11 @@ struct pm_map {
     // photons merged by pm_merge, built by pm_build_merged (PhotonData of the reference)
     DevBuf mpos, mpow, mflags, mrank, mscan;
     uint32_t merged_n = 0, cap_merged = 0;
+    // illumination cut of the current tree (pm_icut_*): per-slot arrays
+    DevBuf ic_pslot, ic_level, ic_range, ic_center, ic_normal, ic_est, ic_exact, ic_coarse, ic_fin, ic_work0, ic_work1,
+        ic_acc;
+    uint32_t icut_slots = 0;
+    uint64_t icut_prep_gen = ~0ull, icut_gen = ~0ull;
     uint64_t build_gen = 0, compat_gen = ~0ull;
     uint32_t compat_k = 0, compat_iters = 0;
     float compat_r = 0.0f;
@@ -195,7 +200,7 @@ pm_status ensure_query_capacity(pm_map* m, uint32_t nq, cudaStream_t st) {
     return PM_OK;
 }
 
-pm_status validate_desc(pm_map* m, const pm_query_desc* d, bool exact_only) {
+pm_status validate_desc(pm_map* m, const pm_query_desc* d, bool exact_only, bool allow_icut = false) {
     if (!d) return fail(m, PM_ERR_INVALID, "query descriptor is NULL");
     if (d->k == 0) return fail(m, PM_ERR_INVALID, "k must be >= 1");
     if (d->k > PM_MAX_K) return fail(m, PM_ERR_UNSUPPORTED, "k = %u exceeds PM_MAX_K = %u", d->k, PM_MAX_K);
@@ -205,9 +210,11 @@ pm_status validate_desc(pm_map* m, const pm_query_desc* d, bool exact_only) {
         return fail(m, PM_ERR_INVALID, "unknown filter %d", d->filter);
     if (d->filter == PM_FILTER_CONE && !(d->cone_k >= 1.0f && std::isfinite(d->cone_k)))
         return fail(m, PM_ERR_INVALID, "cone_k must be finite and >= 1 (got %g)", (double)d->cone_k);
-    if (d->mode != PM_MODE_EXACT && d->mode != PM_MODE_ZHOU_COMPAT)
+    if (d->mode == PM_MODE_ICUT && !allow_icut)
+        return fail(m, PM_ERR_INVALID, "PM_MODE_ICUT is a pm_gather_for mode only");
+    if (d->mode != PM_MODE_EXACT && d->mode != PM_MODE_ZHOU_COMPAT && d->mode != PM_MODE_ICUT)
         return fail(m, PM_ERR_INVALID, "unknown mode %d", d->mode);
-    if (exact_only && d->mode != PM_MODE_EXACT)
+    if (exact_only && d->mode == PM_MODE_ZHOU_COMPAT)
         return fail(m, PM_ERR_INVALID, "this entry point supports PM_MODE_EXACT only");
     if (d->order != PM_ORDER_SORTED && d->order != PM_ORDER_AS_GIVEN)
         return fail(m, PM_ERR_INVALID, "unknown query order %d", d->order);
@@ -311,7 +318,9 @@ pm_status pm_destroy(pm_map* m) {
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
-                     &m->mrank, &m->mscan};
+                     &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
+                     &m->ic_normal, &m->ic_est, &m->ic_exact, &m->ic_coarse, &m->ic_fin, &m->ic_work0, &m->ic_work1,
+                     &m->ic_acc};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -592,14 +601,20 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     return check_cuda(m, "pm_query_backward");
 }
 
+static pm_status icut_interp_run(pm_map* m, float r_max, const float4* qpos, const float4* qnrm, uint32_t nq,
+                                 bool sorted, float4* out, cudaStream_t st, int* nl);
+
 pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit_pos4, const float* d_hit_nrm4,
                         const float* d_ray_dir4, const float* d_ray_origin4, const float* d_ray_influence4,
                         const float* d_clr_diffuse4, const uint32_t* d_idx_shading, uint32_t n, float* d_io_radiance4,
                         float* d_io_recip_dist, void* stream) {
     if (!m) return PM_ERR_INVALID;
-    pm_status s = validate_desc(m, desc, true);
+    pm_status s = validate_desc(m, desc, true, true);
     if (s != PM_OK) return s;
     if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    const bool icut = desc->mode == PM_MODE_ICUT;
+    if (icut && m->icut_gen != m->build_gen)
+        return fail(m, PM_ERR_STATE, "PM_MODE_ICUT needs an illumination cut of the current tree (pm_icut_build)");
     if (n > 0 && (!d_hit_pos4 || !d_hit_nrm4 || !d_ray_dir4 || !d_ray_influence4 || !d_io_radiance4))
         return fail(m, PM_ERR_INVALID, "hit positions, normals, ray directions, influences and radiance must be non-NULL");
     if (n > 0 && d_io_recip_dist && !d_ray_origin4)
@@ -617,22 +632,194 @@ pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit
         if ((s = buf_ensure(m, m->gest, (size_t)n * sizeof(float4), "gest")) != PM_OK) return s;
     }
     const float4* hit = reinterpret_cast<const float4*>(d_hit_pos4);
-    int nl = gather_normals(reinterpret_cast<const float4*>(d_hit_nrm4), reinterpret_cast<const float4*>(d_ray_dir4), n,
-                            P<float4>(m->gnrm), st);
-    const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, hit, n, st, &nl) : nullptr;
-    QueryParams qp = params_of(desc);
-    if (!d_clr_diffuse4) qp.min_found = 0;   // photon visualisation keeps every estimate (GPU/photon_knn.cu:515-519)
-    QueryOutputs out{P<float4>(m->gest), nullptr, nullptr, nullptr};
-    QueryTuning t = tuning_of(m);
-    t.stats = nullptr;
-    nl += query_knn(view_of(m), qp, hit, P<float4>(m->gnrm), order, n, out, P<uint32_t>(m->counter),
-                    P<uint32_t>(m->fixq), t, st);
+    int nl = 0;
+    if (icut) {
+        // kernel_InterpolateIrradiance (GPU/photon_knn.cu:598-660): the cut
+        // interpolated at the hit with the unflipped shading normal
+        s = icut_interp_run(m, desc->r_max, hit, reinterpret_cast<const float4*>(d_hit_nrm4), n,
+                            desc->order == PM_ORDER_SORTED, P<float4>(m->gest), st, &nl);
+        if (s != PM_OK) return s;
+    } else {
+        nl += gather_normals(reinterpret_cast<const float4*>(d_hit_nrm4), reinterpret_cast<const float4*>(d_ray_dir4), n,
+                             P<float4>(m->gnrm), st);
+        const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, hit, n, st, &nl) : nullptr;
+        QueryParams qp = params_of(desc);
+        if (!d_clr_diffuse4) qp.min_found = 0;   // photon visualisation keeps every estimate (GPU/photon_knn.cu:515-519)
+        QueryOutputs out{P<float4>(m->gest), nullptr, nullptr, nullptr};
+        QueryTuning t = tuning_of(m);
+        t.stats = nullptr;
+        nl += query_knn(view_of(m), qp, hit, P<float4>(m->gnrm), order, n, out, P<uint32_t>(m->counter),
+                        P<uint32_t>(m->fixq), t, st);
+    }
     nl += gather_accumulate(P<float4>(m->gest), hit, reinterpret_cast<const float4*>(d_ray_origin4),
                             reinterpret_cast<const float4*>(d_ray_influence4),
                             reinterpret_cast<const float4*>(d_clr_diffuse4), d_idx_shading, n,
                             reinterpret_cast<float4*>(d_io_radiance4), d_io_recip_dist, st);
     m->launches += (uint64_t)nl;
     return check_cuda(m, "pm_gather_for");
+}
+
+// ---- illumination cuts -----------------------------------------------------
+
+static IcutBuffers icut_of(pm_map* m) {
+    IcutBuffers b;
+    b.pslot = P<uint32_t>(m->ic_pslot); b.level = P<uint32_t>(m->ic_level); b.range = P<uint2>(m->ic_range);
+    b.center = P<float4>(m->ic_center); b.normal = P<float4>(m->ic_normal); b.est = P<float4>(m->ic_est);
+    b.exact = P<float4>(m->ic_exact); b.coarse = P<uint32_t>(m->ic_coarse); b.fin = P<uint32_t>(m->ic_fin);
+    b.work[0] = P<uint32_t>(m->ic_work0); b.work[1] = P<uint32_t>(m->ic_work1);
+    b.acc = P<unsigned long long>(m->ic_acc);
+    return b;
+}
+
+// Slot records of the current tree (levels, photon ranges, centres); reads
+// the node count from the device, so it synchronises the stream.
+static pm_status icut_prepare_now(pm_map* m, cudaStream_t st) {
+    if (m->icut_prep_gen == m->build_gen) return PM_OK;
+    if (capturing(st)) return fail(m, PM_ERR_STATE, "illumination cuts cannot be prepared during stream capture");
+    MapHeader h;
+    if (cudaMemcpyAsync(&h, m->hdr.ptr, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return check_cuda(m, "pm_icut: node count");
+    const uint32_t nodes = h.num_nodes;
+    const size_t ns = 2 * ((size_t)nodes + 1);
+    if (ns > (1u << 27)) return fail(m, PM_ERR_UNSUPPORTED, "illumination cuts support at most 2^27 tree slots");
+    pm_status s;
+#define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
+    ENSURE(ic_pslot, ((size_t)nodes + 2) * sizeof(uint32_t));
+    ENSURE(ic_level, ns * sizeof(uint32_t));
+    ENSURE(ic_range, ns * sizeof(uint2));
+    ENSURE(ic_center, ns * sizeof(float4));
+    ENSURE(ic_normal, ns * sizeof(float4));
+    ENSURE(ic_est, ns * sizeof(float4));
+    ENSURE(ic_exact, ns * sizeof(float4));
+    ENSURE(ic_coarse, ns * sizeof(uint32_t));
+    ENSURE(ic_fin, ns * sizeof(uint32_t));
+    ENSURE(ic_work0, ns * sizeof(uint32_t));
+    ENSURE(ic_work1, ns * sizeof(uint32_t));
+    ENSURE(ic_acc, 8 * sizeof(unsigned long long));
+#undef ENSURE
+    m->launches += (uint64_t)icut_prepare(view_of(m), nodes, icut_of(m), st);
+    s = check_cuda(m, "pm_icut: slot records");
+    if (s != PM_OK) return s;
+    m->icut_slots = (uint32_t)ns;
+    m->icut_prep_gen = m->build_gen;
+    return PM_OK;
+}
+
+static pm_status icut_interp_run(pm_map* m, float r_max, const float4* qpos, const float4* qnrm, uint32_t nq,
+                                 bool sorted, float4* out, cudaStream_t st, int* nl) {
+    pm_status s = ensure_query_capacity(m, nq, st);
+    if (s != PM_OK) return s;
+    const uint32_t* order = sorted ? sort_queries(m, qpos, nq, st, nl) : nullptr;
+    *nl += icut_interpolate(view_of(m), icut_of(m), qpos, qnrm, order, nq, r_max * r_max, out, st);
+    return PM_OK;
+}
+
+pm_status pm_icut_build(pm_map* m, const pm_icut_desc* cut, const pm_query_desc* node_query,
+                        const float* d_node_normals4, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!cut) return fail(m, PM_ERR_INVALID, "cut descriptor is NULL");
+    pm_status s = validate_desc(m, node_query, false);
+    if (s != PM_OK) return s;
+    if (cut->refine_iters > 64) return fail(m, PM_ERR_INVALID, "refine_iters must be at most 64");
+    if (!(cut->accuracy >= 0.0f) || !std::isfinite(cut->accuracy))
+        return fail(m, PM_ERR_INVALID, "accuracy must be finite and >= 0");
+    if (d_node_normals4 && !aligned16(d_node_normals4))
+        return fail(m, PM_ERR_INVALID, "node normals must be 16-byte aligned");
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    s = icut_prepare_now(m, st);
+    if (s != PM_OK) return s;
+    const uint32_t ns = m->icut_slots;
+    const MapView v = view_of(m);
+    const IcutBuffers b = icut_of(m);
+    const IcutParams p{cut->use_leafs != 0, cut->level_emin, cut->refine_iters, cut->accuracy};
+    int nl = icut_normals(v, ns, reinterpret_cast<const float4*>(d_node_normals4), b, st);
+    nl += icut_coarse(v, ns, p, b, st);
+    // irradiance at every slot centre with the slot's normal (PhotonMap.cpp:371-384)
+    if (node_query->mode == PM_MODE_ZHOU_COMPAT) {
+        s = compat_run(m, node_query, reinterpret_cast<const float*>(b.center), reinterpret_cast<const float*>(b.normal),
+                       ns, nullptr, reinterpret_cast<float*>(b.exact), nullptr, nullptr, st);
+        if (s != PM_OK) return s;
+    } else {
+        s = ensure_query_capacity(m, ns, st);
+        if (s != PM_OK) return s;
+        const uint32_t* order = node_query->order == PM_ORDER_SORTED ? sort_queries(m, b.center, ns, st, &nl) : nullptr;
+        QueryOutputs out{b.exact, nullptr, nullptr, nullptr};
+        QueryTuning t = tuning_of(m);
+        t.stats = nullptr;
+        nl += query_knn(v, params_of(node_query), b.center, b.normal, order, ns, out, P<uint32_t>(m->counter),
+                        P<uint32_t>(m->fixq), t, st);
+    }
+    nl += icut_final(v, ns, p, b, st);
+    m->launches += (uint64_t)nl;
+    s = check_cuda(m, "pm_icut_build");
+    if (s != PM_OK) return s;
+    m->icut_gen = m->build_gen;
+    return PM_OK;
+}
+
+pm_status pm_icut_slot_count(pm_map* m, uint32_t* count) {
+    if (!m || !count) return fail(m, PM_ERR_INVALID, "count is NULL");
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    MapHeader h;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&h, m->hdr.ptr, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return check_cuda(m, "pm_icut_slot_count");
+    *count = 2 * (h.num_nodes + 1);
+    return PM_OK;
+}
+
+pm_status pm_icut_node_centers(pm_map* m, float* d_centers4, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!d_centers4 || !aligned16(d_centers4)) return fail(m, PM_ERR_INVALID, "centres must be a 16-byte aligned array");
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    pm_status s = icut_prepare_now(m, st);
+    if (s != PM_OK) return s;
+    cudaMemcpyAsync(d_centers4, m->ic_center.ptr, (size_t)m->icut_slots * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    return check_cuda(m, "pm_icut_node_centers");
+}
+
+pm_status pm_icut_interpolate(pm_map* m, float r_max, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
+                              float* d_irr4, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    if (!(r_max > 0.0f) || !std::isfinite(r_max))
+        return fail(m, PM_ERR_INVALID, "r_max must be finite and > 0 (got %g)", (double)r_max);
+    if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_irr4))
+        return fail(m, PM_ERR_INVALID, "query positions, normals and output must be non-NULL");
+    if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_irr4)))
+        return fail(m, PM_ERR_INVALID, "query and output arrays must be 16-byte aligned");
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (m->icut_gen != m->build_gen)
+        return fail(m, PM_ERR_STATE, "no illumination cut for the current tree (call pm_icut_build)");
+    if (nq == 0) return PM_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    int nl = 0;
+    pm_status s = icut_interp_run(m, r_max, reinterpret_cast<const float4*>(d_qpos4),
+                                  reinterpret_cast<const float4*>(d_qnrm4), nq, true, reinterpret_cast<float4*>(d_irr4),
+                                  st, &nl);
+    if (s != PM_OK) return s;
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_icut_interpolate");
+}
+
+pm_status pm_icut_export(pm_map* m, uint32_t max_slots, uint32_t* h_coarse, uint32_t* h_final, uint32_t* h_level,
+                         float* h_center4, float* h_normal4, float* h_est4, float* h_exact4) {
+    if (!m) return PM_ERR_INVALID;
+    if (!m->built || m->icut_gen != m->build_gen)
+        return fail(m, PM_ERR_STATE, "no illumination cut for the current tree (call pm_icut_build)");
+    const uint32_t ns = m->icut_slots;
+    if (max_slots < ns) return fail(m, PM_ERR_INVALID, "need room for %u slots", ns);
+    if (cudaDeviceSynchronize() != cudaSuccess) return check_cuda(m, "pm_icut_export");
+    struct Out { void* dst; const DevBuf* src; size_t elem; } outs[] = {
+        {h_coarse, &m->ic_coarse, 4}, {h_final, &m->ic_fin, 4}, {h_level, &m->ic_level, 4},
+        {h_center4, &m->ic_center, 16}, {h_normal4, &m->ic_normal, 16}, {h_est4, &m->ic_est, 16},
+        {h_exact4, &m->ic_exact, 16}};
+    for (const Out& o : outs)
+        if (o.dst && cudaMemcpy(o.dst, o.src->ptr, (size_t)ns * o.elem, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return check_cuda(m, "pm_icut_export");
+    return PM_OK;
 }
 
 pm_status pm_scale_flux(pm_map* m, float scale, void* stream) {

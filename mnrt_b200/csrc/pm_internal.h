@@ -148,6 +148,35 @@ int compat_node_estimates(const MapView& m, uint32_t max_slots, float rmax, uint
 int compat_query(const MapView& m, const float* est, const QueryParams& p, uint32_t iters, const float4* qpos,
                  const float4* qnrm, uint32_t nq, float* out_radius, const QueryOutputs& out, cudaStream_t st);
 
+// pm_icut.cu: illumination cuts.  Per-slot arrays hold 2 (num_nodes + 1)
+// entries (slot 2j + side of node j, slot 0 = root); pslot holds one entry
+// per node.
+struct IcutParams {
+    bool use_leafs;
+    uint32_t level_emin;
+    uint32_t refine_iters;
+    float accuracy;
+};
+struct IcutBuffers {
+    uint32_t* pslot;             // node -> slot referencing it
+    uint32_t* level;             // slot depth (root 0), kInvalid for empty slots
+    uint2* range;                // slot photons [x, y) in tree order
+    float4* center;              // box centre xyz, largest box side w
+    float4* normal;              // normal xyz (zero: none)
+    float4* est;                 // photon-sum estimate E~ (rgb)
+    float4* exact;               // estimate at the centre (rgb, w = photons used)
+    uint32_t* coarse;            // coarse cut marks
+    uint32_t* fin;               // final cut marks
+    uint32_t* work[2];           // work flags (refinement), mark scratch (coarse cut)
+    unsigned long long* acc;     // level statistics: max bits [0..2], fixed sums [3..5], count [6]
+};
+int icut_prepare(const MapView& m, uint32_t num_nodes, const IcutBuffers& b, cudaStream_t st);
+int icut_normals(const MapView& m, uint32_t nslots, const float4* caller, const IcutBuffers& b, cudaStream_t st);
+int icut_coarse(const MapView& m, uint32_t nslots, const IcutParams& p, const IcutBuffers& b, cudaStream_t st);
+int icut_final(const MapView& m, uint32_t nslots, const IcutParams& p, const IcutBuffers& b, cudaStream_t st);
+int icut_interpolate(const MapView& m, const IcutBuffers& b, const float4* qpos, const float4* qnrm,
+                     const uint32_t* order, uint32_t nq, float r2, float4* out, cudaStream_t st);
+
 // pm_gather.cu
 int gather_normals(const float4* hit_nrm, const float4* ray_dir, uint32_t n, float4* out_nrm, cudaStream_t st);
 int gather_accumulate(const float4* est, const float4* hit_pos, const float4* ray_origin, const float4* influence,

@@ -258,6 +258,8 @@ class PhotonMap:
         n = C.c_uint32(0)
         L.check(self._lib.pm_merged_count(self._h, C.byref(n)), self._h)
         self.num_photons = int(n.value)
+        if getattr(self, "_icut", None) is not None and self.num_photons > 0:
+            self.icut_build(stream=stream, **self._icut)   # PhotonMap.cpp:166-168
         return True
 
     def clear(self) -> None:
@@ -276,6 +278,8 @@ class PhotonMap:
         box filter, estimates from fewer than 8 photons zeroed."""
         kw.setdefault("filter", "box")
         kw.setdefault("min_found", 8)
+        if getattr(self, "_icut", None) is not None:
+            kw.setdefault("mode", L.PM_MODE_ICUT)   # GatherFor with illumination cuts (PhotonMap.cpp:244-257)
         d = self.desc(**kw)
         n = int(sp.pt_inter.shape[0])
         L.check(self._lib.pm_gather_for(self._h, C.byref(d), _ptr(sp.pt_inter), _ptr(sp.normals_s), _ptr(rays.dirs),
@@ -286,14 +290,17 @@ class PhotonMap:
     def gather(self, sp: ShadingPoints, rays: RayChunk, clr_diff_hit: torch.Tensor, io_radiance: torch.Tensor,
                stream=None, **kw) -> None:
         """PhotonMap::Gather (PhotonMap.cpp:195-232): GatherFor with the
-        shading points themselves as targets and no distance accumulator."""
+        shading points themselves as targets and no distance accumulator.
+        Never uses illumination cuts (the reference disables them here,
+        PhotonMap.cpp:206-224)."""
+        kw.setdefault("mode", L.PM_MODE_EXACT)
         self.gather_for(sp, rays, clr_diff_hit, None, io_radiance, None, stream=stream, **kw)
 
     def visualize(self, sp: ShadingPoints, rays: RayChunk, io_radiance: torch.Tensor, stream=None) -> None:
         """PhotonMap::Visualize (PhotonMap.cpp:272-285): the nearest photon
         within 5 % of the global radius, white, no photon-count rule."""
         self.gather_for(sp, rays, None, None, io_radiance, None, stream=stream, k=1, r_max=0.05 * self.r_max,
-                        min_found=0)
+                        min_found=0, mode=L.PM_MODE_EXACT)
 
     def compute_query_radii(self, qpos: torch.Tensor, out: torch.Tensor | None = None, stream=None,
                             **kw) -> torch.Tensor:
@@ -307,3 +314,54 @@ class PhotonMap:
         L.check(self._lib.pm_compute_query_radii(self._h, C.byref(d), _ptr(qpos), nq, _ptr(out), _stream(stream)),
                 self._h)
         return out
+
+    # -- illumination cuts (PhotonMap.cpp:287-452, GPU/illumcut.cu) -------------------
+    def set_illum_cuts(self, enabled: bool = True, use_leafs: bool = True, level_emin: int = 12,
+                       refine_iters: int = 4, accuracy: float = 0.2, **node_query) -> None:
+        """MNRTSettings::SetUseIllumCuts and the ICut* settings (defaults as
+        MNRTSettings.h:491-523): build_map then builds the cut and gather_for
+        with idx_shading_pts interpolates it, as the reference's GatherFor."""
+        self._icut = (dict(use_leafs=use_leafs, level_emin=level_emin, refine_iters=refine_iters, accuracy=accuracy,
+                           **node_query) if enabled else None)
+
+    def icut_build(self, use_leafs: bool = True, level_emin: int = 12, refine_iters: int = 4,
+                   accuracy: float = 0.2, node_normals: torch.Tensor | None = None, stream=None, **kw) -> None:
+        """Builds the illumination cut of the current tree.  kw describes the
+        node-centre estimate (k, r_max, filter, min_found, mode); defaults are
+        the reference's: the map's k and R, box filter, 8 photons at least."""
+        kw.setdefault("filter", "box")
+        kw.setdefault("min_found", 8)
+        d = self.desc(**kw)
+        c = L.IcutDesc(int(bool(use_leafs)), int(level_emin), int(refine_iters), float(accuracy))
+        L.check(self._lib.pm_icut_build(self._h, C.byref(c), C.byref(d), _ptr(node_normals), _stream(stream)),
+                self._h)
+
+    def icut_slot_count(self) -> int:
+        n = C.c_uint32(0)
+        L.check(self._lib.pm_icut_slot_count(self._h, C.byref(n)), self._h)
+        return int(n.value)
+
+    def icut_node_centers(self, device="cuda", stream=None) -> torch.Tensor:
+        """(slots, 4): box centre xyz and largest box side per slot."""
+        out = torch.empty((self.icut_slot_count(), 4), dtype=torch.float32, device=device)
+        L.check(self._lib.pm_icut_node_centers(self._h, _ptr(out), _stream(stream)), self._h)
+        return out
+
+    def icut_interpolate(self, qpos: torch.Tensor, qnrm: torch.Tensor, r_max: float | None = None,
+                         stream=None) -> torch.Tensor:
+        nq = int(qpos.shape[0])
+        out = torch.empty((nq, 4), dtype=torch.float32, device=qpos.device)
+        r = self.r_max if r_max is None else r_max
+        L.check(self._lib.pm_icut_interpolate(self._h, float(r), _ptr(qpos), _ptr(qnrm), nq, _ptr(out),
+                                              _stream(stream)), self._h)
+        return out
+
+    def icut_export(self) -> dict:
+        """Host copies of the cut: coarse, final, level, center, normal, est, exact."""
+        import numpy as np
+        ns = self.icut_slot_count()
+        u = {k: np.empty(ns, np.uint32) for k in ("coarse", "final", "level")}
+        f = {k: np.empty((ns, 4), np.float32) for k in ("center", "normal", "est", "exact")}
+        L.check(self._lib.pm_icut_export(self._h, ns, *(u[k].ctypes.data for k in ("coarse", "final", "level")),
+                                         *(f[k].ctypes.data for k in ("center", "normal", "est", "exact"))), self._h)
+        return {**u, **f}

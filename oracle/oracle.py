@@ -52,6 +52,12 @@ def load() -> C.CDLL:
         "orc_radiance_fp64": (None, [P, P, P, P, u32, P, P, u32, f32, i32, f32, u32, P, i32]),
         "orc_compat": (None, [P, u32, P, P, P, P, u32, u32, f32, u32, i32, f32, u32, P, P, P, P, i32]),
         "orc_backward_fp64": (None, [P, P, P, P, u32, u32, P, P, u32, f32, i32, f32, u32, P, P, P]),
+        "orc_icut_slots": (None, [P, u32, P, P, P, P]),
+        "orc_icut_normals": (None, [P, u32, P, P, P]),
+        "orc_icut_estimate": (None, [P, u32, P, P, P, P, P]),
+        "orc_icut_coarse": (None, [P, u32, P, P, i32, u32, P, P]),
+        "orc_icut_final": (None, [P, u32, P, P, P, u32, f32, P]),
+        "orc_icut_interp": (None, [P, u32, P, P, P, P, P, P, u32, f32, P, P, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -163,6 +169,65 @@ def compat(nodes, tpos4, tpow4, q4, n4, k: int, r_max: float, iters: int = 2, fi
                    n4.ctypes.data, nq, k, r_max, iters, FILTER_IDS[filt], cone_k, min_found, radius.ctypes.data,
                    count.ctypes.data, r2.ctypes.data, rad.ctypes.data, threads)
     return radius, count, r2, rad
+
+
+def icut(nodes, tpow4, use_leafs: bool = True, level_emin: int = 12, normals=None):
+    """Illumination-cut slot records and coarse cut on an exported tree.
+
+    Returns a dict: level, first, end, center (ns, 4), normal (ns, 4) (the
+    given normals, or the photon-derived ones), est (ns, 4), coarse, emin."""
+    lib = load()
+    nodes = _c(nodes, np.uint32)
+    tpow4 = _c(tpow4, np.float32)
+    m = nodes.shape[0] - 1
+    ns = 2 * (m + 1)
+    level = np.empty(ns, np.uint32)
+    first = np.empty(ns, np.uint32)
+    end = np.empty(ns, np.uint32)
+    center = np.empty((ns, 4), np.float32)
+    lib.orc_icut_slots(nodes.ctypes.data, m, level.ctypes.data, first.ctypes.data, end.ctypes.data, center.ctypes.data)
+    if normals is None:
+        normal = np.empty((ns, 4), np.float32)
+        lib.orc_icut_normals(tpow4.ctypes.data, ns, first.ctypes.data, end.ctypes.data, normal.ctypes.data)
+    else:
+        normal = _c(normals, np.float32).copy()
+        normal[:, 3] = 0.0
+    est = np.empty((ns, 4), np.float32)
+    lib.orc_icut_estimate(tpow4.ctypes.data, ns, first.ctypes.data, end.ctypes.data, center.ctypes.data,
+                          normal.ctypes.data, est.ctypes.data)
+    coarse = np.empty(ns, np.uint32)
+    emin = np.full(3, np.nan, np.float32)
+    lib.orc_icut_coarse(nodes.ctypes.data, m, level.ctypes.data, est.ctypes.data, int(bool(use_leafs)), level_emin,
+                        coarse.ctypes.data, emin.ctypes.data)
+    return {"level": level, "first": first, "end": end, "center": center, "normal": normal, "est": est,
+            "coarse": coarse, "emin": emin}
+
+
+def icut_final(nodes, coarse, est4, exact4, iters: int = 4, accuracy: float = 0.2):
+    """Final cut marks from a coarse cut and the node-centre irradiance."""
+    lib = load()
+    nodes = _c(nodes, np.uint32)
+    coarse = _c(coarse, np.uint32)
+    est4, exact4 = _c(est4, np.float32), _c(exact4, np.float32)
+    m = nodes.shape[0] - 1
+    fin = np.empty(2 * (m + 1), np.uint32)
+    lib.orc_icut_final(nodes.ctypes.data, m, coarse.ctypes.data, est4.ctypes.data, exact4.ctypes.data, iters,
+                       accuracy, fin.ctypes.data)
+    return fin
+
+
+def icut_interp(nodes, fin, center4, normal4, exact4, q4, n4, r_max: float, threads: int = 0):
+    """Irradiance interpolated from a cut: (irr (nq, 3) FP64, cut slots reached (nq,))."""
+    lib = load()
+    nodes, fin = _c(nodes, np.uint32), _c(fin, np.uint32)
+    center4, normal4, exact4, q4, n4 = (_c(a, np.float32) for a in (center4, normal4, exact4, q4, n4))
+    nq = q4.shape[0]
+    out = np.empty((nq, 3), np.float64)
+    reached = np.empty(nq, np.uint32)
+    lib.orc_icut_interp(nodes.ctypes.data, nodes.shape[0] - 1, fin.ctypes.data, center4.ctypes.data,
+                        normal4.ctypes.data, exact4.ctypes.data, q4.ctypes.data, n4.ctypes.data, nq, r_max,
+                        out.ctypes.data, reached.ctypes.data, threads)
+    return out, reached
 
 
 def threads_available() -> int:

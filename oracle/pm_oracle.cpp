@@ -656,3 +656,278 @@ void orc_compat(const uint32_t* nodes, uint32_t m, const float* tpos4, const flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Illumination cuts restated on the engine's exported tree (slot 0 = root,
+// slots 2j and 2j + 1 = children of internal node j), following
+// PhotonMap::OnFinalNodeList / GenerateFinalIllumCut (PhotonMap.cpp:287-452),
+// the kernels of GPU/illumcut.cu and dev_InterpolateNodeIrradiance
+// (GPU/photon_knn.cu:338-433), with the engine's stated choices: slots are the
+// tree nodes; a slot's photon sums run lane-strided over 32 partial sums
+// combined by the butterfly 16, 8, 4, 2, 1; the level mean is an exact 64-bit
+// fixed-point sum (scale 2^40 / largest |E~|); the refinement's race between
+// "finished" and "re-added by the parent" resolves to re-added; interpolation
+// visits the slots whose box lies within R.  The cover pass below is the
+// reference's literal top-down level loop (illumcut.cu:384-440).
+namespace {
+
+constexpr uint32_t kIcutLimit = 5000;   // ICUT_PHOTONLIMIT, illumcut.cu:74
+constexpr uint32_t kInv = 0xffffffffu;
+
+float butterfly32(float p[32]) {
+    for (int o = 16; o; o >>= 1) {
+        float q[32];
+        for (int l = 0; l < 32; ++l) q[l] = p[l] + p[l ^ o];
+        std::memcpy(p, q, sizeof(q));
+    }
+    return p[0];
+}
+
+inline float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    float a = ax * bx, b = ay * by, c = az * bz;
+    float s = a + b;
+    return s + c;
+}
+
+void icut_range(const CompatTree& t, uint32_t sid, uint32_t* first, uint32_t* end) {
+    const CSlot s = t.slot(sid);
+    if (s.cnt > 0) { first[sid] = s.ref; end[sid] = s.ref + s.cnt; return; }
+    const uint32_t a = s.ref << 1, b = a | 1u;
+    icut_range(t, a, first, end);
+    icut_range(t, b, first, end);
+    first[sid] = std::min(first[a], first[b]);
+    end[sid] = std::max(end[a], end[b]);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Slot records: level (kInv for empty slots), photon range [first, end),
+// centre xyz + largest side (center4).
+void orc_icut_slots(const uint32_t* nodes, uint32_t m, uint32_t* level, uint32_t* first, uint32_t* end,
+                    float* center4) {
+    CompatTree t{nodes, m, nullptr, nullptr};
+    const uint32_t ns = 2 * (m + 1);
+    for (uint32_t s = 0; s < ns; ++s) {
+        level[s] = kInv; first[s] = end[s] = 0;
+        for (int a = 0; a < 4; ++a) center4[4 * s + a] = 0.0f;
+    }
+    if (t.slot(0).ref == kInv) return;
+    icut_range(t, 0, first, end);
+    std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
+    while (!stack.empty()) {
+        const auto [sid, lvl] = stack.back();
+        stack.pop_back();
+        const CSlot s = t.slot(sid);
+        level[sid] = lvl;
+        float e[3];
+        for (int a = 0; a < 3; ++a) {
+            e[a] = s.hi[a] - s.lo[a];
+            center4[4 * sid + a] = s.lo[a] + 0.5f * e[a];
+        }
+        center4[4 * sid + 3] = std::max(e[0], std::max(e[1], e[2]));
+        if (s.cnt == 0) {
+            stack.push_back({s.ref << 1, lvl + 1});
+            stack.push_back({(s.ref << 1) | 1u, lvl + 1});
+        }
+    }
+}
+
+// Normal per slot from its photons (normalised sum of -d/|d|), slots of
+// fewer than 5,000 photons; zero otherwise.
+void orc_icut_normals(const float* tpow4, uint32_t ns, const uint32_t* first, const uint32_t* end, float* normal4) {
+    for (uint32_t s = 0; s < ns; ++s) {
+        float p[3][32] = {{0}};
+        const uint32_t cnt = end[s] - first[s];
+        if (cnt > 0 && cnt < kIcutLimit) {
+            for (uint32_t i = first[s]; i < end[s]; ++i) {
+                const int l = (int)((i - first[s]) & 31u);
+                float d[3];
+                oct_decode(f2u(tpow4[4 * (size_t)i + 3]), d);
+                const float len = std::sqrt(dot3(d[0], d[1], d[2], d[0], d[1], d[2]));
+                if (len > 0.0f)
+                    for (int a = 0; a < 3; ++a) p[a][l] = p[a][l] - d[a] / len;
+            }
+        }
+        float v[3];
+        for (int a = 0; a < 3; ++a) v[a] = butterfly32(p[a]);
+        const float l = std::sqrt(dot3(v[0], v[1], v[2], v[0], v[1], v[2]));
+        for (int a = 0; a < 3; ++a) normal4[4 * s + a] = l > 0.0f ? v[a] / l : 0.0f;
+        normal4[4 * s + 3] = 0.0f;
+    }
+}
+
+// Photon-sum estimate E~ = sum(front * flux) / side^2 (illumcut.cu:151-209).
+void orc_icut_estimate(const float* tpow4, uint32_t ns, const uint32_t* first, const uint32_t* end,
+                       const float* center4, const float* normal4, float* est4) {
+    for (uint32_t s = 0; s < ns; ++s) {
+        const float* n = normal4 + 4 * s;
+        const uint32_t cnt = end[s] - first[s];
+        const bool eval = cnt > 0 && cnt < kIcutLimit && dot3(n[0], n[1], n[2], n[0], n[1], n[2]) > 0.0f;
+        float p[3][32] = {{0}};
+        if (eval) {
+            for (uint32_t i = first[s]; i < end[s]; ++i) {
+                const int l = (int)((i - first[s]) & 31u);
+                const float* w = tpow4 + 4 * (size_t)i;
+                if (front_f32(n[0], n[1], n[2], f2u(w[3])))
+                    for (int a = 0; a < 3; ++a) p[a][l] = p[a][l] + w[a];
+            }
+        }
+        float v[3];
+        for (int a = 0; a < 3; ++a) v[a] = butterfly32(p[a]);
+        const float side = center4[4 * s + 3];
+        const bool ok = eval && side > 0.0f;
+        const float a2 = side * side;
+        for (int a = 0; a < 3; ++a) est4[4 * s + a] = ok ? v[a] / a2 : 0.0f;
+        est4[4 * s + 3] = 0.0f;
+    }
+}
+
+// Coarse cut: every leaf, or E_min marks -> remove parents -> cover pass.
+// emin_out (3 floats, may be NULL) receives E_min.
+void orc_icut_coarse(const uint32_t* nodes, uint32_t m, const uint32_t* level, const float* est4, int use_leafs,
+                     uint32_t level_emin, uint32_t* coarse, float* emin_out) {
+    CompatTree t{nodes, m, nullptr, nullptr};
+    const uint32_t ns = 2 * (m + 1);
+    if (use_leafs) {
+        for (uint32_t s = 0; s < ns; ++s) {
+            const CSlot c = t.slot(s);
+            coarse[s] = (c.ref != kInv && c.cnt > 0) ? 1u : 0u;
+        }
+        return;
+    }
+    // E_min: mean of the nonzero estimates on level_emin (illumcut.cu:587-625)
+    float mx[3] = {0, 0, 0};
+    uint64_t count = 0;
+    auto on_level = [&](uint32_t s) {
+        const float* e = est4 + 4 * s;
+        return level[s] == level_emin && !(e[0] == 0.0f && e[1] == 0.0f && e[2] == 0.0f);
+    };
+    for (uint32_t s = 0; s < ns; ++s) {
+        if (!on_level(s)) continue;
+        ++count;
+        for (int a = 0; a < 3; ++a) mx[a] = std::max(mx[a], std::fabs(est4[4 * s + a]));
+    }
+    double scale[3];
+    int64_t sum[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a) scale[a] = mx[a] > 0.0f ? 1099511627776.0 / (double)mx[a] : 0.0;
+    for (uint32_t s = 0; s < ns; ++s) {
+        if (!on_level(s)) continue;
+        for (int a = 0; a < 3; ++a) sum[a] += (int64_t)std::llrint((double)est4[4 * s + a] * scale[a]);
+    }
+    float emin[3];
+    for (int a = 0; a < 3; ++a) {
+        if (count == 0) emin[a] = INFINITY;
+        else if (scale[a] == 0.0) emin[a] = 0.0f;
+        else emin[a] = (float)(((double)sum[a] / scale[a]) / (double)count);
+        if (emin_out) emin_out[a] = emin[a];
+    }
+    std::vector<uint32_t> mark0(ns), mark(ns), covered(ns, 0u);
+    uint32_t max_level = 0;
+    for (uint32_t s = 0; s < ns; ++s) {
+        const float* e = est4 + 4 * s;
+        mark0[s] = (level[s] != kInv && e[0] >= emin[0] && e[1] >= emin[1] && e[2] >= emin[2]) ? 1u : 0u;
+        if (level[s] != kInv) max_level = std::max(max_level, level[s]);
+    }
+    // kernel_RemoveParents (illumcut.cu:352-370)
+    for (uint32_t s = 0; s < ns; ++s) {
+        mark[s] = mark0[s];
+        const CSlot c = t.slot(s);
+        if (c.ref != kInv && c.cnt == 0) {
+            const uint32_t l = mark0[2 * c.ref], r = mark0[2 * c.ref + 1];
+            if ((l == 1 && r == 1) || (l == 0 && r == 0)) mark[s] = 0;
+        }
+    }
+    // kernel_UpdateCoveredState, level by level from the root (illumcut.cu:384-440)
+    for (uint32_t lvl = 0; lvl <= max_level; ++lvl) {
+        for (uint32_t s = 0; s < ns; ++s) {
+            if (level[s] != lvl) continue;
+            const CSlot c = t.slot(s);
+            uint32_t my_mark = mark[s];
+            if (c.cnt > 0) {
+                if (covered[s] == 0) my_mark = 1;
+            } else {
+                const uint32_t l = 2 * c.ref, r = l + 1;
+                uint32_t ml = mark[l], mr = mark[r], cl, cr;
+                if (covered[s] == 1) { ml = 0; mr = 0; cl = 1; cr = 1; }
+                else { cl = ml; cr = mr; }
+                mark[l] = ml; mark[r] = mr; covered[l] = cl; covered[r] = cr;
+            }
+            mark[s] = my_mark;
+        }
+    }
+    for (uint32_t s = 0; s < ns; ++s) coarse[s] = level[s] != kInv ? mark[s] : 0u;
+}
+
+// Final cut from the coarse cut (illumcut.cu:488-519, PhotonMap.cpp:387-452).
+void orc_icut_final(const uint32_t* nodes, uint32_t m, const uint32_t* coarse, const float* est4, const float* exact4,
+                    uint32_t iters, float accuracy, uint32_t* fin) {
+    CompatTree t{nodes, m, nullptr, nullptr};
+    const uint32_t ns = 2 * (m + 1);
+    std::vector<uint32_t> work(coarse, coarse + ns), next(ns);
+    for (uint32_t s = 0; s < ns; ++s) fin[s] = 0;
+    for (uint32_t it = 0; it < iters; ++it) {
+        if (std::none_of(work.begin(), work.end(), [](uint32_t w) { return w != 0; })) break;
+        std::fill(next.begin(), next.end(), 0u);
+        for (uint32_t s = 0; s < ns; ++s) {
+            if (!work[s]) continue;
+            const CSlot c = t.slot(s);
+            if (c.ref == kInv) continue;
+            const float* a = est4 + 4 * s;
+            const float* b = exact4 + 4 * s;
+            bool ok = true;
+            for (int k = 0; k < 3; ++k) ok = ok && std::fabs(a[k] - b[k]) < accuracy * b[k];
+            ok = ok || c.cnt > 0;
+            if (ok) fin[s] = 1;
+            else { next[2 * c.ref] = 1; next[2 * c.ref + 1] = 1; }
+        }
+        work.swap(next);
+    }
+    for (uint32_t s = 0; s < ns; ++s)
+        if (work[s]) fin[s] = 1;
+}
+
+// Interpolation at queries (dev_InterpolateNodeIrradiance, photon_knn.cu:
+// 338-433): out (3 nq doubles), reached (nq, cut slots reached).
+void orc_icut_interp(const uint32_t* nodes, uint32_t m, const uint32_t* fin, const float* center4,
+                     const float* normal4, const float* exact4, const float* q4, const float* n4, uint32_t nq,
+                     float R, double* out, uint32_t* reached, int nthreads) {
+    CompatTree t{nodes, m, nullptr, nullptr};
+    const float r2 = R * R;
+    parallel_for_blocks(nq, 64, nthreads, [&](int64_t b, int64_t e) {
+        for (int64_t q = b; q < e; ++q) {
+            const float qx = q4[4 * q], qy = q4[4 * q + 1], qz = q4[4 * q + 2];
+            const float* qn = n4 + 4 * q;
+            double acc[3] = {0, 0, 0}, ws = 0.0;
+            uint32_t nr = 0;
+            std::vector<uint32_t> stack{0u};
+            while (!stack.empty()) {
+                const uint32_t sid = stack.back();
+                stack.pop_back();
+                const CSlot s = t.slot(sid);
+                if (s.ref == kInv || !(box_lb_f32(qx, qy, qz, s.lo, s.hi) < r2)) continue;
+                if (s.cnt == 0 && !fin[sid]) {
+                    stack.push_back(s.ref << 1);
+                    stack.push_back((s.ref << 1) | 1u);
+                    continue;
+                }
+                ++nr;
+                const float* nn = normal4 + 4 * sid;
+                if (dot3(nn[0], nn[1], nn[2], nn[0], nn[1], nn[2]) == 0.0f) continue;
+                const float* c = center4 + 4 * sid;
+                const float dist = std::sqrt(d2_f32(qx, qy, qz, c[0], c[1], c[2]));
+                if (!(c[3] > 0.0f)) continue;
+                const float tt = dist / c[3];
+                const float rbf = tt <= 1.0f ? 1.0f - tt * tt : 0.0f;
+                const float w = rbf * std::max(0.0f, dot3(nn[0], nn[1], nn[2], qn[0], qn[1], qn[2]));
+                for (int a = 0; a < 3; ++a) acc[a] += (double)w * (double)exact4[4 * sid + a];
+                ws += (double)w;
+            }
+            for (int a = 0; a < 3; ++a) out[3 * q + a] = ws != 0.0 ? acc[a] / ws : 0.0;
+            reached[q] = nr;
+        }
+    });
+}
+
+}  // extern "C"

@@ -125,6 +125,32 @@ int main() {
     for (const float4& r : ra) any = any || r.x > 0.0f;
     if (!any) return fail("GatherFor produced no radiance");
 
+    // ---- GatherFor from the illumination cut (MNRTSettings' default: cuts on,
+    // the leaves as the coarse cut), against the same calls on the C ABI
+    pmgpu::PhotonMap pmc(n, make_float3(0, 0, 0), make_float3(1, 1, 1), 0.1f);
+    pmc.SetUseIllumCuts(true);
+    pmc.SetKNNTargetCount(50);
+    pmc.Merge(traced, d_valid);
+    pmc.ScaleFlux(0.5f);
+    pmc.BuildMap();
+    float4 *d_rad_c = to_device(zero4), *d_rad_d = to_device(zero4);
+    float *d_rec_c = to_device(zero1), *d_rec_d = to_device(zero1);
+    pmc.GatherFor(sp, rc, d_clr, d_idx, d_rad_c, d_rec_c);
+    pm_icut_desc cd;
+    cd.use_leafs = 1; cd.level_emin = 12; cd.refine_iters = 4; cd.accuracy = 0.2f;
+    if (pm_icut_build(raw, &cd, &d, nullptr, nullptr) != PM_OK) return fail("pm_icut_build");
+    pm_query_desc di = d;
+    di.mode = PM_MODE_ICUT;
+    if (pm_gather_for(raw, &di, (const float*)d_qpos, (const float*)d_qnrm, (const float*)d_dir, (const float*)d_ori,
+                      (const float*)d_infl, (const float*)d_clr, d_idx, nq, (float*)d_rad_d, d_rec_d, nullptr) != PM_OK)
+        return fail("pm_gather_for (PM_MODE_ICUT)");
+    cudaDeviceSynchronize();
+    const std::vector<float4> rc_ = to_host(d_rad_c, nq), rd_ = to_host(d_rad_d, nq);
+    if (std::memcmp(rc_.data(), rd_.data(), nq * sizeof(float4)) != 0) return fail("GatherFor (cut) radiance");
+    bool any_cut = false;
+    for (const float4& r : rc_) any_cut = any_cut || r.x > 0.0f;
+    if (!any_cut) return fail("GatherFor (cut) produced no radiance");
+
     // ---- KDTreePoint over the photon positions: the reference's radius estimate
     float* d_radii_a = to_device(zero1);
     float* d_radii_b = to_device(zero1);

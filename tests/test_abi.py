@@ -132,3 +132,28 @@ def test_batch_validation_without_gpu(engine_lib):
     assert lib.pm_batch_launch(h, None) == L.PM_ERR_STATE
     assert lib.pm_batch_set_tuning(h, 0, 4, 8, 1) == L.PM_ERR_INVALID
     assert lib.pm_batch_destroy(h) == L.PM_OK
+
+
+def test_icut_validation_without_gpu(engine_lib):
+    lib = engine_lib
+    h = _create(lib)
+    d = L.QueryDesc(k=10, r_max=0.1, filter=L.PM_FILTER_BOX, cone_k=1.0, mode=0, min_found=8, order=0, refine_iters=2)
+    cut = L.IcutDesc(1, 12, 4, 0.2)
+    assert lib.pm_icut_build(h, None, C.byref(d), None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_build(h, C.byref(cut), None, None, None) == L.PM_ERR_INVALID
+    for bad in (L.IcutDesc(1, 12, 65, 0.2), L.IcutDesc(1, 12, 4, -1.0), L.IcutDesc(1, 12, 4, float("nan"))):
+        assert lib.pm_icut_build(h, C.byref(bad), C.byref(d), None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_build(h, C.byref(cut), C.byref(d), 17, None) == L.PM_ERR_INVALID   # misaligned normals
+    assert lib.pm_icut_build(h, C.byref(cut), C.byref(d), None, None) == L.PM_ERR_STATE   # nothing built
+    icut_mode = L.QueryDesc(k=10, r_max=0.1, filter=0, cone_k=1.0, mode=L.PM_MODE_ICUT, min_found=0, order=0,
+                            refine_iters=2)
+    assert lib.pm_icut_build(h, C.byref(cut), C.byref(icut_mode), None, None) == L.PM_ERR_INVALID
+    assert lib.pm_query(h, C.byref(icut_mode), None, None, 0, None, None, None, None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_interpolate(h, 0.0, None, None, 0, None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_interpolate(h, 0.1, None, None, 4, None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_interpolate(h, 0.1, None, None, 0, None, None) == L.PM_ERR_STATE
+    n = C.c_uint32(7)
+    assert lib.pm_icut_slot_count(h, C.byref(n)) == L.PM_ERR_STATE
+    assert lib.pm_icut_node_centers(h, None, None) == L.PM_ERR_INVALID
+    assert lib.pm_icut_export(h, 0, None, None, None, None, None, None, None) == L.PM_ERR_STATE
+    lib.pm_destroy(h)
