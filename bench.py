@@ -437,6 +437,95 @@ def run_diff(args, cfg) -> dict:
     }
 
 
+def run_icut(args, cfg) -> dict:
+    """Final gathering with illumination cuts (the reference's default
+    GatherFor, PhotonMap.cpp:244-257): per step, build the tree and its cut
+    (leaves as the coarse cut, exact-kNN irradiance at every node centre,
+    4 refinement rounds, accuracy 0.2), then interpolate the cut at every
+    query.  Also times the photon-search estimate on the same queries."""
+    import torch
+    from mnrt_b200.photon_map import PhotonMap
+    from oracle import oracle
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    ph, q = make_inputs(cfg, 0)
+    N, Q, k, R = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"]
+    d_pos, d_pow = torch.from_numpy(ph.pos).to(dev), torch.from_numpy(ph.pow).to(dev)
+    d_qp, d_qn = torch.from_numpy(q.pos).to(dev), torch.from_numpy(q.nrm).to(dev)
+    pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
+    pm.reserve(N, Q)
+    out = torch.empty((Q, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    qdesc = dict(k=k, r_max=R, filter="box", min_found=8)
+
+    def step():
+        pm.build(d_pos, d_pow)
+        ev[1].record()
+        pm.icut_build(**qdesc)
+        ev[2].record()
+        pm._lib.pm_icut_interpolate(pm._h, float(R), d_qp.data_ptr(), d_qn.data_ptr(), Q, out.data_ptr(),
+                                     torch.cuda.current_stream().cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    tot, cut, interp = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(); step(); ev[3].record(); ev[3].synchronize()
+        tot.append(ev[0].elapsed_time(ev[3]))
+        cut.append(ev[1].elapsed_time(ev[2]))
+        interp.append(ev[2].elapsed_time(ev[3]))
+    # the photon-search estimate on the same queries, for comparison
+    qo = {"rad": torch.empty((Q, 4), dtype=torch.float32, device=dev)}
+    for _ in range(args.warmup):
+        pm.query(d_qp, d_qn, out=qo, **qdesc)
+    knn = []
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(); pm.query(d_qp, d_qn, out=qo, **qdesc); ev[1].record(); ev[1].synchronize()
+        knn.append(ev[0].elapsed_time(ev[1]))
+    ns = pm.icut_slot_count()
+    cutx = pm.icut_export()
+    info = pm.info()
+    tot_ms, cut_ms, interp_ms, knn_ms = (float(np.mean(x)) for x in (tot, cut, interp, knn))
+    irr = out[:, :3].sum(1).cpu().numpy()
+    direct = qo["rad"][:, :3].sum(1).cpu().numpy()
+    ok = direct > 0
+    ratio = irr[ok] / direct[ok]
+    res = {
+        "metric": "final-gather irradiance from the illumination cut: queries/s (build + cut + interpolation per step)",
+        "value": Q / (tot_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f32 (interpolation sums in f64)", "data": "synthetic",
+        "config": {"workload": cfg["workload"] + "; illumination cut: leaves as coarse cut, 4 refinement rounds, "
+                               "accuracy 0.2, node-centre estimate exact kNN (box, min_found 8)",
+                   "photons": N, "queries": Q, "k": k, "r_max": R,
+                   "l2": "flushed between steps (256 MiB write, untimed)"},
+        "step_ms": tot_ms, "build_ms": tot_ms - cut_ms - interp_ms, "cut_build_ms": cut_ms,
+        "interpolation_ms": interp_ms, "interpolation_queries_per_s": Q / (interp_ms / 1000.0),
+        "knn_query_ms": knn_ms, "interpolation_speedup_over_knn": knn_ms / interp_ms,
+        "slots": ns, "cut_slots": int(cutx["final"].sum()), "device_errors": info.device_errors,
+        "interp_over_knn_estimate": {"median": float(np.median(ratio)),
+                                     "p25": float(np.percentile(ratio, 25)), "p75": float(np.percentile(ratio, 75))},
+    }
+    if not args.no_cpu_baseline:
+        nodes, _tpos, _tpow = pm.export_tree()
+        threads = oracle.threads_available()
+        rng = np.random.default_rng(7)
+        sample = min(Q, 200000)
+        idx = rng.choice(Q, sample, replace=False)
+        t0 = time.perf_counter()
+        oracle.icut_interp(nodes, cutx["final"], cutx["center"], cutx["normal"], cutx["exact"], q.pos[idx],
+                           q.nrm[idx], R, threads)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": sample / dt, "unit": "queries/s", "cores": threads, "kind": "port",
+                               "sample": f"the oracle's interpolation over the engine's cut, {sample:,} random "
+                                         f"queries of {Q:,} (interpolation stage only)"}
+    pm.close()
+    return res
+
+
 def run_batch(args) -> dict:
     """Config 3: 64 photon maps (photon counts log-uniform in [1e4, 2e6], query
     counts log-uniform in [1e3, 1e6], k from {16, 32, 64, 128}, R = 0.05),
@@ -527,7 +616,7 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff", "batch"])
+    ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff", "batch", "icut"])
     ap.add_argument("--maps", type=int, default=64, help="maps of the batch workload")
     ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -541,7 +630,7 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    cfg = workload_config(args.config) if args.config != "batch" else None
+    cfg = workload_config("plain" if args.config == "icut" else args.config) if args.config != "batch" else None
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
@@ -552,6 +641,9 @@ def main(argv=None) -> int:
         return 0
     if args.config == "diff":
         print(json.dumps(run_diff(args, cfg)), flush=True)
+        return 0
+    if args.config == "icut":
+        print(json.dumps(run_icut(args, cfg)), flush=True)
         return 0
     res = run_ours(args, cfg)
     if res is not None:

@@ -297,8 +297,8 @@ PM_API pm_status pm_icut_slot_count(pm_map* map, uint32_t* count);
  * computes normals from its geometry before pm_icut_build.  Empty slots get
  * zeros. */
 PM_API pm_status pm_icut_node_centers(pm_map* map, float* d_centers4, void* stream);
-/* Irradiance interpolated from the cut at each query (xyz; w = cut nodes
- * reached): every cut node reached through nodes whose box lies within r_max
+/* Irradiance interpolated from the cut at each query (xyz; w = cut nodes of
+ * nonzero weight): every cut node reached through nodes whose box lies within r_max
  * of q contributes w = (1 - t^2) max(0, n_node . n_q), t = |centre - q| /
  * side <= 1; E = sum(w E_node) / sum(w), 0 when the weights sum to 0.  The
  * normal is used as given (the reference does not flip it here). */

@@ -31,7 +31,12 @@
 //   7. interpolation at a query q with normal n: every cut slot (or leaf)
 //      reached through slots whose box lies within R of q contributes
 //      w = (1 - t^2) * max(0, n_slot . n), t = |centre - q| / side <= 1;
-//      E(q) = sum(w E) / sum(w) (photon_knn.cu:338-433, 598-660)
+//      E(q) = sum(w E) / sum(w) (photon_knn.cu:338-433, 598-660).  A cut
+//      slot's weight is zero unless q lies in the cube of half-width side
+//      about its centre, so each slot also carries an influence box: the
+//      union of those cubes (slightly widened) over the cut slots where
+//      interpolation below it stops.  The traversal skips slots whose
+//      influence box misses q, which removes only zero terms.
 //
 // Determinism: sums over a slot's photons run lane-strided over one warp and
 // then down a fixed xor butterfly; the level mean of step 4 is an exact
@@ -351,9 +356,80 @@ __global__ void k_icut_finalize(uint32_t nslots, const uint32_t* __restrict__ wo
     if (s < nslots && work[s]) fin[s] = 1u;
 }
 
+// Order-preserving map of floats to unsigned keys (min/max by atomics).
+__device__ __forceinline__ uint32_t fkey(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void k_icut_ibox_init(uint32_t nslots, uint32_t* __restrict__ ibkey) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 6u * nslots) return;
+    ibkey[i] = (i % 6u) < 3u ? 0xffffffffu : 0u;   // lo keys start at +max, hi keys at 0
+}
+
+// Thread per slot where interpolation stops (a cut slot or a leaf with no
+// cut slot above it) and that can carry weight (a normal and a side): its
+// cube [c - h, c + h], h = side widened by 0.1 % plus a few units in the last
+// place of the coordinates, joins the influence box of the slot and of
+// every slot above it.
+__global__ void k_icut_ibox_scatter(const Node* __restrict__ nodes, uint32_t nslots, const uint32_t* __restrict__ pslot,
+                                    const uint32_t* __restrict__ fin, const float4* __restrict__ center,
+                                    const float4* __restrict__ normal, uint32_t* __restrict__ ibkey,
+                                    uint32_t* __restrict__ term) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const uint32_t ref = slot_ref(nodes, s);
+    bool stop = ref != kInvalid && (fin[s] != 0u || slot_cnt(nodes, s) > 0);
+    if (stop) {   // reachable only without a cut slot above it
+        uint32_t p = s > 1u ? pslot[s >> 1] : 0u;
+        for (int g = 0; g < kIcutMaxDepth && s > 1u; ++g) {
+            if (fin[p]) { stop = false; break; }
+            if (p == 0u) break;
+            p = pslot[p >> 1];
+        }
+    }
+    term[s] = stop ? 1u : 0u;
+    if (!stop) return;
+    const float4 c = center[s];
+    const float4 n = normal[s];
+    if (!(c.w > 0.0f) || dot3_rn(n.x, n.y, n.z, n.x, n.y, n.z) == 0.0f) return;
+    const float mag = __fadd_rn(__fadd_rn(__fadd_rn(fabsf(c.x), fabsf(c.y)), fabsf(c.z)), c.w);
+    const float h = __fadd_rn(__fmul_rn(c.w, 1.001f), __fmul_rn(mag, 3.814697265625e-06f));   // + mag * 2^-18
+    const uint32_t lo[3] = {fkey(__fsub_rn(c.x, h)), fkey(__fsub_rn(c.y, h)), fkey(__fsub_rn(c.z, h))};
+    const uint32_t hi[3] = {fkey(__fadd_rn(c.x, h)), fkey(__fadd_rn(c.y, h)), fkey(__fadd_rn(c.z, h))};
+    uint32_t t = s;
+    for (int g = 0; g < kIcutMaxDepth; ++g) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(ibkey + 6u * t + a, lo[a]);
+            atomicMax(ibkey + 6u * t + 3u + a, hi[a]);
+        }
+        if (t == 0u) break;
+        t = pslot[t >> 1];
+    }
+}
+
+__global__ void k_icut_ibox_decode(uint32_t nslots, const uint32_t* __restrict__ ibkey,
+                                   const uint32_t* __restrict__ term, float4* __restrict__ ibox) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const uint32_t* k = ibkey + 6u * s;
+    if (k[0] == 0xffffffffu) {   // nothing below carries weight: an empty box
+        ibox[2u * s] = make_float4(INFINITY, INFINITY, INFINITY, term[s] ? 1.0f : 0.0f);
+        ibox[2u * s + 1u] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+        return;
+    }
+    ibox[2u * s] = make_float4(fkey_inv(k[0]), fkey_inv(k[1]), fkey_inv(k[2]), term[s] ? 1.0f : 0.0f);
+    ibox[2u * s + 1u] = make_float4(fkey_inv(k[3]), fkey_inv(k[4]), fkey_inv(k[5]), 0.0f);
+}
+
 // Thread per query (Morton order when `order` is given): depth-first over the
 // slots whose box lies within R of q, stopping at cut slots and leaves.
-__global__ void __launch_bounds__(128) k_icut_interp(const Node* __restrict__ nodes, const uint32_t* __restrict__ fin,
+__global__ void __launch_bounds__(128) k_icut_interp(const Node* __restrict__ nodes, const float4* __restrict__ ibox,
                                                      const float4* __restrict__ center,
                                                      const float4* __restrict__ normal,
                                                      const float4* __restrict__ exact, const float4* __restrict__ qpos,
@@ -372,7 +448,6 @@ __global__ void __launch_bounds__(128) k_icut_interp(const Node* __restrict__ no
     double ax = 0.0, ay = 0.0, az = 0.0, ws = 0.0;
     uint32_t reached = 0;
     auto contribute = [&](uint32_t sid) {
-        ++reached;
         const float4 nn = __ldg(normal + sid);
         if (dot3_rn(nn.x, nn.y, nn.z, nn.x, nn.y, nn.z) == 0.0f) return;
         const float4 c = __ldg(center + sid);
@@ -381,36 +456,42 @@ __global__ void __launch_bounds__(128) k_icut_interp(const Node* __restrict__ no
         const float t = __fdiv_rn(dist, c.w);
         const float rbf = t <= 1.0f ? __fsub_rn(1.0f, __fmul_rn(t, t)) : 0.0f;
         const float w = __fmul_rn(rbf, fmaxf(0.0f, dot3_rn(nn.x, nn.y, nn.z, qn.x, qn.y, qn.z)));
+        if (w == 0.0f) return;
+        ++reached;
         const float4 e = __ldg(exact + sid);
         ax = __dadd_rn(ax, (double)w * (double)e.x);
         ay = __dadd_rn(ay, (double)w * (double)e.y);
         az = __dadd_rn(az, (double)w * (double)e.z);
         ws = __dadd_rn(ws, (double)w);
     };
-    uint32_t stack[kIcutStack];
-    int sp = 0;
-    {
+    // a slot is entered when its box lies within R of q and its influence box holds q
+    auto enter = [&](uint32_t sid, float4& ib_lo) -> bool {
         float lo[3], hi[3];
         uint32_t ref, cnt;
-        slot_load(nodes, 0u, lo, hi, ref, cnt);
-        if (ref != kInvalid && box_lb(q.x, q.y, q.z, lo, hi) < r2) {
-            if (cnt > 0 || __ldg(fin)) contribute(0u);
-            else stack[sp++] = ref;
-        }
+        slot_load(nodes, sid, lo, hi, ref, cnt);
+        if (ref == kInvalid || !(box_lb(q.x, q.y, q.z, lo, hi) < r2)) return false;
+        ib_lo = __ldg(ibox + 2u * sid);
+        const float4 ib_hi = __ldg(ibox + 2u * sid + 1u);
+        return q.x >= ib_lo.x && q.y >= ib_lo.y && q.z >= ib_lo.z && q.x <= ib_hi.x && q.y <= ib_hi.y &&
+               q.z <= ib_hi.z;
+    };
+    uint32_t stack[kIcutStack];
+    int sp = 0;
+    float4 ib;
+    if (enter(0u, ib)) {
+        if (ib.w != 0.0f) contribute(0u);
+        else stack[sp++] = 0u;
     }
     while (sp > 0) {
-        const uint32_t j = stack[--sp];
+        const uint32_t j = slot_ref(nodes, stack[--sp]);   // internal: node j
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
             const uint32_t sid = 2u * j + (uint32_t)side;
-            float lo[3], hi[3];
-            uint32_t ref, cnt;
-            slot_load(nodes, sid, lo, hi, ref, cnt);
-            if (ref == kInvalid || !(box_lb(q.x, q.y, q.z, lo, hi) < r2)) continue;
-            if (cnt > 0 || __ldg(fin + sid)) {
+            if (!enter(sid, ib)) continue;
+            if (ib.w != 0.0f) {
                 contribute(sid);
             } else if (sp < kIcutStack) {
-                stack[sp++] = ref;
+                stack[sp++] = sid;
             } else {
                 atomicOr(&hdr->errors, kErrStack);
             }
@@ -475,13 +556,18 @@ int icut_final(const MapView& m, uint32_t nslots, const IcutParams& p, const Icu
         ++nl;
     }
     k_icut_finalize<<<blocks(nslots, 256), 256, 0, st>>>(nslots, b.work[cur], b.fin);
-    return nl + 1;
+    // influence boxes of the final cut (b.work[cur ^ 1] holds the stop flags)
+    k_icut_ibox_init<<<blocks(6u * nslots, 256), 256, 0, st>>>(nslots, b.ibkey);
+    k_icut_ibox_scatter<<<blocks(nslots, 256), 256, 0, st>>>(m.nodes, nslots, b.pslot, b.fin, b.center, b.normal,
+                                                            b.ibkey, b.work[cur ^ 1]);
+    k_icut_ibox_decode<<<blocks(nslots, 256), 256, 0, st>>>(nslots, b.ibkey, b.work[cur ^ 1], b.ibox);
+    return nl + 4;
 }
 
 int icut_interpolate(const MapView& m, const IcutBuffers& b, const float4* qpos, const float4* qnrm,
                      const uint32_t* order, uint32_t nq, float r2, float4* out, cudaStream_t st) {
     if (!nq) return 0;
-    k_icut_interp<<<blocks(nq, 128), 128, 0, st>>>(m.nodes, b.fin, b.center, b.normal, b.exact, qpos, qnrm, order, nq,
+    k_icut_interp<<<blocks(nq, 128), 128, 0, st>>>(m.nodes, b.ibox, b.center, b.normal, b.exact, qpos, qnrm, order, nq,
                                                    r2, out, m.hdr);
     return 1;
 }

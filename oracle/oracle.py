@@ -217,7 +217,7 @@ def icut_final(nodes, coarse, est4, exact4, iters: int = 4, accuracy: float = 0.
 
 
 def icut_interp(nodes, fin, center4, normal4, exact4, q4, n4, r_max: float, threads: int = 0):
-    """Irradiance interpolated from a cut: (irr (nq, 3) FP64, cut slots reached (nq,))."""
+    """Irradiance interpolated from a cut: (irr (nq, 3) FP64, cut slots of nonzero weight (nq,))."""
     lib = load()
     nodes, fin = _c(nodes, np.uint32), _c(fin, np.uint32)
     center4, normal4, exact4, q4, n4 = (_c(a, np.float32) for a in (center4, normal4, exact4, q4, n4))

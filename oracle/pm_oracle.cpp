@@ -889,7 +889,7 @@ void orc_icut_final(const uint32_t* nodes, uint32_t m, const uint32_t* coarse, c
 }
 
 // Interpolation at queries (dev_InterpolateNodeIrradiance, photon_knn.cu:
-// 338-433): out (3 nq doubles), reached (nq, cut slots reached).
+// 338-433): out (3 nq doubles), reached (nq, cut slots of nonzero weight).
 void orc_icut_interp(const uint32_t* nodes, uint32_t m, const uint32_t* fin, const float* center4,
                      const float* normal4, const float* exact4, const float* q4, const float* n4, uint32_t nq,
                      float R, double* out, uint32_t* reached, int nthreads) {
@@ -912,7 +912,6 @@ void orc_icut_interp(const uint32_t* nodes, uint32_t m, const uint32_t* fin, con
                     stack.push_back((s.ref << 1) | 1u);
                     continue;
                 }
-                ++nr;
                 const float* nn = normal4 + 4 * sid;
                 if (dot3(nn[0], nn[1], nn[2], nn[0], nn[1], nn[2]) == 0.0f) continue;
                 const float* c = center4 + 4 * sid;
@@ -921,6 +920,8 @@ void orc_icut_interp(const uint32_t* nodes, uint32_t m, const uint32_t* fin, con
                 const float tt = dist / c[3];
                 const float rbf = tt <= 1.0f ? 1.0f - tt * tt : 0.0f;
                 const float w = rbf * std::max(0.0f, dot3(nn[0], nn[1], nn[2], qn[0], qn[1], qn[2]));
+                if (w == 0.0f) continue;
+                ++nr;
                 for (int a = 0; a < 3; ++a) acc[a] += (double)w * (double)exact4[4 * sid + a];
                 ws += (double)w;
             }

@@ -308,7 +308,6 @@ def icut_interp(nodes, fin, center, normal, exact, q4, n4, r_max):
             if cnt == 0 and not fin[sid]:
                 todo += [2 * ref, 2 * ref + 1]
                 continue
-            reached[qi] += 1
             nn = normal[sid]
             if _dot3(nn, nn) == 0 or not center[sid, 3] > 0:
                 continue
@@ -316,6 +315,9 @@ def icut_interp(nodes, fin, center, normal, exact, q4, n4, r_max):
             t = F32(F32(np.sqrt(_dot3(dq, dq))) / center[sid, 3])
             rbf = F32(F32(1) - F32(t * t)) if t <= 1 else F32(0)
             w = F32(rbf * max(F32(0), _dot3(nn, qn)))
+            if w == 0:
+                continue
+            reached[qi] += 1
             acc += float(w) * exact[sid, :3].astype(np.float64)
             ws += float(w)
         if ws != 0.0:
