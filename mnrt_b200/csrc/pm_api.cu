@@ -63,7 +63,7 @@ struct pm_map {
     uint32_t merged_n = 0, cap_merged = 0;
     // illumination cut of the current tree (pm_icut_*): per-slot arrays
     DevBuf ic_pslot, ic_level, ic_range, ic_center, ic_normal, ic_est, ic_exact, ic_coarse, ic_fin, ic_work0, ic_work1,
-        ic_acc, ic_ibox, ic_ibkey;
+        ic_acc, ic_ibox;
     uint32_t icut_slots = 0;
     uint64_t icut_prep_gen = ~0ull, icut_gen = ~0ull;
     uint64_t build_gen = 0, compat_gen = ~0ull;
@@ -320,7 +320,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
                      &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
                      &m->ic_normal, &m->ic_est, &m->ic_exact, &m->ic_coarse, &m->ic_fin, &m->ic_work0, &m->ic_work1,
-                     &m->ic_acc, &m->ic_ibox, &m->ic_ibkey};
+                     &m->ic_acc, &m->ic_ibox};
     for (DevBuf* b : all) buf_free(m, *b);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
@@ -669,7 +669,6 @@ static IcutBuffers icut_of(pm_map* m) {
     b.work[0] = P<uint32_t>(m->ic_work0); b.work[1] = P<uint32_t>(m->ic_work1);
     b.acc = P<unsigned long long>(m->ic_acc);
     b.ibox = P<float4>(m->ic_ibox);
-    b.ibkey = P<uint32_t>(m->ic_ibkey);
     return b;
 }
 
@@ -700,7 +699,6 @@ static pm_status icut_prepare_now(pm_map* m, cudaStream_t st) {
     ENSURE(ic_work1, ns * sizeof(uint32_t));
     ENSURE(ic_acc, 8 * sizeof(unsigned long long));
     ENSURE(ic_ibox, 2 * ns * sizeof(float4));
-    ENSURE(ic_ibkey, 6 * ns * sizeof(uint32_t));
 #undef ENSURE
     m->launches += (uint64_t)icut_prepare(view_of(m), nodes, icut_of(m), st);
     s = check_cuda(m, "pm_icut: slot records");

@@ -356,75 +356,75 @@ __global__ void k_icut_finalize(uint32_t nslots, const uint32_t* __restrict__ wo
     if (s < nslots && work[s]) fin[s] = 1u;
 }
 
-// Order-preserving map of floats to unsigned keys (min/max by atomics).
-__device__ __forceinline__ uint32_t fkey(float f) {
-    const uint32_t b = __float_as_uint(f);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-__device__ __forceinline__ float fkey_inv(uint32_t k) {
-    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
-}
-
-__global__ void k_icut_ibox_init(uint32_t nslots, uint32_t* __restrict__ ibkey) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 6u * nslots) return;
-    ibkey[i] = (i % 6u) < 3u ? 0xffffffffu : 0u;   // lo keys start at +max, hi keys at 0
-}
-
-// Thread per slot where interpolation stops (a cut slot or a leaf with no
-// cut slot above it) and that can carry weight (a normal and a side): its
-// cube [c - h, c + h], h = side widened by 0.1 % plus a few units in the last
-// place of the coordinates, joins the influence box of the slot and of
-// every slot above it.
-__global__ void k_icut_ibox_scatter(const Node* __restrict__ nodes, uint32_t nslots, const uint32_t* __restrict__ pslot,
-                                    const uint32_t* __restrict__ fin, const float4* __restrict__ center,
-                                    const float4* __restrict__ normal, uint32_t* __restrict__ ibkey,
-                                    uint32_t* __restrict__ term) {
+// Thread per slot: whether interpolation stops here (a cut slot or a leaf
+// with no cut slot above it), and the slot's own influence box: for a
+// stopping slot that can carry weight (a normal and a side) the cube
+// [c - h, c + h], h = side widened by 0.1 % plus a few units in the last place
+// of the coordinates; otherwise empty.  lo.w = 1 marks a stopping slot.
+__global__ void k_icut_ibox_own(const Node* __restrict__ nodes, uint32_t nslots, const uint32_t* __restrict__ pslot,
+                                const uint32_t* __restrict__ fin, const float4* __restrict__ center,
+                                const float4* __restrict__ normal, float4* __restrict__ ibox) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslots) return;
     const uint32_t ref = slot_ref(nodes, s);
     bool stop = ref != kInvalid && (fin[s] != 0u || slot_cnt(nodes, s) > 0);
-    if (stop) {   // reachable only without a cut slot above it
-        uint32_t p = s > 1u ? pslot[s >> 1] : 0u;
-        for (int g = 0; g < kIcutMaxDepth && s > 1u; ++g) {
+    if (stop && s > 1u) {   // reachable only without a cut slot above it
+        uint32_t p = pslot[s >> 1];
+        for (int g = 0; g < kIcutMaxDepth; ++g) {
             if (fin[p]) { stop = false; break; }
             if (p == 0u) break;
             p = pslot[p >> 1];
         }
     }
-    term[s] = stop ? 1u : 0u;
-    if (!stop) return;
-    const float4 c = center[s];
-    const float4 n = normal[s];
-    if (!(c.w > 0.0f) || dot3_rn(n.x, n.y, n.z, n.x, n.y, n.z) == 0.0f) return;
-    const float mag = __fadd_rn(__fadd_rn(__fadd_rn(fabsf(c.x), fabsf(c.y)), fabsf(c.z)), c.w);
-    const float h = __fadd_rn(__fmul_rn(c.w, 1.001f), __fmul_rn(mag, 3.814697265625e-06f));   // + mag * 2^-18
-    const uint32_t lo[3] = {fkey(__fsub_rn(c.x, h)), fkey(__fsub_rn(c.y, h)), fkey(__fsub_rn(c.z, h))};
-    const uint32_t hi[3] = {fkey(__fadd_rn(c.x, h)), fkey(__fadd_rn(c.y, h)), fkey(__fadd_rn(c.z, h))};
-    uint32_t t = s;
-    for (int g = 0; g < kIcutMaxDepth; ++g) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            atomicMin(ibkey + 6u * t + a, lo[a]);
-            atomicMax(ibkey + 6u * t + 3u + a, hi[a]);
+    float4 lo = make_float4(INFINITY, INFINITY, INFINITY, stop ? 1.0f : 0.0f);
+    float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    if (stop) {
+        const float4 c = center[s];
+        const float4 n = normal[s];
+        if (c.w > 0.0f && dot3_rn(n.x, n.y, n.z, n.x, n.y, n.z) != 0.0f) {
+            const float mag = __fadd_rn(__fadd_rn(__fadd_rn(fabsf(c.x), fabsf(c.y)), fabsf(c.z)), c.w);
+            const float h = __fadd_rn(__fmul_rn(c.w, 1.001f), __fmul_rn(mag, 3.814697265625e-06f));   // + mag * 2^-18
+            lo = make_float4(__fsub_rn(c.x, h), __fsub_rn(c.y, h), __fsub_rn(c.z, h), 1.0f);
+            hi = make_float4(__fadd_rn(c.x, h), __fadd_rn(c.y, h), __fadd_rn(c.z, h), 0.0f);
         }
-        if (t == 0u) break;
-        t = pslot[t >> 1];
     }
+    ibox[2u * s] = lo;
+    ibox[2u * s + 1u] = hi;
 }
 
-__global__ void k_icut_ibox_decode(uint32_t nslots, const uint32_t* __restrict__ ibkey,
-                                   const uint32_t* __restrict__ term, float4* __restrict__ ibox) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nslots) return;
-    const uint32_t* k = ibkey + 6u * s;
-    if (k[0] == 0xffffffffu) {   // nothing below carries weight: an empty box
-        ibox[2u * s] = make_float4(INFINITY, INFINITY, INFINITY, term[s] ? 1.0f : 0.0f);
-        ibox[2u * s + 1u] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
-        return;
+// Arrival counters of the climb: a node starts with its leaf children counted.
+__global__ void k_icut_ibox_arrive(const Node* __restrict__ nodes, uint32_t m, uint32_t* __restrict__ arrive) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0 || j > m) return;
+    arrive[j] = (nodes[j].c[0].cnt > 0 ? 1u : 0u) + (nodes[j].c[1].cnt > 0 ? 1u : 0u);
+}
+
+// Bottom-up climb (as the tree refit): from every node whose children are
+// both leaves, the union of the children's influence boxes goes into the
+// slot referencing the node unless interpolation stops at that slot (which
+// keeps its own cube); the second arrival at a node continues upwards.
+__global__ void k_icut_ibox_climb(const Node* __restrict__ nodes, uint32_t m, const uint32_t* __restrict__ pslot,
+                                  uint32_t* arrive, float4* ibox) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    uint32_t j = 1u + t;
+    if (!(nodes[j].c[0].cnt > 0 && nodes[j].c[1].cnt > 0)) return;
+    for (int g = 0; g < kIcutMaxDepth; ++g) {
+        const float4 a0 = __ldcg(ibox + 4u * j), a1 = __ldcg(ibox + 4u * j + 1u);
+        const float4 b0 = __ldcg(ibox + 4u * j + 2u), b1 = __ldcg(ibox + 4u * j + 3u);
+        const uint32_t s = pslot[j];
+        const float4 own = __ldcg(ibox + 2u * s);
+        if (own.w == 0.0f) {
+            __stcg(ibox + 2u * s, make_float4(fminf(a0.x, b0.x), fminf(a0.y, b0.y), fminf(a0.z, b0.z), 0.0f));
+            __stcg(ibox + 2u * s + 1u, make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.0f));
+        }
+        if (s == 0u) break;
+        const uint32_t p = s >> 1;
+        __threadfence();
+        if (atomicAdd(&arrive[p], 1u) != 1u) break;   // the sibling subtree is still climbing
+        __threadfence();
+        j = p;
     }
-    ibox[2u * s] = make_float4(fkey_inv(k[0]), fkey_inv(k[1]), fkey_inv(k[2]), term[s] ? 1.0f : 0.0f);
-    ibox[2u * s + 1u] = make_float4(fkey_inv(k[3]), fkey_inv(k[4]), fkey_inv(k[5]), 0.0f);
 }
 
 // Thread per query (Morton order when `order` is given): depth-first over the
@@ -556,11 +556,12 @@ int icut_final(const MapView& m, uint32_t nslots, const IcutParams& p, const Icu
         ++nl;
     }
     k_icut_finalize<<<blocks(nslots, 256), 256, 0, st>>>(nslots, b.work[cur], b.fin);
-    // influence boxes of the final cut (b.work[cur ^ 1] holds the stop flags)
-    k_icut_ibox_init<<<blocks(6u * nslots, 256), 256, 0, st>>>(nslots, b.ibkey);
-    k_icut_ibox_scatter<<<blocks(nslots, 256), 256, 0, st>>>(m.nodes, nslots, b.pslot, b.fin, b.center, b.normal,
-                                                            b.ibkey, b.work[cur ^ 1]);
-    k_icut_ibox_decode<<<blocks(nslots, 256), 256, 0, st>>>(nslots, b.ibkey, b.work[cur ^ 1], b.ibox);
+    // influence boxes of the final cut (b.work[cur ^ 1] is free: arrival counters)
+    const uint32_t nodes_m = nslots / 2u - 1u;
+    k_icut_ibox_own<<<blocks(nslots, 256), 256, 0, st>>>(m.nodes, nslots, b.pslot, b.fin, b.center, b.normal, b.ibox);
+    if (nodes_m == 0) return nl + 2;
+    k_icut_ibox_arrive<<<blocks(nodes_m + 1u, 256), 256, 0, st>>>(m.nodes, nodes_m, b.work[cur ^ 1]);
+    k_icut_ibox_climb<<<blocks(nodes_m, 256), 256, 0, st>>>(m.nodes, nodes_m, b.pslot, b.work[cur ^ 1], b.ibox);
     return nl + 4;
 }
 

@@ -170,7 +170,6 @@ struct IcutBuffers {
     uint32_t* work[2];           // work flags (refinement), mark scratch (coarse cut)
     unsigned long long* acc;     // level statistics: max bits [0..2], fixed sums [3..5], count [6]
     float4* ibox;                // per slot, 2 entries: influence box lo (w = 1: interpolation stops here), hi
-    uint32_t* ibkey;             // per slot, 6 order-preserving keys of the influence box (scratch)
 };
 int icut_prepare(const MapView& m, uint32_t num_nodes, const IcutBuffers& b, cudaStream_t st);
 int icut_normals(const MapView& m, uint32_t nslots, const float4* caller, const IcutBuffers& b, cudaStream_t st);
