@@ -117,27 +117,69 @@ def run_reference(args, cfg) -> dict:
 # ------------------------------------------------------------------ GPU --
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """Clock and throttle samples while the timed region runs: NVML every
+    5 ms from a thread, plus the nvidia-smi line of the profiling recipe every
+    200 ms.  The GPU is found by the CUDA device's PCI bus id."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
     def __init__(self, device_index: int):
         self.idx = device_index
         self.proc = None
         self.file = None
+        self.nvml = None
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+
+    def _bus_id(self) -> str | None:
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.idx)
+            return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:
+            return None
 
     def __enter__(self):
+        import threading
+        bus = self._bus_id()
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByPciBusId(bus) if bus else nv.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h)
+            self._stop = threading.Event()
+
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.005)
+
+            self._thread = threading.Thread(target=loop, daemon=True)
+            self._thread.start()
+        except Exception:
+            self.nvml = None
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", bus if bus else str(self.idx),
+                                          f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -146,23 +188,24 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
-        if self.proc is None or self.file is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.file.flush()
         rows = []
-        for line in Path(self.file.name).read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.file.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        if self.proc is not None and self.file is not None:
+            self.file.flush()
+            for line in Path(self.file.name).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.file.name)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = {names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"}
+        reasons |= {n for mhz, bits in self.samples for b, n in self.REASONS.items() if bits & b}
+        sm = [m for m, _ in self.samples] or [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = self.max_mhz or max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(np.min(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(self.samples), "smi_samples": len(rows),
+                "source": "NVML every 5 ms + nvidia-smi every 200 ms"}
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -268,17 +311,15 @@ def run_ours(args, cfg) -> dict | None:
     ms_per_step = total_ms / args.steps
     value = world * Q / (ms_per_step / 1000.0)
 
-    # end to end through the public API: pinned host in, host radiance out
+    # end to end through the public API: pinned host in, host radiance out.
+    # pm_build_query_host copies the photons in and builds while the queries
+    # copy in (one piece: measured fastest, see --chunks).
     e2e_ms = []
+    hkw = {kk: v for kk, v in qkw.items()}
     for i in range(args.warmup + args.steps):
         flush.zero_()
         e0.record()
-        d_pos.copy_(h_pos, non_blocking=True)
-        d_pow.copy_(h_pow, non_blocking=True)
-        d_qpos.copy_(h_qpos, non_blocking=True)
-        d_qnrm.copy_(h_qnrm, non_blocking=True)
-        step()
-        h_rad.copy_(d_rad, non_blocking=True)
+        pm.build_query_host(h_pos, h_pow, h_qpos, h_qnrm, out=h_rad, chunks=args.chunks, **hkw)
         e1.record()
         e1.synchronize()
         if i >= args.warmup:
@@ -289,6 +330,8 @@ def run_ours(args, cfg) -> dict | None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_total = float(tt.item())
     e2e_value = world * Q / (e2e_total / args.steps / 1000.0)
+    if not torch.equal(h_rad.view(torch.int32), d_rad.cpu().view(torch.int32)):
+        raise RuntimeError("host-buffer path and device path disagree")
 
     kern_ms = float(np.mean(kernels))
     nodes = info.num_nodes
@@ -314,7 +357,8 @@ def run_ours(args, cfg) -> dict | None:
                            "unit": "GB/s", "frac": build_bytes / (build_ms / 1000.0) / 1e9 / peak,
                            "algorithmic_bytes": build_bytes},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * N + 32 * Q,
-                "d2h_bytes_per_step": 16 * Q},
+                "d2h_bytes_per_step": 16 * Q, "call": "pm_build_query_host (pinned host buffers)",
+                "chunks": args.chunks, "ms_per_step": e2e_total / args.steps},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "tree_nodes": nodes,
@@ -627,6 +671,7 @@ def main(argv=None) -> int:
     ap.add_argument("--rounds", type=int, default=0)
     ap.add_argument("--qpw", type=int, default=0, help="queries per warp (group layout)")
     ap.add_argument("--layout", type=int, default=-1, help="k-buffer layout: 0 heap, 1 group, 2 wide tree")
+    ap.add_argument("--chunks", type=int, default=1, help="query chunks of the end-to-end host-buffer call")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

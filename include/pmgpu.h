@@ -185,6 +185,22 @@ PM_API pm_status pm_merged_count(const pm_map* map, uint32_t* count);
 PM_API pm_status pm_query(pm_map* map, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
                    uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, void* stream);
 
+/* Build + query from host memory in one call (PhotonMap::BuildMap followed
+ * by GatherFor's estimate, for a caller whose photons and shading points live
+ * in host memory).  Copies the photons in and builds while the queries copy
+ * in on an internal stream; with chunks > 1 (at most 16; 0 = 1) the queries
+ * are copied, answered and copied back in that many pieces so that copies
+ * overlap queries -- at the cost of query coherence: each piece is Morton
+ * sorted on its own, which measured slower for 2M queries than one piece.
+ * Results are identical, bit for bit, to pm_build + pm_query on the same data
+ * (exact mode).  Host arrays should be pinned (cudaHostAlloc /
+ * cudaHostRegister) for the copies to overlap.  Asynchronous on `stream`:
+ * h_rad4 is complete when the stream's work up to this call is.  Not
+ * allowed during stream capture. */
+PM_API pm_status pm_build_query_host(pm_map* map, const float* h_pos4, const float* h_pow4, uint32_t n, int format,
+                                     const pm_query_desc* desc, const float* h_qpos4, const float* h_qnrm4,
+                                     uint32_t nq, float* h_rad4, uint32_t chunks, void* stream);
+
 /* Brute-force exact kNN over every photon (test and validation path). */
 PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
                               const float* d_qnrm4, uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2,

@@ -68,6 +68,7 @@ SIGNATURES = {
     "pm_autotune": (_I, [_VP, _FP, _FP, _U32, _I, C.POINTER(QueryDesc), _FP, _FP, _U32, _U32, C.POINTER(Tuning), _VP]),
     "pm_build": (_I, [_VP, _FP, _FP, _U32, _I, _VP]),
     "pm_query": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
+    "pm_build_query_host": (_I, [_VP, _FP, _FP, _U32, _I, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _U32, _VP]),
     "pm_query_bruteforce": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_noalloc": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _VP]),
     "pm_query_backward": (_I, [_VP, C.POINTER(QueryDesc), _FP, _FP, _U32, _FP, _UP, _FP, _UP, _FP, _FP, _VP]),

@@ -65,6 +65,10 @@ struct pm_map {
     DevBuf ic_pslot, ic_level, ic_range, ic_center, ic_normal, ic_est, ic_exact, ic_coarse, ic_fin, ic_work0, ic_work1,
         ic_acc, ic_ibox;
     uint32_t icut_slots = 0;
+    // pm_build_query_host: device copies of host inputs, two copy streams, events
+    DevBuf hs_pos, hs_pow, hs_qpos, hs_qnrm, hs_rad;
+    cudaStream_t hs_in = nullptr, hs_out = nullptr;
+    cudaEvent_t hs_ev[36] = {};   // photons in, done, and two per chunk
     uint64_t icut_prep_gen = ~0ull, icut_gen = ~0ull;
     uint64_t build_gen = 0, compat_gen = ~0ull;
     uint32_t compat_k = 0, compat_iters = 0;
@@ -320,8 +324,12 @@ pm_status pm_destroy(pm_map* m) {
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
                      &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
                      &m->ic_normal, &m->ic_est, &m->ic_exact, &m->ic_coarse, &m->ic_fin, &m->ic_work0, &m->ic_work1,
-                     &m->ic_acc, &m->ic_ibox};
+                     &m->ic_acc, &m->ic_ibox, &m->hs_pos, &m->hs_pow, &m->hs_qpos, &m->hs_qnrm, &m->hs_rad};
     for (DevBuf* b : all) buf_free(m, *b);
+    for (cudaEvent_t& e : m->hs_ev)
+        if (e) cudaEventDestroy(e);
+    if (m->hs_in) cudaStreamDestroy(m->hs_in);
+    if (m->hs_out) cudaStreamDestroy(m->hs_out);
     for (cudaEvent_t& e : m->ev)
         if (e) cudaEventDestroy(e);
     delete m;
@@ -466,6 +474,86 @@ pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, c
     m->query_launches = (uint32_t)nl;
     m->launches += (uint64_t)nl;
     return check_cuda(m, "pm_query");
+}
+
+pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow4, uint32_t n, int format,
+                              const pm_query_desc* desc, const float* h_qpos4, const float* h_qnrm4, uint32_t nq,
+                              float* h_rad4, uint32_t chunks, void* stream) {
+    if (!m) return PM_ERR_INVALID;
+    pm_status s = validate_desc(m, desc, true);
+    if (s != PM_OK) return s;
+    if (format != PM_PHOTONS_REFERENCE && format != PM_PHOTONS_PACKED)
+        return fail(m, PM_ERR_INVALID, "unknown photon format %d", format);
+    if (chunks == 0) chunks = 1;
+    if (chunks > 16) return fail(m, PM_ERR_INVALID, "chunks must be at most 16");
+    if (n > 0 && (!h_pos4 || !h_pow4)) return fail(m, PM_ERR_INVALID, "photon arrays must be non-NULL when n > 0");
+    if (nq > 0 && (!h_qpos4 || !h_qnrm4 || !h_rad4))
+        return fail(m, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
+    if (m->max_photons && n > m->max_photons)
+        return fail(m, PM_ERR_INVALID, "n = %u exceeds the map's max_photons = %u", n, m->max_photons);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (capturing(st)) return fail(m, PM_ERR_STATE, "pm_build_query_host cannot run during stream capture");
+    if (!m->hs_in) {
+        if (cudaStreamCreateWithFlags(&m->hs_in, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&m->hs_out, cudaStreamNonBlocking) != cudaSuccess)
+            return check_cuda(m, "pm_build_query_host: streams");
+        for (cudaEvent_t& e : m->hs_ev)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+                return check_cuda(m, "pm_build_query_host: events");
+    }
+    const size_t pb = (size_t)(n ? n : 1) * sizeof(float4), qb = (size_t)(nq ? nq : 1) * sizeof(float4);
+    if ((s = buf_ensure(m, m->hs_pos, pb, "hs_pos")) != PM_OK || (s = buf_ensure(m, m->hs_pow, pb, "hs_pow")) != PM_OK ||
+        (s = buf_ensure(m, m->hs_qpos, qb, "hs_qpos")) != PM_OK ||
+        (s = buf_ensure(m, m->hs_qnrm, qb, "hs_qnrm")) != PM_OK || (s = buf_ensure(m, m->hs_rad, qb, "hs_rad")) != PM_OK)
+        return s;
+    float4* dpos = P<float4>(m->hs_pos);
+    float4* dpow = P<float4>(m->hs_pow);
+    float4* dqp = P<float4>(m->hs_qpos);
+    float4* dqn = P<float4>(m->hs_qnrm);
+    float4* drad = P<float4>(m->hs_rad);
+    cudaEvent_t ev_photons = m->hs_ev[0], ev_done = m->hs_ev[1];
+    // photons in, then the queries in pieces behind them on the copy stream
+    if (n) {
+        cudaMemcpyAsync(dpos, h_pos4, (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(dpow, h_pow4, (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, st);
+    }
+    cudaEventRecord(ev_photons, st);
+    cudaStreamWaitEvent(m->hs_in, ev_photons, 0);
+    if (nq < chunks) chunks = nq ? nq : 1;
+    uint32_t bounds[17];
+    for (uint32_t c = 0; c <= chunks; ++c) bounds[c] = (uint32_t)(((uint64_t)nq * c) / chunks);
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const size_t off = bounds[c], len = bounds[c + 1] - bounds[c];
+        if (len) {
+            cudaMemcpyAsync(dqp + off, reinterpret_cast<const float4*>(h_qpos4) + off, len * sizeof(float4),
+                            cudaMemcpyHostToDevice, m->hs_in);
+            cudaMemcpyAsync(dqn + off, reinterpret_cast<const float4*>(h_qnrm4) + off, len * sizeof(float4),
+                            cudaMemcpyHostToDevice, m->hs_in);
+        }
+        cudaEventRecord(m->hs_ev[2 + 2 * c], m->hs_in);
+    }
+    s = check_cuda(m, "pm_build_query_host: copies in");
+    if (s != PM_OK) return s;
+    s = pm_build(m, reinterpret_cast<const float*>(dpos), reinterpret_cast<const float*>(dpow), n, format, stream);
+    if (s != PM_OK) return s;
+    // each piece is answered once it has arrived; its radiance leaves on the second stream
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const size_t off = bounds[c], len = bounds[c + 1] - bounds[c];
+        cudaStreamWaitEvent(st, m->hs_ev[2 + 2 * c], 0);
+        if (len) {
+            s = pm_query(m, desc, reinterpret_cast<const float*>(dqp + off), reinterpret_cast<const float*>(dqn + off),
+                         (uint32_t)len, reinterpret_cast<float*>(drad + off), nullptr, nullptr, nullptr, stream);
+            if (s != PM_OK) return s;
+        }
+        cudaEventRecord(m->hs_ev[3 + 2 * c], st);
+        cudaStreamWaitEvent(m->hs_out, m->hs_ev[3 + 2 * c], 0);
+        if (len)
+            cudaMemcpyAsync(reinterpret_cast<float4*>(h_rad4) + off, drad + off, len * sizeof(float4),
+                            cudaMemcpyDeviceToHost, m->hs_out);
+    }
+    cudaEventRecord(ev_done, m->hs_out);
+    cudaStreamWaitEvent(st, ev_done, 0);
+    return check_cuda(m, "pm_build_query_host");
 }
 
 pm_status pm_query_bruteforce(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,

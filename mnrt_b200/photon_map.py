@@ -141,6 +141,27 @@ class PhotonMap:
                                    _stream(stream)), self._h)
         self.num_photons = n
 
+    def build_query_host(self, positions: torch.Tensor, powers: torch.Tensor, qpos: torch.Tensor, qnrm: torch.Tensor,
+                         out: torch.Tensor | None = None, chunks: int = 1, packed: bool = True, stream=None,
+                         **kw) -> torch.Tensor:
+        """Build + query from host tensors (pinned for overlapped copies):
+        photons in and build while the queries copy in, query, radiance out;
+        chunks > 1 pipelines query pieces (pm_build_query_host).  Returns the
+        host radiance (nq, 4); complete once the stream reaches this call."""
+        for a in (positions, powers, qpos, qnrm):
+            if a.is_cuda or a.dtype != torch.float32 or not a.is_contiguous() or a.dim() != 2 or a.shape[1] != 4:
+                raise ValueError("host arrays must be contiguous float32 (n, 4) CPU tensors")
+        n, nq = int(positions.shape[0]), int(qpos.shape[0])
+        if out is None:
+            out = torch.empty((nq, 4), dtype=torch.float32, pin_memory=True)
+        d = self.desc(**kw)
+        fmt = L.PM_PHOTONS_PACKED if packed else L.PM_PHOTONS_REFERENCE
+        hp = lambda t: t.data_ptr() if t.numel() else None
+        L.check(self._lib.pm_build_query_host(self._h, hp(positions), hp(powers), n, fmt, C.byref(d), hp(qpos),
+                                              hp(qnrm), nq, hp(out), int(chunks), _stream(stream)), self._h)
+        self.num_photons = n
+        return out
+
     def desc(self, k=None, r_max=None, filter="box", cone_k=1.0, min_found=0, sorted_queries=True,
              mode=L.PM_MODE_EXACT, refine_iters=2) -> L.QueryDesc:
         return L.QueryDesc(k=int(k if k is not None else self.k), r_max=float(r_max if r_max is not None else self.r_max),

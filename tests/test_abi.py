@@ -157,3 +157,20 @@ def test_icut_validation_without_gpu(engine_lib):
     assert lib.pm_icut_node_centers(h, None, None) == L.PM_ERR_INVALID
     assert lib.pm_icut_export(h, 0, None, None, None, None, None, None, None) == L.PM_ERR_STATE
     lib.pm_destroy(h)
+
+
+def test_build_query_host_validation_without_gpu(engine_lib):
+    lib = engine_lib
+    h = _create(lib)
+    d = L.QueryDesc(k=10, r_max=0.1, filter=L.PM_FILTER_BOX, cone_k=1.0, mode=0, min_found=0, order=0, refine_iters=2)
+    f = lib.pm_build_query_host
+    assert f(h, None, None, 0, L.PM_PHOTONS_PACKED, None, None, None, 0, None, 4, None) == L.PM_ERR_INVALID
+    assert f(h, None, None, 0, 9, C.byref(d), None, None, 0, None, 4, None) == L.PM_ERR_INVALID
+    assert f(h, None, None, 0, L.PM_PHOTONS_PACKED, C.byref(d), None, None, 0, None, 17, None) == L.PM_ERR_INVALID
+    assert f(h, None, None, 10, L.PM_PHOTONS_PACKED, C.byref(d), None, None, 0, None, 4, None) == L.PM_ERR_INVALID
+    assert f(h, 16, 16, 10, L.PM_PHOTONS_PACKED, C.byref(d), None, None, 5, None, 4, None) == L.PM_ERR_INVALID
+    assert f(h, 16, 16, 5000, L.PM_PHOTONS_PACKED, C.byref(d), None, None, 0, None, 4, None) == L.PM_ERR_INVALID
+    compat = L.QueryDesc(k=10, r_max=0.1, filter=0, cone_k=1.0, mode=L.PM_MODE_ZHOU_COMPAT, min_found=0, order=0,
+                         refine_iters=2)
+    assert f(h, None, None, 0, L.PM_PHOTONS_PACKED, C.byref(compat), None, None, 0, None, 4, None) == L.PM_ERR_INVALID
+    lib.pm_destroy(h)
