@@ -208,6 +208,18 @@ class ClockSampler:
                 "source": "NVML every 5 ms + nvidia-smi every 200 ms"}
 
 
+def rank_max(values: list[float], dev=None) -> list[float]:
+    """Max over ranks of each value (device times of the timed region); the
+    values themselves without a process group of more than one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def measured_peaks() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -303,11 +315,7 @@ def run_ours(args, cfg) -> dict | None:
     clocks = clk.summary()
     launches = pm.info().launches - launches0
     info = pm.info()
-    total_ms = float(np.sum(steps_ms))
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = rank_max([float(np.sum(steps_ms))], dev)[0]
     ms_per_step = total_ms / args.steps
     value = world * Q / (ms_per_step / 1000.0)
 
@@ -324,11 +332,7 @@ def run_ours(args, cfg) -> dict | None:
         e1.synchronize()
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e_total = float(np.sum(e2e_ms))
-    if world > 1:
-        tt = torch.tensor([e2e_total], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
+    e2e_total = rank_max([float(np.sum(e2e_ms))], dev)[0]
     e2e_value = world * Q / (e2e_total / args.steps / 1000.0)
     if not torch.equal(h_rad.view(torch.int32), d_rad.cpu().view(torch.int32)):
         raise RuntimeError("host-buffer path and device path disagree")
