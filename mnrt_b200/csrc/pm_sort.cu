@@ -2,13 +2,13 @@
 // (uint64 key, uint32 value) pairs.  They replace the CUDPP scan / compact /
 // radix sort the reference builds its tree with (MNCudaPrimitives.cpp:160-227).
 //
-// Radix sort: 8-bit digits, reduce-then-scan per pass.
-//   1. k_digit_hist: every tile of kTile keys counts its digits
-//      (digit-major layout hist[d * tiles + t], so one exclusive scan over
-//      the whole array yields every tile's global offset per digit);
+// Radix sort: 8-bit digits, reduce-then-scan per pass (no inter-block waits).
+//   1. k_digit_hist: every tile counts its digits (warp-aggregated), in the
+//      digit-major layout hist[d * tiles + t], so one exclusive scan over the
+//      whole array yields every tile's global offset per digit;
 //   2. exclusive scan of hist;
-//   3. k_digit_scatter: every tile ranks its keys stably (warp match_any +
-//      per-warp digit counts) and scatters them to offset + rank.
+//   3. k_digit_scatter: every tile ranks its keys stably, orders them by
+//      digit in shared memory and writes each digit's run contiguously.
 // Stability across passes makes the result sorted by the full key, with the
 // input order breaking ties.
 #include "pm_internal.h"
@@ -18,11 +18,6 @@ namespace pm {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;      // elements per thread per scan tile
 constexpr int kScanTile = kScanThreads * kScanItems;
-
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;   // 4096 keys per tile
-constexpr int kSortWarps = kSortThreads / 32;
 
 // ------------------------------------------------------------------ scan --
 
@@ -121,6 +116,20 @@ int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scra
 }
 
 // ------------------------------------------------------------ radix sort --
+//
+// One pass = k_digit_hist (per tile digit counts, digit-major so that one
+// exclusive scan gives every tile its global offset per digit), the scan,
+// and k_digit_scatter.  A tile is kSortTile keys; warp w of its block owns
+// keys [w * 256, (w + 1) * 256) of the tile, taken in rounds of 32, so the
+// order (warp, round, lane) is the input order.  The scatter ranks each key
+// among the tile's keys of its digit (warp match_any plus per-warp digit
+// counters), places the tile's keys sorted by digit in shared memory, and
+// writes every digit's run out contiguously.
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortRounds = 8;                                 // rounds of 32 keys per warp
+constexpr int kSortTile = kSortThreads * kSortRounds;          // 2048 keys per tile
 
 template <class Key>
 __global__ void __launch_bounds__(kSortThreads) k_digit_hist(const Key* __restrict__ keys, uint32_t n,
@@ -128,11 +137,15 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_hist(const Key* __restri
     __shared__ uint32_t s_hist[256];
     s_hist[threadIdx.x] = 0;
     __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
-#pragma unroll 4
-    for (int i = 0; i < kSortItems; ++i) {
-        const uint64_t g = base + (uint64_t)i * kSortThreads + threadIdx.x;
-        if (g < n) atomicAdd(&s_hist[(uint32_t)(keys[g] >> shift) & 0xffu], 1u);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * kSortTile + (uint64_t)warp * (32 * kSortRounds);
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t g = base + (uint64_t)r * 32 + lane;
+        const bool valid = g < n;
+        const uint32_t digit = valid ? ((uint32_t)(keys[g] >> shift) & 0xffu) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, digit);
+        if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[digit], (uint32_t)__popc(peers));
     }
     __syncthreads();
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s_hist[threadIdx.x];
@@ -145,42 +158,75 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
                                                                   const uint32_t* __restrict__ offsets,
                                                                   Key* __restrict__ keys_out,
                                                                   uint32_t* __restrict__ vals_out) {
-    __shared__ uint32_t s_base[256];              // global offset + keys of this digit seen so far
-    __shared__ uint32_t s_warp[kSortWarps][256];  // per-warp count, then per-warp start
+    __shared__ uint32_t s_cnt[kSortWarps][256];   // per-warp digit counts, then per-warp starts within the digit
+    __shared__ uint32_t s_start[256];             // tile-local start of each digit
+    __shared__ uint32_t s_global[256];            // global position of the tile's first key of each digit
+    __shared__ uint32_t s_warpsum[32];
+    __shared__ Key s_key[kSortTile];
+    __shared__ uint32_t s_val[kSortTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    s_base[threadIdx.x] = offsets[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
-    const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    for (int i = 0; i < kSortItems; ++i) {
-        const uint64_t g = base + (uint64_t)i * kSortThreads + threadIdx.x;
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) s_cnt[w][threadIdx.x] = 0;
+    s_global[threadIdx.x] = offsets[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+    __syncthreads();
+    const uint64_t tile0 = (uint64_t)blockIdx.x * kSortTile;
+    const uint64_t base = tile0 + (uint64_t)warp * (32 * kSortRounds);
+    Key key[kSortRounds];
+    uint32_t val[kSortRounds], rank[kSortRounds];
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t g = base + (uint64_t)r * 32 + lane;
         const bool valid = g < n;
-        Key key = valid ? keys_in[g] : Key(0);
-        uint32_t val = valid ? vals_in[g] : 0u;
-        const uint32_t digit = valid ? ((uint32_t)(key >> shift) & 0xffu) : 256u;
-#pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) s_warp[w][threadIdx.x] = 0;
-        __syncthreads();
+        key[r] = valid ? keys_in[g] : Key(0);
+        val[r] = valid ? vals_in[g] : 0u;
+        const uint32_t digit = valid ? ((uint32_t)(key[r] >> shift) & 0xffu) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, digit);
-        const uint32_t rank_in_warp = __popc(peers & lt_mask);
-        if (valid && rank_in_warp == 0) s_warp[warp][digit] = __popc(peers);
-        __syncthreads();
-        {   // thread d: turn per-warp counts for digit d into start offsets
-            uint32_t run = s_base[threadIdx.x];
+        rank[r] = valid ? s_cnt[warp][digit] + __popc(peers & lt) : 0u;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) s_cnt[warp][digit] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {   // thread d: per-warp starts within digit d, then the tile-local digit starts
+        uint32_t run = 0;
 #pragma unroll
-            for (int w = 0; w < kSortWarps; ++w) {
-                const uint32_t c = s_warp[w][threadIdx.x];
-                s_warp[w][threadIdx.x] = run;
-                run += c;
-            }
-            s_base[threadIdx.x] = run;
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = s_cnt[w][threadIdx.x];
+            s_cnt[w][threadIdx.x] = run;
+            run += c;
         }
-        __syncthreads();
-        if (valid) {
-            const uint32_t dst = s_warp[warp][digit] + rank_in_warp;
-            keys_out[dst] = key;
-            vals_out[dst] = val;
+        uint32_t x = run;   // block exclusive scan of the digit totals
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
+        if (lane == 31) s_warpsum[warp] = x;
         __syncthreads();
+        uint32_t wp = 0;
+        for (int w = 0; w < warp; ++w) wp += s_warpsum[w];
+        s_start[threadIdx.x] = wp + x - run;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t g = base + (uint64_t)r * 32 + lane;
+        if (g < n) {
+            const uint32_t digit = (uint32_t)(key[r] >> shift) & 0xffu;
+            const uint32_t local = s_start[digit] + s_cnt[warp][digit] + rank[r];
+            s_key[local] = key[r];
+            s_val[local] = val[r];
+        }
+    }
+    __syncthreads();
+    const uint32_t tile_n = (uint32_t)min((uint64_t)kSortTile, (uint64_t)n - tile0);
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kSortThreads) {
+        const Key kk = s_key[i];
+        const uint32_t digit = (uint32_t)(kk >> shift) & 0xffu;
+        const uint32_t dst = s_global[digit] + (i - s_start[digit]);
+        keys_out[dst] = kk;
+        vals_out[dst] = s_val[i];
     }
 }
 
