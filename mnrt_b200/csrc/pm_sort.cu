@@ -3,7 +3,7 @@
 // radix sort the reference builds its tree with (MNCudaPrimitives.cpp:160-227).
 //
 // Radix sort: 8-bit digits, reduce-then-scan per pass (no inter-block waits).
-//   1. k_digit_hist: every tile counts its digits (warp-aggregated), in the
+//   1. k_digit_hist: every tile counts its digits (one histogram per warp), in the
 //      digit-major layout hist[d * tiles + t], so one exclusive scan over the
 //      whole array yields every tile's global offset per digit;
 //   2. exclusive scan of hist;
@@ -122,8 +122,8 @@ int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scra
 // and k_digit_scatter.  A tile is kSortTile keys; warp w of its block owns
 // keys [w * 256, (w + 1) * 256) of the tile, taken in rounds of 32, so the
 // order (warp, round, lane) is the input order.  The scatter ranks each key
-// among the tile's keys of its digit (warp match_any plus per-warp digit
-// counters), places the tile's keys sorted by digit in shared memory, and
+// among the tile's keys of its digit (the lanes sharing its digit from eight
+// ballots, plus per-warp digit counters), places the tile's keys sorted by digit in shared memory, and
 // writes every digit's run out contiguously.
 
 constexpr int kSortThreads = 256;
@@ -134,21 +134,28 @@ constexpr int kSortTile = kSortThreads * kSortRounds;          // 2048 keys per 
 template <class Key>
 __global__ void __launch_bounds__(kSortThreads) k_digit_hist(const Key* __restrict__ keys, uint32_t n,
                                                                int shift, uint32_t ntiles, uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s_hist[256];
-    s_hist[threadIdx.x] = 0;
-    __syncthreads();
+    __shared__ uint32_t s_hist[kSortWarps][256];   // one histogram per warp: contention only within a warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) s_hist[w][threadIdx.x] = 0;
+    __syncthreads();
     const uint64_t base = (uint64_t)blockIdx.x * kSortTile + (uint64_t)warp * (32 * kSortRounds);
+    Key kk[kSortRounds];
 #pragma unroll
     for (int r = 0; r < kSortRounds; ++r) {
         const uint64_t g = base + (uint64_t)r * 32 + lane;
-        const bool valid = g < n;
-        const uint32_t digit = valid ? ((uint32_t)(keys[g] >> shift) & 0xffu) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, digit);
-        if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[digit], (uint32_t)__popc(peers));
+        kk[r] = g < n ? keys[g] : Key(0);
+    }
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t g = base + (uint64_t)r * 32 + lane;
+        if (g < n) atomicAdd(&s_hist[warp][(uint32_t)(kk[r] >> shift) & 0xffu], 1u);
     }
     __syncthreads();
-    hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s_hist[threadIdx.x];
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) c += s_hist[w][threadIdx.x];
+    hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = c;
 }
 
 template <class Key>
@@ -181,7 +188,13 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
         key[r] = valid ? keys_in[g] : Key(0);
         val[r] = valid ? vals_in[g] : 0u;
         const uint32_t digit = valid ? ((uint32_t)(key[r] >> shift) & 0xffu) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, digit);
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);   // lanes with the same digit: 8 ballots
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t ones = __ballot_sync(0xffffffffu, (digit >> b) & 1u);
+            peers &= ((digit >> b) & 1u) ? ones : ~ones;
+        }
         rank[r] = valid ? s_cnt[warp][digit] + __popc(peers & lt) : 0u;
         __syncwarp();
         if (valid && lane == __ffs(peers) - 1) s_cnt[warp][digit] += __popc(peers);
