@@ -179,3 +179,23 @@ def test_icut_state_rules(cuda):
     pm2.merge(PhotonData(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda), packed=True))
     pm2.build_map()
     assert pm2.icut_interpolate(qp, qn).shape == (100, 4)
+
+
+@pytest.mark.parametrize("n", [0, 1, 20])
+def test_icut_tiny_maps(cuda, n):
+    """Empty map, one photon, one leaf as the whole tree: the cut is built,
+    interpolation answers zeros or the single leaf, nothing faults."""
+    ph = gen.photons(max(n, 1), seed=1400 + n, caustic_frac=0.0)
+    pm = PhotonMap(max(n, 1), global_q_radius_max=0.2, knn_target_count=8)
+    pm.build(to_dev(ph.pos[:n], cuda), to_dev(ph.pow[:n], cuda))
+    pm.icut_build(min_found=0)
+    q = gen.queries(64, seed=1401)
+    got = pm.icut_interpolate(to_dev(q.pos, cuda), to_dev(q.nrm, cuda)).cpu().numpy()
+    cut = pm.icut_export()
+    assert cut["final"].shape == (2 * (pm.info().num_nodes + 1),)
+    if n == 0:
+        assert not got.any() and not cut["final"].any()
+    else:
+        assert cut["final"][0] == 1        # the root is the one leaf
+        assert np.isfinite(got).all()
+    assert pm.info().device_errors == 0

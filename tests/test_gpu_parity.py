@@ -320,3 +320,18 @@ def test_build_query_host_matches_device_calls(cuda, chunks, pinned):
                      min_found=8)["rad"].cpu()
     assert torch.equal(got.view(torch.int32), want.view(torch.int32))
     assert pm.info().device_errors == 0
+
+
+def test_build_query_host_empty_inputs(cuda):
+    from mnrt_b200.photon_map import PhotonMap
+    ph = gen.photons(1000, seed=73)
+    q = gen.queries(10, seed=74)
+    pm = PhotonMap(ph.n, global_q_radius_max=0.1, knn_target_count=8)
+    z4 = torch.zeros((0, 4), dtype=torch.float32)
+    out = pm.build_query_host(torch.from_numpy(ph.pos), torch.from_numpy(ph.pow), z4, z4)
+    torch.cuda.synchronize()
+    assert out.shape == (0, 4)
+    out = pm.build_query_host(z4, z4, torch.from_numpy(q.pos), torch.from_numpy(q.nrm))
+    torch.cuda.synchronize()
+    assert out.shape == (10, 4) and not out.any()
+    assert pm.info().device_errors == 0
