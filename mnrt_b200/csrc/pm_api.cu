@@ -46,7 +46,7 @@ struct pm_map {
     // photon-sized
     DevBuf pos, pow, inv, nodes, hdr;
     DevBuf keys0, keys1, vals0, vals1, scratch, kfirst, klast, ksplit, kkeep, krank, parent, arrive, nleaf, partials;
-    DevBuf wflag, wrank, wcnt, wfirst, wchild, wroot, wscan, rootmark;   // 32-wide tree
+    DevBuf wflag, wcnt, wfirst, wchild, wroot, wscan, rootmark;   // 32-wide tree
     // query-sized
     DevBuf qkeys0, qkeys1, qvals0, qvals1, qscratch, counter, fixq;
     DevBuf stats;           // query counters (profiling level 2)
@@ -173,7 +173,6 @@ pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
     ENSURE(nleaf, (cap + 1) * sizeof(uint32_t));
     ENSURE(partials, (8 * 1184 + 16) * sizeof(uint32_t));
     ENSURE(wflag, cap * sizeof(uint32_t));
-    ENSURE(wrank, cap * sizeof(uint32_t));
     ENSURE(wcnt, cap * sizeof(uint32_t));
     ENSURE(wfirst, cap * sizeof(uint32_t));
     ENSURE(wchild, (cap + 1) * 2 * sizeof(ChildSlot));
@@ -240,7 +239,7 @@ MapView view_of(pm_map* m) {
 
 WideBuffers wide_of(pm_map* m) {
     WideBuffers w;
-    w.wflag = P<uint32_t>(m->wflag); w.wrank = P<uint32_t>(m->wrank); w.wcnt = P<uint32_t>(m->wcnt);
+    w.wflag = P<uint32_t>(m->wflag); w.wcnt = P<uint32_t>(m->wcnt);
     w.wfirst = P<uint32_t>(m->wfirst); w.wchild = P<ChildSlot>(m->wchild); w.wroot = P<ChildSlot>(m->wroot);
     w.scratch = P<uint32_t>(m->wscan);
     return w;
@@ -317,7 +316,7 @@ pm_status pm_destroy(pm_map* m) {
     if (!m) return PM_ERR_INVALID;
     DevBuf* all[] = {&m->pos, &m->pow, &m->inv, &m->nodes, &m->hdr, &m->keys0, &m->keys1, &m->vals0, &m->vals1,
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
-                     &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wrank, &m->wcnt, &m->wfirst,
+                     &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wcnt, &m->wfirst,
                      &m->wchild, &m->wroot, &m->wscan, &m->rootmark, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
                      &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,

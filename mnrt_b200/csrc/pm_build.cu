@@ -32,6 +32,7 @@ namespace pm {
 
 constexpr int kBoundsThreads = 256;
 constexpr int kBoundsBlocksMax = 1184;   // 8 per SM on 148 SMs
+constexpr int kLeafBoxBlocks = 1184;     // 8 blocks of 8 warps per SM, grid-stride over the nodes
 
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
@@ -247,8 +248,8 @@ __global__ void k_emit(const float4* __restrict__ pos, uint32_t n, uint32_t leaf
         const uint32_t cl = side ? last : gamma;
         const uint32_t size = cl - cf + 1;
         ChildSlot s;
-        if (size <= leaf_size) {
-            leaf_box(pos, cf, size, s);
+        if (size <= leaf_size) {   // box filled in by k_leaf_boxes
+            s = empty_slot();
             s.ref = cf;
             s.cnt = size;
             ++leaves;
@@ -265,6 +266,45 @@ __global__ void k_emit(const float4* __restrict__ pos, uint32_t n, uint32_t leaf
     nodes[id] = nd;
     arrive[id] = leaves;
     nleaf[id] = leaves;
+}
+
+// Leaf boxes: warp per compacted node (grid-stride over nodes 1..m), lane i
+// takes photon i of a leaf, min / max by warp reductions on order-preserving
+// keys of the coordinates.
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void k_leaf_boxes(const float4* __restrict__ pos, Node* __restrict__ nodes, const MapHeader* __restrict__ hdr) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t m = hdr->num_nodes;
+    for (uint32_t j = 1u + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); j <= m; j += warps) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const uint32_t cnt = nodes[j].c[side].cnt;
+            if (cnt == 0) continue;
+            const uint32_t ref = nodes[j].c[side].ref;
+            float4 p = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
+            float4 q = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+            if (lane < cnt) { p = pos[ref + lane]; q = p; }
+            const uint32_t lx = __reduce_min_sync(0xffffffffu, ord_key(p.x));
+            const uint32_t ly = __reduce_min_sync(0xffffffffu, ord_key(p.y));
+            const uint32_t lz = __reduce_min_sync(0xffffffffu, ord_key(p.z));
+            const uint32_t hx = __reduce_max_sync(0xffffffffu, ord_key(q.x));
+            const uint32_t hy = __reduce_max_sync(0xffffffffu, ord_key(q.y));
+            const uint32_t hz = __reduce_max_sync(0xffffffffu, ord_key(q.z));
+            if (lane == 0) {
+                float* lo = nodes[j].c[side].lo;
+                lo[0] = ord_float(lx); lo[1] = ord_float(ly); lo[2] = ord_float(lz);
+                lo[3] = ord_float(hx); lo[4] = ord_float(hy); lo[5] = ord_float(hz);
+            }
+        }
+    }
 }
 
 // Thread per compacted node: nodes whose two children are leaves start a
@@ -337,8 +377,9 @@ int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, in
             const int ns = exclusive_scan(bb.kkeep, bb.krank, ni, total + 1, total, st);
             k_emit<<<gi, tb, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank,
                                       total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
+            k_leaf_boxes<<<kLeafBoxBlocks, 256, 0, st>>>(out_pos, nodes, hdr);
             k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
-            return 5 + ns;
+            return 6 + ns;
         }
     }
     k_emit<<<1, 32, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank, nullptr,
@@ -393,53 +434,107 @@ __global__ void k_wide_flags(const uint32_t* __restrict__ parent, const uint32_t
     wflag[t] = f;
 }
 
-// Walks the kWideLevels-level expansion of wide node `id`, calling f(slot, is_wide_child) for
-// every child slot in depth-first, left-to-right order.
-template <class F>
-__device__ void wide_expand(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark, uint32_t id, F&& f) {
-    uint32_t st_node[2 * kWideLevels + 2];
-    uint8_t st_side[2 * kWideLevels + 2], st_lvl[2 * kWideLevels + 2];
-    int sp = 0;
-    st_node[sp] = id; st_side[sp] = 1; st_lvl[sp] = 1; ++sp;
-    st_node[sp] = id; st_side[sp] = 0; st_lvl[sp] = 1; ++sp;
-    while (sp > 0) {
-        --sp;
-        const uint32_t nd = st_node[sp], side = st_side[sp], lvl = st_lvl[sp];
-        const ChildSlot s = nodes[nd].c[side];
-        if (s.ref == kInvalid) continue;
-        if (s.cnt > 0) { f(s, false); continue; }
-        if (lvl == kWideLevels || is_marked_root(rootmark, s.ref)) { f(s, true); continue; }
-        st_node[sp] = s.ref; st_side[sp] = 1; st_lvl[sp] = (uint8_t)(lvl + 1); ++sp;
-        st_node[sp] = s.ref; st_side[sp] = 0; st_lvl[sp] = (uint8_t)(lvl + 1); ++sp;
+// Warp-cooperative expansion of wide node `id`: the slots reached by expanding
+// kWideLevels binary levels, in tree order (left to right), item i held by
+// lane i.  A slot ends the expansion when it is a leaf, or an internal node
+// at the last level or at a map's root (which becomes a wide child); empty
+// slots are dropped.  Items are compacted level by level through `sbuf`
+// (64 words of the warp's shared memory).  Returns the item count (<= 32).
+constexpr uint32_t kItemPending = 0, kItemLeaf = 1, kItemWide = 2;
+
+__device__ uint32_t wide_expand_warp(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
+                                     uint32_t id, uint32_t lane, uint32_t* sbuf, uint32_t& slot, uint32_t& state) {
+    uint32_t count = 2;
+    slot = 2u * id + lane;
+    state = kItemPending;
+    for (int lvl = 1; lvl <= kWideLevels; ++lvl) {
+        uint32_t nout = 0, ref = kInvalid;
+        if (lane < count) {
+            nout = 1;
+            if (state == kItemPending) {
+                const ChildSlot& s = nodes[slot >> 1].c[slot & 1u];
+                ref = s.ref;
+                if (ref == kInvalid) nout = 0;
+                else if (s.cnt > 0) state = kItemLeaf;
+                else if (lvl == kWideLevels || is_marked_root(rootmark, ref)) state = kItemWide;
+                else nout = 2;
+            }
+        }
+        uint32_t x = nout;   // inclusive scan of the output counts
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        const uint32_t at = x - nout, total = __shfl_sync(0xffffffffu, x, 31);
+        if (nout == 1) {
+            sbuf[at] = slot;
+            sbuf[32 + at] = state;
+        } else if (nout == 2) {
+            sbuf[at] = 2u * ref;
+            sbuf[at + 1] = 2u * ref + 1u;
+            sbuf[32 + at] = kItemPending;
+            sbuf[32 + at + 1] = kItemPending;
+        }
+        __syncwarp();
+        count = total;
+        if (lane < count) { slot = sbuf[lane]; state = sbuf[32 + lane]; }
+        __syncwarp();
     }
+    return count;
 }
 
+// Warp per 32 consecutive compacted nodes: the child count of every wide
+// node among them (0 for the others).
 __global__ void k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
                              const uint32_t* __restrict__ wflag, const MapHeader* __restrict__ hdr, uint32_t bound,
                              uint32_t* __restrict__ wcnt) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= bound) return;
-    uint32_t c = 0;
-    if (t < hdr->num_nodes && wflag[t]) wide_expand(nodes, rootmark, t + 1, [&](const ChildSlot&, bool) { ++c; });
-    wcnt[t] = c;
+    __shared__ uint32_t s_buf[8][64];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (t0 >= bound) return;
+    const uint32_t m = hdr->num_nodes;
+    const uint32_t t = t0 + lane;
+    const bool wide = t < m && t < bound && wflag[t];
+    uint32_t mine = 0;
+    uint32_t todo = __ballot_sync(0xffffffffu, wide);
+    while (todo) {
+        const uint32_t b = __ffs(todo) - 1;
+        todo &= todo - 1;
+        uint32_t slot, state;
+        const uint32_t c = wide_expand_warp(nodes, rootmark, t0 + b + 1u, lane, s_buf[wib], slot, state);
+        if (lane == b) mine = c;
+    }
+    if (t < bound) wcnt[t] = mine;
 }
 
 __global__ void k_wide_emit(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
                             const uint32_t* __restrict__ wflag, const uint32_t* __restrict__ wcnt,
                             const uint32_t* __restrict__ wfirst, const MapHeader* __restrict__ hdr, uint32_t bound,
                             ChildSlot* __restrict__ wchild) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= bound || t >= hdr->num_nodes || !wflag[t]) return;
-    ChildSlot* out = wchild + wfirst[t];
-    uint32_t j = 0;
-    wide_expand(nodes, rootmark, t + 1, [&](const ChildSlot& s, bool wide) {
-        ChildSlot c = s;
-        if (wide) {
-            c.ref = wfirst[s.ref - 1];
-            c.cnt = kWideFlag | wcnt[s.ref - 1];
+    __shared__ uint32_t s_buf[8][64];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (t0 >= bound) return;
+    const uint32_t m = hdr->num_nodes;
+    const uint32_t t = t0 + lane;
+    uint32_t todo = __ballot_sync(0xffffffffu, t < m && t < bound && wflag[t]);
+    while (todo) {
+        const uint32_t b = __ffs(todo) - 1;
+        todo &= todo - 1;
+        uint32_t slot, state;
+        const uint32_t tb = t0 + b;
+        const uint32_t c = wide_expand_warp(nodes, rootmark, tb + 1u, lane, s_buf[wib], slot, state);
+        if (lane < c) {
+            ChildSlot s = nodes[slot >> 1].c[slot & 1u];
+            if (state == kItemWide) {
+                const uint32_t r = s.ref;
+                s.ref = wfirst[r - 1];
+                s.cnt = kWideFlag | wcnt[r - 1];
+            }
+            wchild[wfirst[tb] + lane] = s;
         }
-        out[j++] = c;
-    });
+    }
 }
 
 // The traversal's start slot: the super-root's slot, pointing at the wide node.
@@ -458,12 +553,12 @@ int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint
     int nl = 0;
     const uint32_t bound = n > 1 ? n - 1 : 1;   // internal nodes are at most n - 1
     const uint32_t tb = 128, grid = (bound + tb - 1) / tb;
+    const uint32_t wgrid = (bound + 32u * 8u - 1u) / (32u * 8u);   // 8 warps per block, 32 nodes per warp
     if (n > 1) {
         k_wide_flags<<<grid, tb, 0, st>>>(parent, rootmark, hdr, bound, wb.wflag);
-        nl += 1 + exclusive_scan(wb.wflag, wb.wrank, bound, wb.scratch + 1, wb.scratch, st);
-        k_wide_count<<<grid, tb, 0, st>>>(nodes, rootmark, wb.wflag, hdr, bound, wb.wcnt);
-        nl += 1 + exclusive_scan(wb.wcnt, wb.wfirst, bound, wb.scratch + 1, wb.scratch, st);
-        k_wide_emit<<<grid, tb, 0, st>>>(nodes, rootmark, wb.wflag, wb.wcnt, wb.wfirst, hdr, bound, wb.wchild);
+        k_wide_count<<<wgrid, 256, 0, st>>>(nodes, rootmark, wb.wflag, hdr, bound, wb.wcnt);
+        nl += 2 + exclusive_scan(wb.wcnt, wb.wfirst, bound, wb.scratch + 1, wb.scratch, st);
+        k_wide_emit<<<wgrid, 256, 0, st>>>(nodes, rootmark, wb.wflag, wb.wcnt, wb.wfirst, hdr, bound, wb.wchild);
         ++nl;
     }
     k_wide_root<<<1, 1, 0, st>>>(nodes, wb.wcnt, wb.wfirst, wb.wroot);

@@ -70,7 +70,6 @@ struct BuildBuffers {
 
 struct WideBuffers {
     uint32_t* wflag;       // per compacted node: is a wide node
-    uint32_t* wrank;       // scan of wflag
     uint32_t* wcnt;        // per wide node: child count
     uint32_t* wfirst;      // scan of wcnt: first child slot
     ChildSlot* wchild;     // child slots of all wide nodes
