@@ -268,10 +268,10 @@ QueryParams params_of(const pm_query_desc* d) {
 
 // Morton order of the queries (returns the permutation or nullptr).
 const uint32_t* sort_queries(pm_map* m, const float4* qpos, uint32_t nq, cudaStream_t st, int* launches) {
-    *launches += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint64_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
-    uint64_t* keys[2] = {P<uint64_t>(m->qkeys0), P<uint64_t>(m->qkeys1)};
+    *launches += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint32_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
+    uint32_t* keys[2] = {P<uint32_t>(m->qkeys0), P<uint32_t>(m->qkeys1)};
     uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
-    const int cur = radix_sort_pairs(keys, vals, nq, 48, P<uint32_t>(m->qscratch), st, launches);
+    const int cur = radix_sort_pairs32(keys, vals, nq, kQueryKeyBits, P<uint32_t>(m->qscratch), st, launches);
     return vals[cur];
 }
 
@@ -1119,12 +1119,13 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
     int nl = 0;
     const uint32_t* order = nullptr;
     if (desc->order == PM_ORDER_SORTED) {
-        uint64_t* keys[2] = {reinterpret_cast<uint64_t*>(base + kNoallocKeys0),
-                             reinterpret_cast<uint64_t*>(base + kNoallocKeys1)};
+        uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(base + kNoallocKeys0),
+                             reinterpret_cast<uint32_t*>(base + kNoallocKeys1)};
         uint32_t* vals[2] = {reinterpret_cast<uint32_t*>(base + kNoallocVals0),
                              reinterpret_cast<uint32_t*>(base + kNoallocVals1)};
         nl += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), keys[0], vals[0], st);
-        const int cur = radix_sort_pairs(keys, vals, nq, 48, reinterpret_cast<uint32_t*>(base + kNoallocSort), st, &nl);
+        const int cur = radix_sort_pairs32(keys, vals, nq, kQueryKeyBits, reinterpret_cast<uint32_t*>(base + kNoallocSort),
+                                           st, &nl);
         order = vals[cur];
     }
     QueryTuning t = tuning_of(m);

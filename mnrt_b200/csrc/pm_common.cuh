@@ -178,6 +178,24 @@ __device__ __forceinline__ uint32_t quantize16(float v, float lo, float scale) {
     return (uint32_t)t;
 }
 
+// 10 bits -> every third bit of 30.
+__device__ __forceinline__ uint32_t spread3_10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// 30-bit Morton code from the top 10 bits of each axis' 16-bit quantisation:
+// the order queries are processed in (coherence only; results do not depend
+// on it).
+__device__ __forceinline__ uint32_t morton30(float x, float y, float z, const float* lo, float scale) {
+    return (spread3_10(quantize16(x, lo[0], scale) >> 6) << 2) | (spread3_10(quantize16(y, lo[1], scale) >> 6) << 1) |
+           spread3_10(quantize16(z, lo[2], scale) >> 6);
+}
+
 __device__ __forceinline__ uint64_t morton48(float x, float y, float z, const float* lo, float scale) {
     return (spread3_16(quantize16(x, lo[0], scale)) << 2) | (spread3_16(quantize16(y, lo[1], scale)) << 1) |
            spread3_16(quantize16(z, lo[2], scale));

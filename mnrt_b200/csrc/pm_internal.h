@@ -108,8 +108,9 @@ struct QueryOutputs {
     uint32_t* count;     // optional
 };
 
-int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint64_t* keys, uint32_t* vals,
+int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
                        cudaStream_t st);
+constexpr int kQueryKeyBits = 30;   // bits of the query Morton keys (sorted as uint32)
 struct QueryTuning {
     int layout;             // 0: lane per query with a shared-memory heap; 1: group buffers
     int queries_per_warp;   // group layout: 1, 2, 4 or 8 (32, 16, 8 or 4 lanes per query)

@@ -1247,18 +1247,21 @@ __global__ void __launch_bounds__(kBruteThreads) k_knn_brute(KnnArgs a, uint32_t
 }
 
 __global__ void k_query_morton(const float4* __restrict__ qpos, uint32_t nq, const MapHeader* __restrict__ hdr,
-                               uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                               uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nq) return;
     const float ext = fmaxf(fmaxf(__fsub_rn(hdr->hi[0], hdr->lo[0]), __fsub_rn(hdr->hi[1], hdr->lo[1])),
                             __fsub_rn(hdr->hi[2], hdr->lo[2]));
     const float scale = (ext > 0.0f && isfinite(ext)) ? __fdiv_rn(65536.0f, ext) : 0.0f;
     const float4 p = qpos[i];
-    keys[i] = morton48(p.x, p.y, p.z, hdr->lo, scale);
+    keys[i] = morton30(p.x, p.y, p.z, hdr->lo, scale);
     vals[i] = i;
 }
 
-int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint64_t* keys, uint32_t* vals,
+// 30-bit query keys: 4 radix passes instead of the tree's 6 (a cell is 1/1024
+// of the map's extent per axis, finer than the query spacing of the measured
+// workloads).
+int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
                       cudaStream_t st) {
     if (!nq) return 0;
     k_query_morton<<<(nq + 255) / 256, 256, 0, st>>>(qpos, nq, hdr, keys, vals);
