@@ -398,7 +398,8 @@ typedef struct pm_timings {
 PM_API pm_status pm_set_profiling(pm_map* map, int enable);
 PM_API pm_status pm_last_timings(pm_map* map, pm_timings* out);
 
-/* Traversal counters of the last pm_query with the group layout, collected
+/* Traversal counters of the last pm_query with a binary layout (PM_KBUF_HEAP or
+ * PM_KBUF_GROUP; the 32-wide layout keeps no counters), collected
  * when profiling is enabled with level 2 (costs some speed).  Synchronous.
  * out[0..7]: queries, internal nodes visited (per warp), leaves visited (per
  * warp), photons tested (per warp), candidates appended, selections, radius

@@ -200,7 +200,7 @@ class PhotonMap:
                   "redos", "unbounded")
 
     def query_stats(self) -> dict:
-        """Traversal counters of the last query (needs set_profiling(2))."""
+        """Traversal counters of the last query with a binary layout (needs set_profiling(2))."""
         import numpy as np
         out = np.zeros(8, np.uint64)
         L.check(self._lib.pm_query_stats(self._h, out.ctypes.data, 8), self._h)
