@@ -228,13 +228,13 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+def profiled_traffic(kernel: str, workload: str, field: str = "dram_bytes_per_launch"):
+    """Bytes per launch (DRAM by default) from the committed ncu summary, if one exists."""
     f = ROOT / "profiles" / f"{kernel}_{workload}.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(field + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -356,6 +356,7 @@ def run_ours(args, cfg) -> dict | None:
         "query_kernel_ms": kern_ms, "query_only_mqueries_per_s": Q / (float(np.mean(queries)) / 1000.0) / 1e6,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": profiled_traffic("k_knn_group", args.config), "kernel": "k_knn_group",
+                     "l2_traffic": profiled_traffic("k_knn_group", args.config, "l2_bytes_per_launch"),
                      "algorithmic_bytes_per_launch": alg_bytes, "peak_source": peak_kind},
         "roofline_build": {"bound": "hbm", "achieved": build_bytes / (build_ms / 1000.0) / 1e9, "peak": peak,
                            "unit": "GB/s", "frac": build_bytes / (build_ms / 1000.0) / 1e9 / peak,
