@@ -781,22 +781,32 @@ __device__ __forceinline__ double est_fp64_group(const KnnArgs& a, const uint64_
     return r2d;
 }
 
-// The sorted neighbour row of one query (rank sort by exact (d^2, caller
-// index)).  Out of line and with scalar arguments: only list-producing calls
-// reach it, and keeping it out of the hot instance measured 7.85 -> 7.61 ms
-// together with the statistics compiled out of the wide instances.
+// The sorted neighbour row of one query: the n kept keys, made exact
+// ((d^2, caller index), unique), padded to a power of two and bitonic-sorted
+// in place in the group's buffer (capacity >= that power of two).  Out of
+// line and with scalar arguments: only list-producing calls reach it, and
+// keeping it out of the hot instance measured 7.85 -> 7.61 ms together with
+// the statistics compiled out of the wide instances.
 template <int G>
 __device__ __noinline__ void write_neighbours(uint64_t* buf, uint32_t n, uint32_t s, uint32_t gmask,
                                               const float4* __restrict__ pos, uint32_t* row, uint32_t k,
                                               uint32_t ph_off) {
-    for (uint32_t e = s; e < n; e += G) buf[e] = exact_key(buf[e], pos);
+    uint32_t N = 1;
+    while (N < n) N <<= 1;
+    for (uint32_t e = s; e < N; e += G) buf[e] = e < n ? exact_key(buf[e], pos) : ~0ull;
     __syncwarp(gmask);
-    for (uint32_t e = s; e < n; e += G) {
-        const uint64_t v = buf[e];
-        uint32_t rank = 0;
-        for (uint32_t f = 0; f < n; ++f) rank += buf[f] < v ? 1u : 0u;
-        row[rank] = (uint32_t)v - ph_off;
+    for (uint32_t size = 2; size <= N; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = s; i < N / 2; i += G) {
+                const uint32_t lo = ((i & ~(stride - 1u)) << 1) | (i & (stride - 1u)), hi = lo + stride;
+                const uint64_t x = buf[lo], y = buf[hi];
+                const bool up = (lo & size) == 0;
+                if ((x > y) == up) { buf[lo] = y; buf[hi] = x; }
+            }
+            __syncwarp(gmask);
+        }
     }
+    for (uint32_t e = s; e < n; e += G) row[e] = (uint32_t)buf[e] - ph_off;
     for (uint32_t j = n + s; j < k; j += G) row[j] = kInvalid;
     __syncwarp(gmask);
 }
