@@ -103,7 +103,7 @@ __global__ void k_batch_geom(const uint32_t* __restrict__ acc, uint32_t m, Batch
     const float ext = fmaxf(fmaxf(__fsub_rn(hi[0], g.lo[0]), __fsub_rn(hi[1], g.lo[1])), __fsub_rn(hi[2], g.lo[2]));
     g.mscale = (ext > 0.0f && isfinite(ext)) ? __fdiv_rn(65536.0f, ext) : 0.0f;
     g.max_power = ord2f(a[6]);
-    g.fix_scale = g.max_power > 0.0f ? __fdiv_rn(1099511627776.0f, g.max_power) : 0.0f;   // 2^40 / max
+    g.fix_scale = fix_scale_of(g.max_power);
     g.pad[0] = g.pad[1] = 0;
     g.root.lo[0] = g.root.lo[1] = g.root.lo[2] = INFINITY;
     g.root.hi[0] = g.root.hi[1] = g.root.hi[2] = -INFINITY;

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kBoundsThreads) k_bounds(const float4* __restr
     rb = __float_as_uint(s_v[0][7]);
     for (int a = 0; a < 3; ++a) { hdr->lo[a] = r[a]; hdr->hi[a] = r[a + 3]; }
     hdr->max_power = r[6];
-    hdr->fix_scale = (r[6] > 0.0f) ? __fdiv_rn(1099511627776.0f, r[6]) : 0.0f;   // 2^40 / max
+    hdr->fix_scale = fix_scale_of(r[6]);
     hdr->n = n;
     if (rb) atomicOr(&hdr->errors, kErrNonFinite);
     *reinterpret_cast<unsigned int*>(partials + 8 * gridDim.x) = 0u;   // ready for the next build
@@ -345,7 +345,7 @@ __global__ void k_scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         hdr->max_power = __fmul_rn(hdr->max_power, fabsf(scale));
-        hdr->fix_scale = (hdr->max_power > 0.0f) ? __fdiv_rn(1099511627776.0f, hdr->max_power) : 0.0f;
+        hdr->fix_scale = fix_scale_of(hdr->max_power);
     }
     if (i >= n) return;
     float4 w = pw[i];

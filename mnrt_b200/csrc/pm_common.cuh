@@ -49,7 +49,7 @@ struct MapHeader {
     float lo[3];
     float hi[3];
     float max_power;
-    float fix_scale;    // 2^40 / max_power (0 if max_power == 0)
+    float fix_scale;    // fix_scale_of(max_power): fixed-point scale of the kNN flux sums
     uint32_t n;
     uint32_t num_nodes; // internal nodes (excluding the super-root at index 0)
     uint32_t errors;
@@ -57,6 +57,16 @@ struct MapHeader {
 };
 
 // ------------------------------------------------------------ arithmetic --
+
+// Fixed-point scale of the kNN flux sums: 2^53 / max |flux| (0 without flux,
+// clamped to 2^127 for tiny flux), so a term is at most 2^53 and the up to
+// 128 terms of one query sum below 2^60.  The resolution, 2^-53 of the
+// largest photon flux, keeps channels of very small flux exact to FP64-like
+// relative precision.
+constexpr float kFixOne = 9007199254740992.0f;   // 2^53
+__device__ __forceinline__ float fix_scale_of(float max_power) {
+    return max_power > 0.0f ? fminf(__fdiv_rn(kFixOne, max_power), 1.7014118346046923e38f) : 0.0f;
+}
 
 __device__ __forceinline__ float d2_rn(float qx, float qy, float qz, float px, float py, float pz) {
     const float dx = __fsub_rn(px, qx), dy = __fsub_rn(py, qy), dz = __fsub_rn(pz, qz);

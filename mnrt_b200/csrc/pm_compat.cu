@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(kCompatThreads) k_compat_query(CompatArgs a) {
         if (finite && count > 0 && count >= a.min_found && r2u > 0.0f) {
             const double r2d = (double)r2u;
             const double kc = (double)a.cone_k;
-            const float scale = a.hdr->fix_scale;
+            // 2^40 / max flux: a range may hold far more than 128 photons
+            const float scale = __fmul_rn(a.hdr->fix_scale, 1.220703125e-4f);
             long long c0 = 0, c1 = 0, c2 = 0;
             range_search(a.nodes, a.pos, qp.x, qp.y, qp.z, r2, [&](uint32_t t, float) {
                 const float4 w = a.pow[t];

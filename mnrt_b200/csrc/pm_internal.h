@@ -26,7 +26,7 @@ struct __align__(16) BatchGeom {
     ChildSlot wroot;       // the same subtree in the 32-wide tree
     float lo[3];           // photon bounds, lower corner
     float mscale;          // Morton scale of the map's cubic cell
-    float fix_scale;       // 2^40 / largest flux channel
+    float fix_scale;       // fix_scale_of(largest flux channel)
     float max_power;
     uint32_t pad[2];
 };

@@ -139,7 +139,7 @@ struct Filter64 {
         edge2 = 0.0; edge = 0.0f; inv = 0.0f;
         if (f == 1) {
             const double e = __dmul_rn((double)cone_k, __dsqrt_rn(r2));
-            edge2 = __dmul_rn(e, e);
+            edge2 = __dmul_rn(__dmul_rn((double)cone_k, (double)cone_k), r2);   // exact r^2 for k_c = 1
             edge = __double2float_rn(e);
         } else if (f == 2) {
             edge2 = r2;
@@ -176,17 +176,22 @@ __device__ __forceinline__ long long fixed_term(float w, float phi, float scale)
 }
 
 // FP32 filter weights (the common path).  Their absolute error is below
-// about 8e-7 (FP32 d^2 against FP64, the reciprocal square root, r), so the
-// estimate's relative error is below 8e-7 * sum(flux) / sum(w * flux) plus
-// about 3e-7 from r^2: the FP32 path is kept when sum(w * flux) is at least
-// sum(flux) / 6 (bound 5.1e-6), decided on the fixed-point sums (identical in
-// every kernel), and the query is re-evaluated with FP64 distances otherwise.
+// about 8e-7 (FP32 d^2 against FP64, the reciprocal square root, r), so a
+// channel's relative error is below 8e-7 * sum(flux) / sum(w * flux) of that
+// channel plus about 3e-7 from r^2: the FP32 path is kept when, in every
+// channel, sum(w * flux) is at least sum(flux) / 6 (bound 5.1e-6), decided on
+// the fixed-point sums (identical in every kernel); the query is re-evaluated
+// with FP64 distances otherwise.
 __device__ __forceinline__ float filter_inv32(int filter, float r2, float cone_k) {
     if (filter == 1) return __frcp_rn(__fmul_rn(cone_k, __fsqrt_rn(r2)));
     if (filter == 2) return __frcp_rn(r2);
     return 0.0f;
 }
 
+// The k-th neighbour's FP32 weight is 0 only up to that absolute error (its
+// FP64 weight is exactly 1 - 1/k_c, 0 for k_c = 1); the per-channel FP64 test
+// below sends every query where that matters to the FP64 path, which is exact
+// on the edge.
 __device__ __forceinline__ float filter_weight32(int filter, float d2, float inv) {
     if (filter == 1) {
         const float d = d2 > 0.0f ? __fmul_rn(d2, rsqrtf(d2)) : 0.0f;
@@ -197,8 +202,8 @@ __device__ __forceinline__ float filter_weight32(int filter, float d2, float inv
 }
 
 struct EstAcc {
-    long long c0, c1, c2;   // weighted flux, fixed point
-    long long f;            // unweighted flux (all channels), fixed point
+    long long c0, c1, c2;   // weighted flux per channel, fixed point (scale s = fix_scale)
+    uint32_t f0, f1, f2;    // |flux| per channel at s * 2^-29, each term rounded up
 };
 
 // One neighbour's terms from its loaded flux record w.
@@ -209,7 +214,10 @@ __device__ __forceinline__ void est_add32w(const KnnArgs& a, const float4& w, fl
     acc.c0 += fixed_term(wt, w.x, scale);
     acc.c1 += fixed_term(wt, w.y, scale);
     acc.c2 += fixed_term(wt, w.z, scale);
-    acc.f += fixed_term(1.0f, __fadd_rn(__fadd_rn(w.x, w.y), w.z), scale);
+    const float s32 = __fmul_rn(scale, 1.862645149230957e-09f);   // 2^-29
+    acc.f0 += __float2uint_ru(__fmul_rn(fabsf(w.x), s32));
+    acc.f1 += __float2uint_ru(__fmul_rn(fabsf(w.y), s32));
+    acc.f2 += __float2uint_ru(__fmul_rn(fabsf(w.z), s32));
 }
 
 __device__ __forceinline__ void est_add32(const KnnArgs& a, uint32_t t, float d2, float inv, float nx, float ny,
@@ -220,7 +228,10 @@ __device__ __forceinline__ void est_add32(const KnnArgs& a, uint32_t t, float d2
     acc.c0 += fixed_term(wt, w.x, scale);
     acc.c1 += fixed_term(wt, w.y, scale);
     acc.c2 += fixed_term(wt, w.z, scale);
-    acc.f += fixed_term(1.0f, __fadd_rn(__fadd_rn(w.x, w.y), w.z), scale);
+    const float s32 = __fmul_rn(scale, 1.862645149230957e-09f);   // 2^-29
+    acc.f0 += __float2uint_ru(__fmul_rn(fabsf(w.x), s32));
+    acc.f1 += __float2uint_ru(__fmul_rn(fabsf(w.y), s32));
+    acc.f2 += __float2uint_ru(__fmul_rn(fabsf(w.z), s32));
 }
 
 __device__ __forceinline__ void est_add64(const KnnArgs& a, uint32_t t, const Filter64& flt, float nx, float ny,
@@ -233,8 +244,17 @@ __device__ __forceinline__ void est_add64(const KnnArgs& a, uint32_t t, const Fi
     acc.c2 += fixed_term(wt, w.z, scale);
 }
 
+// Per channel: the FP32 weights' absolute error becomes a relative error of
+// that channel's estimate scaled by its sum(flux) / sum(w * flux), so every
+// channel must pass on its own (a channel whose flux sits in low-weight
+// neighbours, e.g. the k-th at weight zero, would otherwise slip through).
+// The unweighted sums are kept in 32 bits at 2^24 / max flux with every term
+// rounded up, which can only send more queries to FP64.
 __device__ __forceinline__ bool est_needs_fp64(int filter, const EstAcc& acc) {
-    return filter != 0 && 6 * (acc.c0 + acc.c1 + acc.c2) < acc.f;
+    if (filter == 0) return false;
+    const double k29 = 536870912.0;   // 2^29: the unweighted sums' scale to the weighted sums'
+    return 6.0 * (double)acc.c0 < (double)acc.f0 * k29 || 6.0 * (double)acc.c1 < (double)acc.f1 * k29 ||
+           6.0 * (double)acc.c2 < (double)acc.f2 * k29;
 }
 
 __device__ __forceinline__ float4 est_result(const EstAcc& acc, int filter, double r2, float cone_k, float scale,
@@ -258,7 +278,7 @@ __device__ __forceinline__ double est_fp64_heap(const KnnArgs& a, const uint64_t
     const float scale = *a.scale_ptr;
     Filter64 flt;
     flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
-    acc = EstAcc{0, 0, 0, 0};
+    acc = EstAcc{0, 0, 0, 0, 0, 0};
     for (uint32_t j = 0; j < hn; ++j) est_add64(a, (uint32_t)h[j * stride], flt, nx, ny, nz, scale, acc);
     return r2d;
 }
@@ -302,7 +322,7 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
     if (hn > 0 && hn >= a.min_found && r2 > 0.0f) {
         const float scale = *a.scale_ptr;
         const float inv = filter_inv32(a.filter, r2, a.cone_k);
-        EstAcc acc = {0, 0, 0, 0};
+        EstAcc acc = {0, 0, 0, 0, 0, 0};
         for (uint32_t j = 0; j < hn; ++j) {
             const uint64_t key = h[j * stride];
             est_add32(a, (uint32_t)key, __uint_as_float((uint32_t)(key >> 32)), inv, nx, ny, nz, scale, acc);
@@ -773,7 +793,7 @@ __device__ __forceinline__ double est_fp64_group(const KnnArgs& a, const uint64_
     const float scale = *a.scale_ptr;
     Filter64 flt;
     flt.init(a.filter, a.cone_k, qx, qy, qz, r2d);
-    acc = EstAcc{0, 0, 0, 0};
+    acc = EstAcc{0, 0, 0, 0, 0, 0};
     for (uint32_t e = s; e < n; e += G) est_add64(a, (uint32_t)buf[e], flt, nx, ny, nz, scale, acc);
     acc.c0 = gsum_i64<G>(acc.c0, gmask);
     acc.c1 = gsum_i64<G>(acc.c1, gmask);
@@ -829,7 +849,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
     if (n > 0 && n >= a.min_found && r2 > 0.0f) {
         const float scale = *a.scale_ptr;
         const float inv = filter_inv32(a.filter, r2, a.cone_k);
-        EstAcc acc = {0, 0, 0, 0};
+        EstAcc acc = {0, 0, 0, 0, 0, 0};
         // two neighbours per step, both flux records requested before either is
         // used (measured 8.34 -> 8.07 ms; four at once spills)
         for (uint32_t e = s; e < n; e += 2 * G) {
@@ -844,7 +864,9 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
         acc.c0 = gsum_i64<G>(acc.c0, gmask);
         acc.c1 = gsum_i64<G>(acc.c1, gmask);
         acc.c2 = gsum_i64<G>(acc.c2, gmask);
-        acc.f = gsum_i64<G>(acc.f, gmask);
+        acc.f0 = __reduce_add_sync(gmask, acc.f0);
+        acc.f1 = __reduce_add_sync(gmask, acc.f1);
+        acc.f2 = __reduce_add_sync(gmask, acc.f2);
         double r2d = (double)r2;
         if (est_needs_fp64(a.filter, acc)) {
             if (kFix) {

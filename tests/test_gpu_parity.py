@@ -335,3 +335,19 @@ def test_build_query_host_empty_inputs(cuda):
     torch.cuda.synchronize()
     assert out.shape == (10, 4) and not out.any()
     assert pm.info().device_errors == 0
+
+
+@pytest.mark.parametrize("k,filt", [(1, "cone"), (2, "cone"), (2, "epanechnikov"), (5, "cone")])
+def test_channel_imbalanced_flux_small_k(cuda, oracle_mod, k, filt):
+    """Per-channel accuracy of the FP32 fast path: when one channel's flux sits
+    almost entirely in low-weight neighbours (the k-th at weight zero), that
+    channel alone must trigger the FP64 re-evaluation."""
+    ph = gen.photons(60000, seed=910, caustic_frac=0.2)
+    rng = np.random.default_rng(911)
+    tiny = rng.random(ph.n) < 0.5
+    ph.pow[tiny, 2] *= np.float32(1e-4)          # half the photons carry almost no blue
+    ph.pow[~tiny, 0] *= np.float32(1e-4)         # the other half almost no red
+    q = gen.queries(5000, seed=912)
+    res = run(ph, q, cuda, k, 1.5, filt, leaf=32, tuning=dict(kbuf_layout=2))
+    assert res["info"].device_errors == 0
+    check_against_oracle(oracle_mod, ph, q, res, k, 1.5, filt)
