@@ -10,10 +10,14 @@ R = 0.05, cone filter, FP32.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank runs an independent replica (its own seeded map and
-query set): the path has no data exchange, so scaling is weak and value is
-the total queries/s of all ranks.  --impl reference times the CPU port of the
-reference algorithm (oracle/, multithreaded kd-tree) on the same workload.
+Under torchrun (one rank per GPU) the plain, final-gather and icut
+workloads run an independent replica per rank (its own seeded map and query
+set, no data exchange): scaling is weak and value is the total queries/s of
+all ranks.  The batch workload divides its maps over the ranks by LPT; the
+diff workload builds the map on every rank, divides the queries and sums the
+adjoint's partial gradients with one all-reduce (mnrt_b200/shard.py).
+--impl reference times the CPU port of the reference algorithm (oracle/,
+multithreaded kd-tree) on the same workload.
 """
 from __future__ import annotations
 
@@ -242,10 +246,11 @@ def profiled_traffic(kernel: str, workload: str, field: str = "dram_bytes_per_la
     return None
 
 
-def run_ours(args, cfg) -> dict | None:
+def init_ranks():
+    """(world, rank, local rank, device) from the torchrun environment; a
+    world above one gets an NCCL process group with a short timeout."""
     import torch
     import torch.distributed as dist
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -254,6 +259,29 @@ def run_ours(args, cfg) -> dict | None:
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    return world, rank, local, dev
+
+
+def close_ranks(world: int) -> None:
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def barrier(world: int) -> None:
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_ours(args, cfg) -> dict | None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local, dev = init_ranks()
 
     from mnrt_b200.photon_map import PhotonMap
 
@@ -369,9 +397,7 @@ def run_ours(args, cfg) -> dict | None:
         "tree_nodes": nodes,
         "device_errors": info.device_errors,
     }
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    close_ranks(world)
     if rank != 0:
         return None
     if world == 1 and not args.no_cpu_baseline:
@@ -386,33 +412,40 @@ def run_ours(args, cfg) -> dict | None:
     return result
 
 
-def run_diff(args, cfg) -> dict:
+def run_diff(args, cfg) -> dict | None:
     """Differentiation workload: forward (build + query with neighbour lists)
     and adjoint (dL/dpower, dL/dposition) of L = sum |E - T|^2, T from powers
-    scaled by seeded U[0.5, 1.5]; then gradient descent on the powers."""
+    scaled by seeded U[0.5, 1.5]; then gradient descent on the powers.
+    Under torchrun the map is built on every rank and the queries are divided
+    (contiguous ranges); each rank's adjoint is a partial sum over its
+    queries, and one all-reduce of the two gradients (inside the timed step)
+    completes it.  Loss and line-search sums are all-reduced scalars."""
     import torch
     from mnrt_b200.photon_map import PhotonMap
+    from mnrt_b200.shard import allreduce_gradients, allreduce_scalars, query_range
 
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
-    ph, q = make_inputs(cfg, 0)
+    world, rank, local, dev = init_ranks()
+    ph, q = make_inputs(cfg, 0)          # one map and one query set, divided by query range
     N, Q, k, R, filt = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"], cfg["filter"]
+    qa, qb = query_range(Q, rank, world)
+    Qr = qb - qa
     rng = np.random.default_rng(4242)
     tpow = ph.pow.copy()
     tpow[:, :3] *= rng.uniform(0.5, 1.5, size=(N, 3)).astype(np.float32)
     d_pos, d_pow = torch.from_numpy(ph.pos).to(dev), torch.from_numpy(ph.pow).to(dev)
     d_tpow = torch.from_numpy(tpow).to(dev)
-    d_qpos, d_qnrm = torch.from_numpy(q.pos).to(dev), torch.from_numpy(q.nrm).to(dev)
+    d_qpos = torch.from_numpy(np.ascontiguousarray(q.pos[qa:qb])).to(dev)
+    d_qnrm = torch.from_numpy(np.ascontiguousarray(q.nrm[qa:qb])).to(dev)
     pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
-    pm.reserve(N, Q)
+    pm.reserve(N, Qr)
     kw = dict(k=k, r_max=R, filter=filt)
     pm.build(d_pos, d_tpow)
     target = pm.query(d_qpos, d_qnrm, **kw)["rad"][:, :3].clone()
-    out = {"rad": torch.empty((Q, 4), dtype=torch.float32, device=dev),
-           "nbr": torch.empty((Q, k), dtype=torch.int32, device=dev),
-           "count": torch.empty((Q,), dtype=torch.int32, device=dev)}
-    out_plain = {"rad": torch.empty((Q, 4), dtype=torch.float32, device=dev)}
-    g = torch.zeros((Q, 4), dtype=torch.float32, device=dev)
+    out = {"rad": torch.empty((Qr, 4), dtype=torch.float32, device=dev),
+           "nbr": torch.empty((Qr, k), dtype=torch.int32, device=dev),
+           "count": torch.empty((Qr,), dtype=torch.int32, device=dev)}
+    out_plain = {"rad": torch.empty((Qr, 4), dtype=torch.float32, device=dev)}
+    g = torch.zeros((Qr, 4), dtype=torch.float32, device=dev)
     gpow = torch.empty((N, 4), dtype=torch.float32, device=dev)
     gpos = torch.empty((N, 4), dtype=torch.float32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
@@ -425,10 +458,12 @@ def run_diff(args, cfg) -> dict:
     def bwd():
         g[:, :3] = 2.0 * (out["rad"][:, :3] - target)
         pm.query_backward(d_qpos, d_qnrm, g, nbr=out["nbr"], count=out["count"], grad_pow=gpow, grad_pos=gpos, **kw)
+        allreduce_gradients(gpow, gpos)
 
     for _ in range(args.warmup):
         fwd(out_plain); fwd(out); bwd()
     t_fwd, t_bwd = [], []
+    barrier(world)
     for _ in range(args.steps):
         flush.zero_()
         ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
@@ -442,7 +477,9 @@ def run_diff(args, cfg) -> dict:
         flush.zero_()
         ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
         plain.append(ev[0].elapsed_time(ev[1]))
-    fwd_ms, bwd_ms, plain_ms = float(np.mean(t_fwd)), float(np.mean(t_bwd)), float(np.mean(plain))
+    barrier(world)
+    fwd_ms, bwd_ms, plain_ms, step_ms = rank_max([float(np.mean(t_fwd)), float(np.mean(t_bwd)), float(np.mean(plain)),
+                                                  float(np.mean(np.add(t_fwd, t_bwd)))], dev)
 
     # gradient descent on the powers; E is linear in them, so the step along
     # -dL/dpower is the exact line-search minimiser alpha = |grad|^2 / |A grad|^2
@@ -456,28 +493,34 @@ def run_diff(args, cfg) -> dict:
         pm.build(d_pos, pw)
         pm.query(d_qpos, d_qnrm, out=out, **kw)
         res = out["rad"][:, :3] - target
-        losses.append(float((res.double() ** 2).sum()))
+        losses.append(allreduce_scalars([float((res.double() ** 2).sum())])[0])
         if it == steps:
             break
         g[:, :3] = 2.0 * res
         pm.query_backward(d_qpos, d_qnrm, g, nbr=out["nbr"], count=out["count"], grad_pow=gpow, want_pos=False, **kw)
+        allreduce_gradients(gpow)
         dirp[:, :3] = gpow[:, :3]
         dirp[:, 3] = pw[:, 3]                       # direction bits ride along
         pm.build(d_pos, dirp)
         ag = pm.query(d_qpos, d_qnrm, out=out_plain, **kw)["rad"][:, :3].double()
         num = float((gpow[:, :3].double() ** 2).sum())
-        den = 2.0 * float((ag ** 2).sum())
+        den = 2.0 * allreduce_scalars([float((ag ** 2).sum())])[0]
         alpha = num / den if den > 0 else 0.0
         pw[:, :3] -= float(alpha) * gpow[:, :3]
     torch.cuda.synchronize()
     gd_s = time.perf_counter() - t0
     pm.close()
+    close_ranks(world)
+    if rank != 0:
+        return None
     return {
         "metric": "forward + adjoint time of the radiance estimate (differentiation workload)",
-        "value": fwd_ms + bwd_ms, "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "dtype": "f32 (adjoint sums in f64)", "data": "synthetic",
+        "value": step_ms, "unit": "ms", "higher_is_better": False, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "scaling": "strong", "dtype": "f32 (adjoint sums in f64)", "data": "synthetic",
         "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R, "filter": filt,
-                   "l2": "flushed between steps (256 MiB write, untimed)"},
+                   "l2": "flushed between steps (256 MiB write, untimed)",
+                   "parallelism": "one GPU" if world == 1 else
+                   f"map on every rank, queries divided over {world} ranks, gradient all-reduce (NCCL, f64)"},
         "forward_ms": fwd_ms, "forward_no_lists_ms": plain_ms, "backward_ms": bwd_ms,
         "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms, "fwd_bwd_over_fwd_no_lists": (fwd_ms + bwd_ms) / plain_ms,
         "gradient_descent": {"steps": steps, "loss_first": losses[0], "loss_last": losses[-1],
@@ -486,19 +529,18 @@ def run_diff(args, cfg) -> dict:
     }
 
 
-def run_icut(args, cfg) -> dict:
+def run_icut(args, cfg) -> dict | None:
     """Final gathering with illumination cuts (the reference's default
     GatherFor, PhotonMap.cpp:244-257): per step, build the tree and its cut
     (leaves as the coarse cut, exact-kNN irradiance at every node centre,
     4 refinement rounds, accuracy 0.2), then interpolate the cut at every
-    query.  Also times the photon-search estimate on the same queries."""
+    query.  Also times the photon-search estimate on the same queries.
+    Under torchrun every rank runs its own map and queries (replicas)."""
     import torch
     from mnrt_b200.photon_map import PhotonMap
-    from oracle import oracle
 
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
-    ph, q = make_inputs(cfg, 0)
+    world, rank, local, dev = init_ranks()
+    ph, q = make_inputs(cfg, rank)
     N, Q, k, R = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"]
     d_pos, d_pow = torch.from_numpy(ph.pos).to(dev), torch.from_numpy(ph.pow).to(dev)
     d_qp, d_qn = torch.from_numpy(q.pos).to(dev), torch.from_numpy(q.nrm).to(dev)
@@ -520,6 +562,7 @@ def run_icut(args, cfg) -> dict:
     for _ in range(args.warmup):
         step()
     tot, cut, interp = [], [], []
+    barrier(world)
     for _ in range(args.steps):
         flush.zero_()
         ev[0].record(); step(); ev[3].record(); ev[3].synchronize()
@@ -535,22 +578,25 @@ def run_icut(args, cfg) -> dict:
         flush.zero_()
         ev[0].record(); pm.query(d_qp, d_qn, out=qo, **qdesc); ev[1].record(); ev[1].synchronize()
         knn.append(ev[0].elapsed_time(ev[1]))
+    barrier(world)
     ns = pm.icut_slot_count()
     cutx = pm.icut_export()
     info = pm.info()
-    tot_ms, cut_ms, interp_ms, knn_ms = (float(np.mean(x)) for x in (tot, cut, interp, knn))
+    tot_ms, cut_ms, interp_ms, knn_ms = rank_max([float(np.mean(x)) for x in (tot, cut, interp, knn)], dev)
     irr = out[:, :3].sum(1).cpu().numpy()
     direct = qo["rad"][:, :3].sum(1).cpu().numpy()
     ok = direct > 0
     ratio = irr[ok] / direct[ok]
     res = {
         "metric": "final-gather irradiance from the illumination cut: queries/s (build + cut + interpolation per step)",
-        "value": Q / (tot_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "dtype": "f32 (interpolation sums in f64)", "data": "synthetic",
+        "value": world * Q / (tot_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "scaling": "weak", "dtype": "f32 (interpolation sums in f64)",
+        "data": "synthetic",
         "config": {"workload": cfg["workload"] + "; illumination cut: leaves as coarse cut, 4 refinement rounds, "
                                "accuracy 0.2, node-centre estimate exact kNN (box, min_found 8)",
                    "photons": N, "queries": Q, "k": k, "r_max": R,
-                   "l2": "flushed between steps (256 MiB write, untimed)"},
+                   "l2": "flushed between steps (256 MiB write, untimed)",
+                   "parallelism": f"{world} independent replica(s), one per GPU"},
         "step_ms": tot_ms, "build_ms": tot_ms - cut_ms - interp_ms, "cut_build_ms": cut_ms,
         "interpolation_ms": interp_ms, "interpolation_queries_per_s": Q / (interp_ms / 1000.0),
         "knn_query_ms": knn_ms, "interpolation_speedup_over_knn": knn_ms / interp_ms,
@@ -558,7 +604,12 @@ def run_icut(args, cfg) -> dict:
         "interp_over_knn_estimate": {"median": float(np.median(ratio)),
                                      "p25": float(np.percentile(ratio, 25)), "p75": float(np.percentile(ratio, 75))},
     }
-    if not args.no_cpu_baseline:
+    close_ranks(world)
+    if rank != 0:
+        pm.close()
+        return None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
         nodes, _tpos, _tpow = pm.export_tree()
         threads = oracle.threads_available()
         rng = np.random.default_rng(7)
@@ -575,46 +626,53 @@ def run_icut(args, cfg) -> dict:
     return res
 
 
-def run_batch(args) -> dict:
+def run_batch(args) -> dict | None:
     """Config 3: 64 photon maps (photon counts log-uniform in [1e4, 2e6], query
     counts log-uniform in [1e3, 1e6], k from {16, 32, 64, 128}, R = 0.05),
     built and queried as one batch (eager and CUDA-graph replay) against 64
-    sequential per-map build + query calls."""
+    sequential per-map build + query calls.  Under torchrun the maps are
+    divided over the ranks by LPT over photons + queries; each rank builds and
+    queries its own maps as one batch, with no exchange: the whole batch's
+    queries over the slowest rank's time."""
     import torch
     from mnrt_b200 import gen
-    from mnrt_b200.batch import PhotonMapBatch, make_desc
+    from mnrt_b200.batch import PhotonMapBatch
     from mnrt_b200.photon_map import PhotonMap
+    from mnrt_b200.shard import lpt_assign, map_costs
 
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
+    world, rank, local, dev = init_ranks()
     spec = gen.batch_spec(args.maps, seed=777)
-    phs = [gen.photons(n, seed=sd, caustic_frac=0.2) for n, sd in zip(spec.n, spec.seeds)]
-    qs = [gen.queries(nq, seed=sd + 500) for nq, sd in zip(spec.nq, spec.seeds)]
-    descs = [dict(k=k, r_max=0.05, filter="cone") for k in spec.k]
-    poff = np.concatenate([[0], np.cumsum(spec.n)]).astype(np.uint32)
-    qoff = np.concatenate([[0], np.cumsum(spec.nq)]).astype(np.uint32)
+    N_all, Q_all = int(np.sum(spec.n)), int(np.sum(spec.nq))
+    mine = lpt_assign(map_costs(spec.n, spec.nq), world)[rank]
+    ns, nqs, ks = [int(spec.n[i]) for i in mine], [int(spec.nq[i]) for i in mine], [int(spec.k[i]) for i in mine]
+    phs = [gen.photons(spec.n[i], seed=spec.seeds[i], caustic_frac=0.2) for i in mine]
+    qs = [gen.queries(spec.nq[i], seed=spec.seeds[i] + 500) for i in mine]
+    descs = [dict(k=k, r_max=0.05, filter="cone") for k in ks]
+    poff = np.concatenate([[0], np.cumsum(ns)]).astype(np.uint32)
+    qoff = np.concatenate([[0], np.cumsum(nqs)]).astype(np.uint32)
     N, Q = int(poff[-1]), int(qoff[-1])
-    d_pos = torch.from_numpy(np.concatenate([p.pos for p in phs])).to(dev)
-    d_pw = torch.from_numpy(np.concatenate([p.pow for p in phs])).to(dev)
-    d_qp = torch.from_numpy(np.concatenate([q.pos for q in qs])).to(dev)
-    d_qn = torch.from_numpy(np.concatenate([q.nrm for q in qs])).to(dev)
+    cat = lambda xs: torch.from_numpy(np.concatenate(xs) if xs else np.zeros((0, 4), np.float32)).to(dev)
+    d_pos, d_pw = cat([p.pos for p in phs]), cat([p.pow for p in phs])
+    d_qp, d_qn = cat([q.pos for q in qs]), cat([q.nrm for q in qs])
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def timed(fn):
         for _ in range(args.warmup):
             fn()
+        barrier(world)
         ts = []
         for _ in range(args.steps):
             flush.zero_()
             e0.record(); fn(); e1.record(); e1.synchronize()
             ts.append(e0.elapsed_time(e1))
+        barrier(world)
         return float(np.mean(ts))
 
-    # 64 sequential plain-form calls (storage reserved beforehand)
+    # sequential plain-form calls, one per map (storage reserved beforehand)
     maps = []
     for i, (ph, q) in enumerate(zip(phs, qs)):
-        pm = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=spec.k[i])
+        pm = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=ks[i])
         pm.reserve(ph.n, q.n)
         a, b = int(poff[i]), int(poff[i + 1])
         c, d = int(qoff[i]), int(qoff[i + 1])
@@ -629,33 +687,45 @@ def run_batch(args) -> dict:
     seq_ms = timed(sequential)
     for m in maps:
         m[0].close()
-    batch = PhotonMapBatch()
-    out = batch.outputs(descs, qoff, dev)
-    bt = batch.autotune(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
+    graph_ms = eager_ms = 0.0
+    errors, bt = 0, None
+    if mine:
+        batch = PhotonMapBatch()
+        out = batch.outputs(descs, qoff, dev)
+        bt = batch.autotune(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
 
-    def eager():
-        batch.build(d_pos, d_pw, poff)
-        batch.query(descs, d_qp, d_qn, qoff, out=out)
+        def eager():
+            batch.build(d_pos, d_pw, poff)
+            batch.query(descs, d_qp, d_qn, qoff, out=out)
 
-    eager_ms = timed(eager)
-    batch.capture(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
-    graph_ms = timed(lambda: batch.launch())
-    info = batch.info()
-    batch.close()
-    clocks = None
+        eager_ms = timed(eager)
+        batch.capture(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
+        graph_ms = timed(lambda: batch.launch())
+        errors = batch.info().device_errors
+        batch.close()
+    else:   # a rank without maps still takes every collective step
+        timed(lambda: None)
+        timed(lambda: None)
+    seq_ms, eager_ms, graph_ms, errors = rank_max([seq_ms, eager_ms, graph_ms, float(errors)], dev)
+    close_ranks(world)
+    if rank != 0:
+        return None
     return {
         "metric": "batched photon maps: kNN radiance estimates/s (build + query of all maps per step)",
-        "value": Q / (graph_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"batch: {args.maps} maps, {N:,} photons, {Q:,} queries (log-uniform sizes, "
+        "value": Q_all / (graph_ms / 1000.0), "unit": "queries/s", "higher_is_better": True, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "scaling": "strong", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batch: {args.maps} maps, {N_all:,} photons, {Q_all:,} queries (log-uniform sizes, "
                                f"seed 777), k in {{16,32,64,128}}, R=0.05, cone filter",
-                   "maps": args.maps, "photons": N, "queries": Q, "l2": "flushed between steps (256 MiB write, untimed)"},
+                   "maps": args.maps, "photons": N_all, "queries": Q_all,
+                   "l2": "flushed between steps (256 MiB write, untimed)",
+                   "parallelism": "one GPU" if world == 1 else f"maps by LPT over {world} ranks, no exchange",
+                   "rank0_maps": len(mine), "rank0_photons": N, "rank0_queries": Q},
         "batched_graph_ms": graph_ms, "batched_eager_ms": eager_ms, "sequential_per_map_ms": seq_ms,
-        "sequential_queries_per_s": Q / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q / (eager_ms / 1000.0),
-        "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": info.device_errors,
-        "batch_tuning": {"leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block,
-                         "rounds_per_chunk": bt.rounds_per_chunk, "wide_tree": bt.kbuf_layout == 2,
-                         "chosen_by": "pm_batch_autotune"},
+        "sequential_queries_per_s": Q_all / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q_all / (eager_ms / 1000.0),
+        "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": int(errors),
+        "batch_tuning": None if bt is None else {
+            "leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block, "rounds_per_chunk": bt.rounds_per_chunk,
+            "wide_tree": bt.kbuf_layout == 2, "chosen_by": "pm_batch_autotune (rank 0)"},
     }
 
 
@@ -687,13 +757,19 @@ def main(argv=None) -> int:
         print(json.dumps(run_reference(args, cfg)), flush=True)
         return 0
     if args.config == "batch":
-        print(json.dumps(run_batch(args)), flush=True)
+        res = run_batch(args)
+        if res is not None:
+            print(json.dumps(res), flush=True)
         return 0
     if args.config == "diff":
-        print(json.dumps(run_diff(args, cfg)), flush=True)
+        res = run_diff(args, cfg)
+        if res is not None:
+            print(json.dumps(res), flush=True)
         return 0
     if args.config == "icut":
-        print(json.dumps(run_icut(args, cfg)), flush=True)
+        res = run_icut(args, cfg)
+        if res is not None:
+            print(json.dumps(res), flush=True)
         return 0
     res = run_ours(args, cfg)
     if res is not None:
