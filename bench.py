@@ -3,7 +3,7 @@
 
 One step = one pass of the hot path over one synthetic photon map: build the
 point kd-tree over N photons, then the k-nearest radiance estimate at Q query
-points (Morton sort included).  Default workload ("plain"): 1,048,576 photons
+points (Hilbert-order query sort included).  Default workload ("plain"): 1,048,576 photons
 (80% uniform on the five room walls, 20% in a sigma=0.01 caustic on the
 floor), 2,073,600 uniform wall queries (one per 1920x1080 pixel), k = 100,
 R = 0.05, cone filter, FP32.
@@ -377,7 +377,7 @@ def run_ours(args, cfg) -> dict | None:
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R,
-                   "filter": cfg["filter"], "query_order": "as given" if args.unsorted else "Morton-sorted",
+                   "filter": cfg["filter"], "query_order": "as given" if args.unsorted else "Hilbert-sorted",
                    "l2": "flushed between steps (256 MiB write, untimed)",
                    "parallelism": f"{world} independent replica(s), one per GPU", "tuning": tuning},
         "build_ms": build_ms, "query_ms": float(np.mean(queries)), "query_sort_ms": float(np.mean(sorts)),

@@ -82,7 +82,7 @@ typedef struct pm_query_desc {
     float cone_k;        /* cone filter constant k_c >= 1 (Jensen 2001), used by PM_FILTER_CONE */
     int mode;            /* PM_MODE_EXACT or PM_MODE_ZHOU_COMPAT (PM_MODE_ICUT: pm_gather_for only) */
     uint32_t min_found;  /* estimates from fewer photons are zeroed (reference uses 8) */
-    int order;           /* PM_ORDER_SORTED: Morton-sort the queries first; AS_GIVEN: keep order */
+    int order;           /* PM_ORDER_SORTED: sort the queries along a Hilbert curve first; AS_GIVEN: keep order */
     uint32_t refine_iters; /* ZHOU_COMPAT only: histogram refinement rounds (reference default 2) */
 } pm_query_desc;
 
@@ -141,7 +141,7 @@ typedef struct pm_tuning {
  * sample of at most max_sample queries (0 = all), applies the fastest to the
  * map, writes it to *best and leaves the map built with it.  Synchronous.
  * A sample is sparser than the full set, which weakens the reuse of the
- * previous query's radius bound between Morton neighbours: tune on all
+ * previous query's radius bound between Hilbert neighbours: tune on all
  * queries (or a dense spatial subset) when the setting matters. */
 PM_API pm_status pm_autotune(pm_map* map, const float* d_pos4, const float* d_pow4, uint32_t n, int format,
                              const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
@@ -190,7 +190,7 @@ PM_API pm_status pm_query(pm_map* map, const pm_query_desc* desc, const float* d
  * in host memory).  Copies the photons in and builds while the queries copy
  * in on an internal stream; with chunks > 1 (at most 16; 0 = 1) the queries
  * are copied, answered and copied back in that many pieces so that copies
- * overlap queries -- at the cost of query coherence: each piece is Morton
+ * overlap queries -- at the cost of query coherence: each piece is Hilbert
  * sorted on its own, which measured slower for 2M queries than one piece.
  * Results are identical, bit for bit, to pm_build + pm_query on the same data
  * (exact mode).  Host arrays should be pinned (cudaHostAlloc /
@@ -219,7 +219,7 @@ PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, con
  * bit, as pm_query on a built map.
  *   - The map must already be built.  The caller passes every input and
  *     output buffer, as for pm_query.
- *   - The query scratch (Morton sort keys, the list of queries re-evaluated
+ *   - The query scratch (Hilbert sort keys, the list of queries re-evaluated
  *     with FP64 distances, the work counters) lives in one fixed array of
  *     about 7.2 MiB inside this library.  Every GPU that loads
  *     the library holds it until the process exits.
@@ -390,7 +390,7 @@ typedef struct pm_timings {
     float build_ms;          /* whole pm_build */
     float build_sort_ms;     /* Morton codes + radix sort inside pm_build */
     float query_ms;          /* whole pm_query */
-    float query_sort_ms;     /* query Morton sort inside pm_query (0 when AS_GIVEN) */
+    float query_sort_ms;     /* query Hilbert sort inside pm_query (0 when AS_GIVEN) */
     float query_kernel_ms;   /* the kNN kernel alone */
     uint32_t build_launches; /* kernels launched by the last pm_build */
     uint32_t query_launches; /* kernels launched by the last pm_query */

@@ -266,9 +266,9 @@ QueryParams params_of(const pm_query_desc* d) {
     return p;
 }
 
-// Morton order of the queries (returns the permutation or nullptr).
+// Hilbert order of the queries (returns the permutation or nullptr).
 const uint32_t* sort_queries(pm_map* m, const float4* qpos, uint32_t nq, cudaStream_t st, int* launches) {
-    *launches += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint32_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
+    *launches += query_order_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint32_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
     uint32_t* keys[2] = {P<uint32_t>(m->qkeys0), P<uint32_t>(m->qkeys1)};
     uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
     const int cur = radix_sort_pairs32(keys, vals, nq, kQueryKeyBits, P<uint32_t>(m->qscratch), st, launches);
@@ -1123,7 +1123,7 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
                              reinterpret_cast<uint32_t*>(base + kNoallocKeys1)};
         uint32_t* vals[2] = {reinterpret_cast<uint32_t*>(base + kNoallocVals0),
                              reinterpret_cast<uint32_t*>(base + kNoallocVals1)};
-        nl += query_morton_keys(qpos, nq, P<MapHeader>(m->hdr), keys[0], vals[0], st);
+        nl += query_order_keys(qpos, nq, P<MapHeader>(m->hdr), keys[0], vals[0], st);
         const int cur = radix_sort_pairs32(keys, vals, nq, kQueryKeyBits, reinterpret_cast<uint32_t*>(base + kNoallocSort),
                                            st, &nl);
         order = vals[cur];
@@ -1269,8 +1269,8 @@ pm_status batch_query_device(pm_batch* b, uint32_t kmax, const float* d_qpos4, c
                               P<uint64_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
     uint64_t* keys[2] = {P<uint64_t>(m->qkeys0), P<uint64_t>(m->qkeys1)};
     uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
-    const int cur = nq > 1 ? radix_sort_pairs(keys, vals, nq, 48 + map_id_bits(b->num_maps), P<uint32_t>(m->qscratch),
-                                              st, &nl)
+    const int cur = nq > 1 ? radix_sort_pairs(keys, vals, nq, kBatchQueryMapShift + map_id_bits(b->num_maps),
+                                              P<uint32_t>(m->qscratch), st, &nl)
                            : 0;
     QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
     QueryTuning t = tuning_of(m);

@@ -7,9 +7,10 @@
 //   (map id << 48) | 48-bit Morton code in the map's own cubic cell,
 // so one radix tree holds every map: the map id bits split first, and the
 // node whose range is exactly a map's photons roots that map's subtree
-// (k_batch_roots).  The query sorts all queries by the same kind of key and
-// runs one persistent launch over them (k_knn_group<32, *, true>), each query
-// reading its map's root slot and parameters.
+// (k_batch_roots).  The query sorts all queries by (map id << 30) | 30-bit
+// Hilbert index in the map's cell and runs one persistent launch over them
+// (k_knn_group<32, *, true>), each query reading its map's root slot and
+// parameters.
 #include "pm_internal.h"
 
 namespace pm {
@@ -113,7 +114,22 @@ __global__ void k_batch_geom(const uint32_t* __restrict__ acc, uint32_t m, Batch
     if (a[7]) atomicOr(&hdr->errors, kErrNonFinite);
 }
 
-// Photon (or query) keys: map id in bits 48..63, Morton code in the map's cell.
+// Query keys: map id above bit 30, Hilbert index in the map's cell (the
+// processing order only; 30 + map-id bits sort in fewer passes than the
+// photons' 48-bit codes).
+__global__ void k_batch_query_keys(const float4* __restrict__ pts, const uint32_t* __restrict__ off, uint32_t m,
+                                   uint32_t n, const BatchGeom* __restrict__ geom, uint64_t* __restrict__ keys,
+                                   uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t map = map_of(off, m, i);
+    const BatchGeom& g = geom[map];
+    const float4 p = pts[i];
+    keys[i] = ((uint64_t)map << kBatchQueryMapShift) | hilbert30(p.x, p.y, p.z, g.lo, g.mscale);
+    vals[i] = i;
+}
+
+// Photon keys: map id in bits 48..63, Morton code in the map's cell.
 __global__ void k_batch_keys(const float4* __restrict__ pts, const uint32_t* __restrict__ off, uint32_t m, uint32_t n,
                              const BatchGeom* __restrict__ geom, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -227,7 +243,7 @@ int batch_bounds_and_keys(const float4* pos, const float4* pw, const uint32_t* p
 int batch_query_keys(const float4* qpos, const uint32_t* q_off, uint32_t m, uint32_t nq, const BatchGeom* geom,
                      uint64_t* keys, uint32_t* vals, cudaStream_t st) {
     if (!nq) return 0;
-    k_batch_keys<<<(nq + 255) / 256, 256, 0, st>>>(qpos, q_off, m, nq, geom, keys, vals);
+    k_batch_query_keys<<<(nq + 255) / 256, 256, 0, st>>>(qpos, q_off, m, nq, geom, keys, vals);
     return 1;
 }
 

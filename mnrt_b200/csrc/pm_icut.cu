@@ -427,7 +427,7 @@ __global__ void k_icut_ibox_climb(const Node* __restrict__ nodes, uint32_t m, co
     }
 }
 
-// Thread per query (Morton order when `order` is given): depth-first over the
+// Thread per query (Hilbert order when `order` is given): depth-first over the
 // slots whose box lies within R of q, stopping at cut slots and leaves.
 __global__ void __launch_bounds__(128) k_icut_interp(const Node* __restrict__ nodes, const float4* __restrict__ ibox,
                                                      const float4* __restrict__ center,

@@ -108,9 +108,10 @@ struct QueryOutputs {
     uint32_t* count;     // optional
 };
 
-int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
+int query_order_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
                        cudaStream_t st);
-constexpr int kQueryKeyBits = 30;   // bits of the query Morton keys (sorted as uint32)
+constexpr int kQueryKeyBits = 30;         // bits of the query Hilbert keys (sorted as uint32)
+constexpr int kBatchQueryMapShift = 30;   // batch query keys: (map id << 30) | 30-bit Hilbert index in the map's cell
 struct QueryTuning {
     int layout;             // 0: lane per query with a shared-memory heap; 1: group buffers
     int queries_per_warp;   // group layout: 1, 2, 4 or 8 (32, 16, 8 or 4 lanes per query)

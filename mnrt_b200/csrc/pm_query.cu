@@ -7,7 +7,7 @@
 // refinements, gather) with one thread and a local-memory stack per query,
 // this kernel finds the exact k nearest photons in one pass:
 //
-//   * queries are processed in Morton order; one warp owns 32 consecutive
+//   * queries are processed in Hilbert order; one warp owns 32 consecutive
 //     queries (one per lane) and traverses the tree jointly: a child is
 //     visited when any lane's box lower bound passes its threshold, so
 //     control flow is warp-uniform and a leaf's photons are fetched once per
@@ -1044,7 +1044,7 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
             uint32_t map = 0;
             const uint32_t slot_main = (kFix && inrange) ? a0.fix_in[slot_q] : slot_q;   // slot of the sorted launch
             if (kBatch && inrange) {
-                map = (uint32_t)(a0.qkeys[slot_main] >> 48);
+                map = (uint32_t)(a0.qkeys[slot_main] >> kBatchQueryMapShift);
                 const BatchQuery bq = a0.bq[map];
                 a.k = bq.k; a.r2max = bq.r2max; a.rmax = bq.rmax; a.filter = bq.filter; a.cone_k = bq.cone_k;
                 a.min_found = bq.min_found; a.nbr_off = bq.nbr_off; a.q_off = bq.q_off; a.ph_off = bq.ph_off;
@@ -1286,25 +1286,25 @@ __global__ void __launch_bounds__(kBruteThreads) k_knn_brute(KnnArgs a, uint32_t
     if (valid) finish_query(a, heap, kBruteThreads, hn, q, qx, qy, qz, nx, ny, nz);
 }
 
-__global__ void k_query_morton(const float4* __restrict__ qpos, uint32_t nq, const MapHeader* __restrict__ hdr,
-                               uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+__global__ void k_query_hilbert(const float4* __restrict__ qpos, uint32_t nq, const MapHeader* __restrict__ hdr,
+                                uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nq) return;
     const float ext = fmaxf(fmaxf(__fsub_rn(hdr->hi[0], hdr->lo[0]), __fsub_rn(hdr->hi[1], hdr->lo[1])),
                             __fsub_rn(hdr->hi[2], hdr->lo[2]));
     const float scale = (ext > 0.0f && isfinite(ext)) ? __fdiv_rn(65536.0f, ext) : 0.0f;
     const float4 p = qpos[i];
-    keys[i] = morton30(p.x, p.y, p.z, hdr->lo, scale);
+    keys[i] = hilbert30(p.x, p.y, p.z, hdr->lo, scale);
     vals[i] = i;
 }
 
 // 30-bit query keys: 4 radix passes instead of the tree's 6 (a cell is 1/1024
 // of the map's extent per axis, finer than the query spacing of the measured
 // workloads).
-int query_morton_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
-                      cudaStream_t st) {
+int query_order_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
+                     cudaStream_t st) {
     if (!nq) return 0;
-    k_query_morton<<<(nq + 255) / 256, 256, 0, st>>>(qpos, nq, hdr, keys, vals);
+    k_query_hilbert<<<(nq + 255) / 256, 256, 0, st>>>(qpos, nq, hdr, keys, vals);
     return 1;
 }
 
