@@ -298,7 +298,7 @@ def run_ours(args, cfg) -> dict | None:
     pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
     tuning = "defaults"
     if args.leaf or args.wpb or args.rounds or args.qpw or args.layout >= 0:
-        pm.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 32,
+        pm.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4, rounds_per_chunk=args.rounds or 8,
                       queries_per_warp=args.qpw or 1, kbuf_layout=args.layout if args.layout >= 0 else 2)
         tuning = "set by flags"
     elif not args.no_autotune:   # untimed: picks the kernel setting on a query sample

@@ -120,7 +120,8 @@ enum { PM_KBUF_HEAP = 0,   /* one lane per query, max-heap in shared memory */
        PM_KBUF_WIDE = 2    /* one query per warp over the 32-wide tree, candidate buffer + exact selection */ };
 
 /* Tuning knobs (chosen by the autotuner): photons per leaf (1..32), warps per
- * query block (1..8), query rounds per work chunk (1..4096), queries per warp
+ * query block (1..8), rounds in the smallest work chunk (1..4096; warps take
+ * chunks by guided self-scheduling: long chunks first, this size last), queries per warp
  * (1, 2, 4, 8; group layout) and the k-buffer layout (PM_KBUF_*). */
 PM_API pm_status pm_set_tuning(pm_map* map, uint32_t leaf_size, int warps_per_block, int rounds_per_chunk,
                                int queries_per_warp, int kbuf_layout);

@@ -51,7 +51,7 @@ class PhotonMapBatch:
         if st != L.PM_OK:
             raise L.PMError(st, self._lib.pm_batch_last_error(self._h).decode())
 
-    def set_tuning(self, leaf_size: int = 32, warps_per_block: int = 4, rounds_per_chunk: int = 32,
+    def set_tuning(self, leaf_size: int = 32, warps_per_block: int = 4, rounds_per_chunk: int = 8,
                    wide: bool = True) -> None:
         """wide: traverse the 32-wide tree (else the binary one)."""
         self._check(self._lib.pm_batch_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk, int(wide)))

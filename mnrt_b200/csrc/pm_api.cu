@@ -32,7 +32,7 @@ struct pm_map {
     // workload (k = 100); pm_set_tuning / the autotuner override them
     uint32_t leaf_size = 32;
     int warps_per_block = 4;
-    int rounds_per_chunk = 32;
+    int rounds_per_chunk = 8;    // the smallest work chunk of the guided schedule, in rounds
     int queries_per_warp = 1;
     int kbuf_layout = PM_KBUF_WIDE;
     pm_alloc_fn alloc = nullptr;

@@ -351,6 +351,37 @@ __device__ __forceinline__ void load_root(const ChildSlot* slot, float* lo, floa
     hi[1] = b.x; hi[2] = b.y; ref = __float_as_uint(b.z); cnt = __float_as_uint(b.w);
 }
 
+// Guided self-scheduling (Polychronopoulos & Kuck, 1987) of the sorted
+// queries, in rounds (a round = the queries one warp takes at once): warps
+// take chunk numbers from one atomic counter; group g holds P chunks (P = the
+// grid's warps) of s_g = max(rmin, rem_g / 2P + 1) rounds each, rem_g the
+// rounds left before the group.  Early chunks are long, so fewer queries
+// start without the radius bound of their predecessor (every chunk's first
+// query does); the last chunks are rmin rounds, so the launch's tail stays
+// short.  Against fixed 32-round chunks: 65k -> 31k chunks on 2.07M queries
+// and 7.62 -> 7.29 ms for the query kernel.  rmax caps a chunk where query
+// costs differ widely (a batch of maps with different k and sizes: uncapped,
+// one chunk of costly queries outlasts the rest of the launch).  Returns
+// false past the end.
+__device__ __forceinline__ bool guided_chunk(uint32_t c, uint32_t total, uint32_t P, uint32_t rmin, uint32_t rmax,
+                                             uint32_t& begin, uint32_t& len) {
+    uint32_t base = 0;
+    for (;;) {
+        if (base >= total) return false;
+        const uint32_t s = max(rmin, min(rmax, (total - base) / (2u * P) + 1u));
+        if (c < P) {
+            const uint64_t b = (uint64_t)base + (uint64_t)c * s;
+            if (b >= total) return false;
+            begin = (uint32_t)b;
+            len = min(s, total - (uint32_t)b);
+            return true;
+        }
+        c -= P;
+        const uint64_t nb = (uint64_t)base + (uint64_t)P * s;
+        base = nb >= total ? total : (uint32_t)nb;
+    }
+}
+
 // One warp = 32 queries (one per lane) traversing together.
 __global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -362,19 +393,20 @@ __global__ void __launch_bounds__(256) k_knn_tree(KnnArgs a) {
     uint64_t* heap = reinterpret_cast<uint64_t*>(wbase) + lane;
     uint32_t* stack = reinterpret_cast<uint32_t*>(wbase + (size_t)32 * k * sizeof(uint64_t));
     const float r2max = a.r2max;
-    const uint32_t chunk_q = a.rounds_per_chunk * 32;
-    const uint32_t nchunks = (a.nq + chunk_q - 1) / chunk_q;
+    const uint32_t total_rounds = (a.nq + 31u) / 32u;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
 
     for (;;) {
         uint32_t chunk = 0;
         if (lane == 0) chunk = atomicAdd(a.work_counter, 1u);
         chunk = __shfl_sync(kFull, chunk, 0);
-        if (chunk >= nchunks) break;
+        uint32_t rbegin = 0, rlen = 0;
+        if (!guided_chunk(chunk, total_rounds, nwarps, a.rounds_per_chunk, 0xffffffffu, rbegin, rlen)) break;
         // previous round's result of this lane (for the radius bound)
         float pqx = 0.f, pqy = 0.f, pqz = 0.f, pr = 0.f;
         bool pvalid = false;
-        for (uint32_t round = 0; round < a.rounds_per_chunk; ++round) {
-            const uint32_t slot_q = chunk * chunk_q + round * 32 + lane;
+        for (uint32_t round = 0; round < rlen; ++round) {
+            const uint32_t slot_q = (rbegin + round) * 32 + lane;
             const bool inrange = slot_q < a.nq;
             if (!__any_sync(kFull, inrange)) break;
             uint32_t qo = 0;
@@ -1023,20 +1055,23 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
     uint64_t* buf = reinterpret_cast<uint64_t*>(wb) + (size_t)g * C;
     uint32_t* hist = reinterpret_cast<uint32_t*>(wb + (size_t)QW * C * sizeof(uint64_t)) + g * 256;
     uint32_t* stack = reinterpret_cast<uint32_t*>(wb + (size_t)QW * (C * sizeof(uint64_t) + 256 * sizeof(uint32_t)));
-    const uint32_t chunk_q = a0.rounds_per_chunk * QW;
     const uint32_t nq = kFix ? *a0.nq_dev : a0.nq;
-    const uint32_t nchunks = (nq + chunk_q - 1) / chunk_q;
+    const uint32_t total_rounds = (nq + QW - 1) / QW;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
 
     for (;;) {
         uint32_t chunk = 0;
         if (lane == 0) chunk = atomicAdd(a0.work_counter, 1u);
         chunk = __shfl_sync(kFull, chunk, 0);
-        if (chunk >= nchunks) break;
+        uint32_t rbegin = 0, rlen = 0;
+        if (!guided_chunk(chunk, total_rounds, nwarps, a0.rounds_per_chunk,
+                          kBatch ? 4u * a0.rounds_per_chunk : 0xffffffffu, rbegin, rlen))
+            break;
         float pqx = 0.f, pqy = 0.f, pqz = 0.f, pr = 0.f;
         bool pvalid = false;
         uint32_t pmap = 0;   // batch: map of the previous round's query
-        for (uint32_t round = 0; round < a0.rounds_per_chunk; ++round) {
-            const uint32_t slot_q = chunk * chunk_q + round * QW + g;
+        for (uint32_t round = 0; round < rlen; ++round) {
+            const uint32_t slot_q = (rbegin + round) * QW + g;
             const bool inrange = slot_q < nq;
             if (!__any_sync(kFull, inrange)) break;
             // per-query arguments: the launch's, or (batch) those of the query's map

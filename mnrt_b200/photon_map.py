@@ -106,7 +106,7 @@ class PhotonMap:
     def get_photon_count(self) -> int:
         return self.num_photons
 
-    def set_tuning(self, leaf_size: int = 32, warps_per_block: int = 4, rounds_per_chunk: int = 32,
+    def set_tuning(self, leaf_size: int = 32, warps_per_block: int = 4, rounds_per_chunk: int = 8,
                    queries_per_warp: int = 1, kbuf_layout: int = L.PM_KBUF_WIDE) -> None:
         L.check(self._lib.pm_set_tuning(self._h, leaf_size, warps_per_block, rounds_per_chunk, queries_per_warp,
                                         kbuf_layout), self._h)
