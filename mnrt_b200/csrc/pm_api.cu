@@ -1054,7 +1054,7 @@ pm_status pm_export_tree(pm_map* m, uint32_t* host_nodes, uint32_t max_nodes, fl
 namespace {
 
 constexpr uint32_t kNoallocMaxQ = PM_NOALLOC_MAX_QUERIES;
-constexpr size_t kNoallocSortWords = 33024;   // >= sort_scratch_words(kNoallocMaxQ) = 32778, checked at set-up
+constexpr size_t kNoallocSortWords = 33024;   // >= sort_scratch_words(kNoallocMaxQ) = 33024, checked at set-up
 constexpr size_t kNoallocAlign = 256;
 constexpr size_t noalloc_round(size_t b) { return (b + kNoallocAlign - 1) / kNoallocAlign * kNoallocAlign; }
 constexpr size_t kNoallocKeys0 = 0;

@@ -3,11 +3,13 @@
 // radix sort the reference builds its tree with (MNCudaPrimitives.cpp:160-227).
 //
 // Radix sort: 8-bit digits, reduce-then-scan per pass (no inter-block waits).
-//   1. k_digit_hist: every tile counts its digits (one histogram per warp), in the
-//      digit-major layout hist[d * tiles + t], so one exclusive scan over the
-//      whole array yields every tile's global offset per digit;
-//   2. exclusive scan of hist;
-//   3. k_digit_scatter: every tile ranks its keys stably, orders them by
+//   1. k_digit_hist: every tile counts its digits (one histogram per warp), in
+//      the digit-major layout hist[d * tiles + t];
+//   2. k_digit_rowscan: block d scans row d in place (the tile's offset among
+//      the keys of digit d) and writes the row total (above 4M keys: one
+//      exclusive scan of the whole array, which yields global offsets);
+//   3. k_digit_scatter: every tile adds the exclusive scan of the 256 row
+//      totals (the digit's start), ranks its keys stably, orders them by
 //      digit in shared memory and writes each digit's run contiguously.
 // Stability across passes makes the result sorted by the full key, with the
 // input order breaking ties.
@@ -158,24 +160,57 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_hist(const Key* __restri
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = c;
 }
 
+// Block d: exclusive scan of hist[d * ntiles, (d + 1) * ntiles) in place,
+// the row total to digit_total[d].
+__global__ void __launch_bounds__(kScanThreads) k_digit_rowscan(uint32_t* __restrict__ hist, uint32_t ntiles,
+                                                                 uint32_t* __restrict__ digit_total) {
+    __shared__ uint32_t s_warp[32];
+    uint32_t* row = hist + (size_t)blockIdx.x * ntiles;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < ntiles; base += kScanTile) {
+        const uint32_t first = base + threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            v[i] = first + i < ntiles ? row[first + i] : 0u;
+            sum += v[i];
+        }
+        uint32_t total;
+        uint32_t run = carry + block_exclusive_scan(sum, s_warp, total);
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            if (first + i < ntiles) row[first + i] = run;
+            run += v[i];
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
+}
+
 template <class Key>
 __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __restrict__ keys_in,
                                                                   const uint32_t* __restrict__ vals_in, uint32_t n,
                                                                   int shift, uint32_t ntiles,
                                                                   const uint32_t* __restrict__ offsets,
+                                                                  const uint32_t* __restrict__ digit_total,
                                                                   Key* __restrict__ keys_out,
                                                                   uint32_t* __restrict__ vals_out) {
     __shared__ uint32_t s_cnt[kSortWarps][256];   // per-warp digit counts, then per-warp starts within the digit
     __shared__ uint32_t s_start[256];             // tile-local start of each digit
     __shared__ uint32_t s_global[256];            // global position of the tile's first key of each digit
     __shared__ uint32_t s_warpsum[32];
+    __shared__ uint32_t s_warptot[32];
     __shared__ Key s_key[kSortTile];
     __shared__ uint32_t s_val[kSortTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) s_cnt[w][threadIdx.x] = 0;
-    s_global[threadIdx.x] = offsets[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+    // thread d: this tile's offset among the keys of digit d, and digit d's
+    // row total (null: offsets are already global); used after the ranking
+    const uint32_t toff = offsets[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+    const uint32_t tot = digit_total ? digit_total[threadIdx.x] : 0u;
     __syncthreads();
     const uint64_t tile0 = (uint64_t)blockIdx.x * kSortTile;
     const uint64_t base = tile0 + (uint64_t)warp * (32 * kSortRounds);
@@ -209,17 +244,18 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
             s_cnt[w][threadIdx.x] = run;
             run += c;
         }
-        uint32_t x = run;   // block exclusive scan of the digit totals
+        uint32_t x = run, y = tot;   // block exclusive scans: the tile's digit counts, the row totals
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const uint32_t xo = __shfl_up_sync(0xffffffffu, x, o), yo = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) { x += xo; y += yo; }
         }
-        if (lane == 31) s_warpsum[warp] = x;
+        if (lane == 31) { s_warpsum[warp] = x; s_warptot[warp] = y; }
         __syncthreads();
-        uint32_t wp = 0;
-        for (int w = 0; w < warp; ++w) wp += s_warpsum[w];
+        uint32_t wp = 0, wt = 0;
+        for (int w = 0; w < warp; ++w) { wp += s_warpsum[w]; wt += s_warptot[w]; }
         s_start[threadIdx.x] = wp + x - run;
+        s_global[threadIdx.x] = wt + y - tot + toff;
     }
     __syncthreads();
 #pragma unroll
@@ -243,10 +279,17 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
     }
 }
 
+// Up to this many tiles (4M keys) a pass scans the digit rows with one
+// launch of 256 blocks; above it a block walks its long row serially (the
+// adjoint's 67M-pair sort measured 0.27 ms slower with row scans), and the
+// generic scan of the whole digit-major array (three launches, every SM
+// busy) takes over.
+constexpr uint32_t kRowScanMaxTiles = 2048;
+
 size_t sort_scratch_words(uint32_t n) {
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
-    const size_t hist = (size_t)tiles * 256;
-    return hist + scan_scratch_words((uint32_t)hist) + 1;
+    const size_t hist = (size_t)tiles * 256;   // per-tile digit counts
+    return hist + (tiles <= kRowScanMaxTiles ? 256 : scan_scratch_words((uint32_t)hist) + 1);
 }
 
 // Sorts by bits [0, key_bits) of the keys.  Returns which buffer holds the
@@ -259,13 +302,19 @@ static int radix_sort_impl(Key* keys[2], uint32_t* vals[2], uint32_t n, int key_
     int nl = 0;
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     uint32_t* hist = scratch;
-    uint32_t* scan_tmp = scratch + (size_t)tiles * 256;
+    uint32_t* tail = scratch + (size_t)tiles * 256;   // row totals, or the whole-array scan's scratch
+    const bool rows = tiles <= kRowScanMaxTiles;
     int cur = 0;
     for (int shift = 0; shift < key_bits; shift += 8) {
         k_digit_hist<Key><<<tiles, kSortThreads, 0, st>>>(keys[cur], n, shift, tiles, hist);
-        nl += 2 + exclusive_scan(hist, hist, tiles * 256u, scan_tmp, nullptr, st);
+        if (rows) {
+            k_digit_rowscan<<<256, kScanThreads, 0, st>>>(hist, tiles, tail);
+            nl += 3;
+        } else {
+            nl += 2 + exclusive_scan(hist, hist, tiles * 256u, tail, nullptr, st);
+        }
         k_digit_scatter<Key><<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
-                                                              keys[cur ^ 1], vals[cur ^ 1]);
+                                                              rows ? tail : nullptr, keys[cur ^ 1], vals[cur ^ 1]);
         cur ^= 1;
     }
     if (launches) *launches += nl;
