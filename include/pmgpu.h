@@ -195,7 +195,8 @@ PM_API pm_status pm_query(pm_map* map, const pm_query_desc* desc, const float* d
  * sorted on its own, which measured slower for 2M queries than one piece.
  * Results are identical, bit for bit, to pm_build + pm_query on the same data
  * (exact mode).  Host arrays should be pinned (cudaHostAlloc /
- * cudaHostRegister) for the copies to overlap.  Asynchronous on `stream`:
+ * cudaHostRegister) for the copies to overlap; a pinned h_rad4 is written in
+ * place by the query kernel, with no download after it.  Asynchronous on `stream`:
  * h_rad4 is complete when the stream's work up to this call is.  Not
  * allowed during stream capture. */
 PM_API pm_status pm_build_query_host(pm_map* map, const float* h_pos4, const float* h_pow4, uint32_t n, int format,

@@ -475,6 +475,17 @@ pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, c
     return check_cuda(m, "pm_query");
 }
 
+// Device address of a page-locked host array (cudaHostAlloc /
+// cudaHostRegister, mapped under unified addressing), or nullptr.
+static void* host_mapped(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+}
+
 pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow4, uint32_t n, int format,
                               const pm_query_desc* desc, const float* h_qpos4, const float* h_qnrm4, uint32_t nq,
                               float* h_rad4, uint32_t chunks, void* stream) {
@@ -510,6 +521,15 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
     float4* dqp = P<float4>(m->hs_qpos);
     float4* dqn = P<float4>(m->hs_qnrm);
     float4* drad = P<float4>(m->hs_rad);
+    // A page-locked radiance array is written in place by the query kernel
+    // (each estimate once, 16 bytes over PCIe while the search runs), which
+    // takes the download off the critical path: 9.83 -> 9.27 ms end to end on
+    // the plain workload.  A pageable one goes through a device copy.  The
+    // normals are always copied in: read in place as well, they queue behind
+    // the posted radiance writes on the link (12.76 ms with both in place;
+    // 9.57 ms with the normals alone).
+    const bool rad_in_place = host_mapped(h_rad4) != nullptr;
+    if (rad_in_place) drad = reinterpret_cast<float4*>(host_mapped(h_rad4));
     cudaEvent_t ev_photons = m->hs_ev[0], ev_done = m->hs_ev[1];
     // photons in, then the queries in pieces behind them on the copy stream
     if (n) {
@@ -546,7 +566,7 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
         }
         cudaEventRecord(m->hs_ev[3 + 2 * c], st);
         cudaStreamWaitEvent(m->hs_out, m->hs_ev[3 + 2 * c], 0);
-        if (len)
+        if (len && !rad_in_place)
             cudaMemcpyAsync(reinterpret_cast<float4*>(h_rad4) + off, drad + off, len * sizeof(float4),
                             cudaMemcpyDeviceToHost, m->hs_out);
     }

@@ -302,17 +302,21 @@ def test_radix_sort_and_scan_through_tree_order(cuda, n):
     assert (cnts <= 16).all()
 
 
-@pytest.mark.parametrize("chunks,pinned", [(1, True), (3, True), (4, False), (16, True)])
+@pytest.mark.parametrize("chunks,pinned", [(1, True), (3, True), (1, False), (4, False), (16, True)])
 def test_build_query_host_matches_device_calls(cuda, chunks, pinned):
     """pm_build_query_host (host buffers, chunked and overlapped) gives the
-    bits of pm_build + pm_query on device buffers."""
+    bits of pm_build + pm_query on device buffers: a page-locked radiance
+    array written in place by the query kernel, a pageable one through a
+    device copy."""
     from mnrt_b200.photon_map import PhotonMap
     ph = gen.photons(80000, seed=71, caustic_frac=0.2)
     q = gen.queries(30001, seed=72)
     pm = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=64)
     h = lambda a: (torch.from_numpy(np.ascontiguousarray(a)).pin_memory() if pinned
                    else torch.from_numpy(np.ascontiguousarray(a)))
-    got = pm.build_query_host(h(ph.pos), h(ph.pow), h(q.pos), h(q.nrm), chunks=chunks, filter="cone", min_found=8)
+    out = None if pinned else torch.empty((q.n, 4), dtype=torch.float32)   # None: a page-locked output
+    got = pm.build_query_host(h(ph.pos), h(ph.pow), h(q.pos), h(q.nrm), out=out, chunks=chunks, filter="cone",
+                              min_found=8)
     torch.cuda.synchronize()
     pm2 = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=64)
     pm2.build(torch.from_numpy(ph.pos).to(cuda), torch.from_numpy(ph.pow).to(cuda))
