@@ -660,7 +660,8 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     const bool recompute = d_nbr == nullptr;
     s = ensure_bwd_capacity(m, chunk, k, recompute, nchunks > 1, st);
     if (s != PM_OK) return s;
-    if (recompute) {
+    const bool sorted = desc->order == PM_ORDER_SORTED;
+    if (recompute || sorted) {
         s = ensure_query_capacity(m, chunk, st);
         if (s != PM_OK) return s;
     }
@@ -674,7 +675,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     a.min_found = desc->min_found;
     a.qrec = P<double4>(m->qrec); a.qr2 = P<double>(m->qr2); a.qcnt = P<uint32_t>(m->qcnt);
     a.keys = nullptr; a.vals = nullptr;
-    a.nbr = nullptr; a.count_in = nullptr;
+    a.nbr = nullptr; a.count_in = nullptr; a.order = nullptr;
     BwdBuffers b;
     b.keys[0] = P<uint32_t>(m->bkeys0); b.keys[1] = P<uint32_t>(m->bkeys1);
     b.vals[0] = P<uint32_t>(m->bvals0); b.vals[1] = P<uint32_t>(m->bvals1);
@@ -685,15 +686,16 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     for (uint32_t c = 0; c < nchunks; ++c) {
         const uint32_t q0 = c * chunk;
         const uint32_t nqc = nq ? ((nq - q0) < chunk ? (nq - q0) : chunk) : 0;
+        // the chunk's queries in Hilbert order: the recomputed forward and the
+        // adjoint's per-query pass walk them in it
+        a.order = (sorted && nqc > 0) ? sort_queries(m, a.qpos + q0, nqc, st, &nl) : nullptr;
         if (recompute) {
             if (nqc > 0) {
-                const float4* qp = a.qpos + q0;
-                const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, qp, nqc, st, &nl) : nullptr;
                 QueryOutputs out{P<float4>(m->rrad), P<uint32_t>(m->rnbr), P<float>(m->rr2), P<uint32_t>(m->rcnt)};
                 QueryTuning t = tuning_of(m);
                 t.stats = nullptr;
-                nl += query_knn(view_of(m), params_of(desc), qp, a.qnrm + q0, order, nqc, out, P<uint32_t>(m->counter),
-                                P<uint32_t>(m->fixq), t, st);
+                nl += query_knn(view_of(m), params_of(desc), a.qpos + q0, a.qnrm + q0, a.order, nqc, out,
+                                P<uint32_t>(m->counter), P<uint32_t>(m->fixq), t, st);
             }
             a.nbr = P<uint32_t>(m->rnbr);
             a.count_in = P<uint32_t>(m->rcnt);

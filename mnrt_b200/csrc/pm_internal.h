@@ -211,6 +211,7 @@ struct BwdArgs {
     uint32_t* qcnt;           // per chunk query: neighbours carrying gradient
     uint32_t* keys;           // pair keys / values (set by backward_chunk)
     uint32_t* vals;
+    const uint32_t* order;    // the chunk's queries in Hilbert order (chunk-local ids), or nullptr
 };
 struct BwdBuffers {
     uint32_t* keys[2];
