@@ -355,3 +355,4 @@ def test_channel_imbalanced_flux_small_k(cuda, oracle_mod, k, filt):
     res = run(ph, q, cuda, k, 1.5, filt, leaf=32, tuning=dict(kbuf_layout=2))
     assert res["info"].device_errors == 0
     check_against_oracle(oracle_mod, ph, q, res, k, 1.5, filt)
+

@@ -143,3 +143,25 @@ def test_random_compat(cuda, oracle_mod, seed):
     assert (np.abs(got[:, :3] - o_rad) / np.maximum(np.abs(o_rad), floor)).max() <= 1e-5
     assert pm.info().device_errors == 0
     pm.close()
+
+
+@pytest.mark.parametrize("nq", [1, 97, 20000])
+def test_chunk_schedules_give_identical_bits(cuda, nq):
+    """Warps take query chunks by guided self-scheduling (long chunks first,
+    rounds_per_chunk rounds last).  The schedule only decides which warp
+    answers which query and which radius bound a query starts from, so every
+    layout, warp count and chunk size must give the same bits."""
+    ph = gen.photons(50000, seed=3100, caustic_frac=0.2)
+    q = gen.queries(nq, seed=3101, cluster_frac=0.5)
+    ref = None
+    for layout, qpw, wpb, rounds in [(2, 1, 4, 8), (2, 1, 1, 1), (2, 1, 8, 4096), (1, 4, 2, 3), (1, 1, 4, 4096),
+                                     (0, 1, 4, 1), (0, 1, 2, 4096)]:
+        res = run(ph, q, cuda, 48, 0.08, "cone", leaf=24,
+                  tuning=dict(kbuf_layout=layout, queries_per_warp=qpw, warps_per_block=wpb, rounds_per_chunk=rounds))
+        assert res["info"].device_errors == 0
+        got = {key: res[key] for key in ("rad", "r2", "count", "nbr")}
+        if ref is None:
+            ref = got
+            continue
+        for key in ref:
+            assert np.array_equal(got[key], ref[key]), (layout, qpw, wpb, rounds, key)
