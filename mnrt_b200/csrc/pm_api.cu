@@ -68,7 +68,7 @@ struct pm_map {
     // pm_build_query_host: device copies of host inputs, two copy streams, events
     DevBuf hs_pos, hs_pow, hs_qpos, hs_qnrm, hs_rad;
     cudaStream_t hs_in = nullptr, hs_out = nullptr;
-    cudaEvent_t hs_ev[36] = {};   // photons in, done, and two per chunk
+    cudaEvent_t hs_ev[50] = {};   // photons in, done, and three per chunk
     uint64_t icut_prep_gen = ~0ull, icut_gen = ~0ull;
     uint64_t build_gen = 0, compat_gen = ~0ull;
     uint32_t compat_k = 0, compat_iters = 0;
@@ -447,6 +447,33 @@ static pm_status compat_run(pm_map* m, const pm_query_desc* desc, const float* d
     return check_cuda(m, "PM_MODE_ZHOU_COMPAT");
 }
 
+// The exact query of validated arguments: Hilbert sort of the positions,
+// then the search.  nrm_ready (optional) is an event the search waits for
+// after the sort, so a caller still copying the normals in overlaps the sort
+// with that copy.
+static pm_status query_exact_run(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4,
+                                 uint32_t nq, float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count,
+                                 cudaStream_t st, cudaEvent_t nrm_ready) {
+    if (nq == 0) return PM_OK;
+    pm_status s = ensure_query_capacity(m, nq, st);
+    if (s != PM_OK) return s;
+    const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
+    const bool prof = m->profiling && !capturing(st);
+    if (prof) cudaEventRecord(m->ev[3], st);
+    int nl = 0;
+    const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, qpos, nq, st, &nl) : nullptr;
+    if (prof) cudaEventRecord(m->ev[4], st);
+    if (nrm_ready) cudaStreamWaitEvent(st, nrm_ready, 0);
+    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
+    nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
+                    P<uint32_t>(m->counter), P<uint32_t>(m->fixq), tuning_of(m), st);
+    if (prof) cudaEventRecord(m->ev[5], st);
+    m->have_query_ev = prof;
+    m->query_launches = (uint32_t)nl;
+    m->launches += (uint64_t)nl;
+    return check_cuda(m, "pm_query");
+}
+
 pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, const float* d_qnrm4, uint32_t nq,
                    float* d_rad4, uint32_t* d_nbr, float* d_r2, uint32_t* d_count, void* stream) {
     pm_status s = query_common(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, false);
@@ -456,23 +483,7 @@ pm_status pm_query(pm_map* m, const pm_query_desc* desc, const float* d_qpos4, c
         if (d_nbr) return fail(m, PM_ERR_INVALID, "PM_MODE_ZHOU_COMPAT returns no neighbour lists (d_nbr must be NULL)");
         return compat_run(m, desc, d_qpos4, d_qnrm4, nq, nullptr, d_rad4, d_r2, d_count, st);
     }
-    if (nq == 0) return PM_OK;
-    s = ensure_query_capacity(m, nq, st);
-    if (s != PM_OK) return s;
-    const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
-    const bool prof = m->profiling && !capturing(st);
-    if (prof) cudaEventRecord(m->ev[3], st);
-    int nl = 0;
-    const uint32_t* order = desc->order == PM_ORDER_SORTED ? sort_queries(m, qpos, nq, st, &nl) : nullptr;
-    if (prof) cudaEventRecord(m->ev[4], st);
-    QueryOutputs out{reinterpret_cast<float4*>(d_rad4), d_nbr, d_r2, d_count};
-    nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
-                    P<uint32_t>(m->counter), P<uint32_t>(m->fixq), tuning_of(m), st);
-    if (prof) cudaEventRecord(m->ev[5], st);
-    m->have_query_ev = prof;
-    m->query_launches = (uint32_t)nl;
-    m->launches += (uint64_t)nl;
-    return check_cuda(m, "pm_query");
+    return query_exact_run(m, desc, d_qpos4, d_qnrm4, nq, d_rad4, d_nbr, d_r2, d_count, st, nullptr);
 }
 
 // Device address of a page-locked host array (cudaHostAlloc /
@@ -521,14 +532,14 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
     float4* dqp = P<float4>(m->hs_qpos);
     float4* dqn = P<float4>(m->hs_qnrm);
     float4* drad = P<float4>(m->hs_rad);
-    // A page-locked radiance array is written in place by the query kernel
+    // A page-locked, 16-byte aligned radiance array is written in place by the query kernel
     // (each estimate once, 16 bytes over PCIe while the search runs), which
     // takes the download off the critical path: 9.83 -> 9.27 ms end to end on
     // the plain workload.  A pageable one goes through a device copy.  The
     // normals are always copied in: read in place as well, they queue behind
     // the posted radiance writes on the link (12.76 ms with both in place;
     // 9.57 ms with the normals alone).
-    const bool rad_in_place = host_mapped(h_rad4) != nullptr;
+    const bool rad_in_place = nq > 0 && aligned16(h_rad4) && host_mapped(h_rad4) != nullptr;
     if (rad_in_place) drad = reinterpret_cast<float4*>(host_mapped(h_rad4));
     cudaEvent_t ev_photons = m->hs_ev[0], ev_done = m->hs_ev[1];
     // photons in, then the queries in pieces behind them on the copy stream
@@ -541,31 +552,37 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
     if (nq < chunks) chunks = nq ? nq : 1;
     uint32_t bounds[17];
     for (uint32_t c = 0; c <= chunks; ++c) bounds[c] = (uint32_t)(((uint64_t)nq * c) / chunks);
-    for (uint32_t c = 0; c < chunks; ++c) {
+    for (uint32_t c = 0; c < chunks; ++c) {   // positions first: the piece's sort needs only them
         const size_t off = bounds[c], len = bounds[c + 1] - bounds[c];
-        if (len) {
+        if (len)
             cudaMemcpyAsync(dqp + off, reinterpret_cast<const float4*>(h_qpos4) + off, len * sizeof(float4),
                             cudaMemcpyHostToDevice, m->hs_in);
+        cudaEventRecord(m->hs_ev[2 + 3 * c], m->hs_in);
+        if (len)
             cudaMemcpyAsync(dqn + off, reinterpret_cast<const float4*>(h_qnrm4) + off, len * sizeof(float4),
                             cudaMemcpyHostToDevice, m->hs_in);
-        }
-        cudaEventRecord(m->hs_ev[2 + 2 * c], m->hs_in);
+        cudaEventRecord(m->hs_ev[3 + 3 * c], m->hs_in);
     }
     s = check_cuda(m, "pm_build_query_host: copies in");
     if (s != PM_OK) return s;
     s = pm_build(m, reinterpret_cast<const float*>(dpos), reinterpret_cast<const float*>(dpow), n, format, stream);
     if (s != PM_OK) return s;
-    // each piece is answered once it has arrived; its radiance leaves on the second stream
+    if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    // each piece is sorted once its positions have arrived and searched once
+    // its normals have; its radiance leaves on the second stream
     for (uint32_t c = 0; c < chunks; ++c) {
         const size_t off = bounds[c], len = bounds[c + 1] - bounds[c];
-        cudaStreamWaitEvent(st, m->hs_ev[2 + 2 * c], 0);
+        cudaStreamWaitEvent(st, m->hs_ev[2 + 3 * c], 0);
         if (len) {
-            s = pm_query(m, desc, reinterpret_cast<const float*>(dqp + off), reinterpret_cast<const float*>(dqn + off),
-                         (uint32_t)len, reinterpret_cast<float*>(drad + off), nullptr, nullptr, nullptr, stream);
+            s = query_exact_run(m, desc, reinterpret_cast<const float*>(dqp + off),
+                                reinterpret_cast<const float*>(dqn + off), (uint32_t)len,
+                                reinterpret_cast<float*>(drad + off), nullptr, nullptr, nullptr, st, m->hs_ev[3 + 3 * c]);
             if (s != PM_OK) return s;
+        } else {
+            cudaStreamWaitEvent(st, m->hs_ev[3 + 3 * c], 0);
         }
-        cudaEventRecord(m->hs_ev[3 + 2 * c], st);
-        cudaStreamWaitEvent(m->hs_out, m->hs_ev[3 + 2 * c], 0);
+        cudaEventRecord(m->hs_ev[4 + 3 * c], st);
+        cudaStreamWaitEvent(m->hs_out, m->hs_ev[4 + 3 * c], 0);
         if (len && !rad_in_place)
             cudaMemcpyAsync(reinterpret_cast<float4*>(h_rad4) + off, drad + off, len * sizeof(float4),
                             cudaMemcpyDeviceToHost, m->hs_out);

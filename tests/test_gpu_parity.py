@@ -326,6 +326,27 @@ def test_build_query_host_matches_device_calls(cuda, chunks, pinned):
     assert pm.info().device_errors == 0
 
 
+def test_build_query_host_misaligned_pinned_output(cuda):
+    """A page-locked output that is not 16-byte aligned cannot take the
+    kernel's float4 stores: it goes through the device copy and still gets
+    the device calls' bits."""
+    from mnrt_b200.photon_map import PhotonMap
+    ph = gen.photons(20000, seed=77, caustic_frac=0.2)
+    q = gen.queries(3001, seed=78)
+    pm = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=32)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    buf = torch.zeros(q.n * 4 + 1, dtype=torch.float32).pin_memory()
+    out = buf[1:].view(q.n, 4)
+    assert out.data_ptr() % 16 != 0
+    pm.build_query_host(pin(ph.pos), pin(ph.pow), pin(q.pos), pin(q.nrm), out=out, filter="cone")
+    torch.cuda.synchronize()
+    pm2 = PhotonMap(ph.n, global_q_radius_max=0.05, knn_target_count=32)
+    pm2.build(torch.from_numpy(ph.pos).to(cuda), torch.from_numpy(ph.pow).to(cuda))
+    want = pm2.query(torch.from_numpy(q.pos).to(cuda), torch.from_numpy(q.nrm).to(cuda), filter="cone")["rad"].cpu()
+    assert torch.equal(out.view(torch.int32), want.view(torch.int32))
+    assert pm.info().device_errors == 0
+
+
 def test_build_query_host_empty_inputs(cuda):
     from mnrt_b200.photon_map import PhotonMap
     ph = gen.photons(1000, seed=73)
