@@ -276,12 +276,14 @@ def _morton48(p, lo, scale):
     return (spread(q[:, 0]) << np.uint64(2)) | (spread(q[:, 1]) << np.uint64(1)) | spread(q[:, 2])
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4095, 4096, 4097, 65537, 100003])
+@pytest.mark.parametrize("n", [1, 2, 3, 2047, 2048, 2049, 4097, 65537, 100003, 4194305])
 def test_radix_sort_and_scan_through_tree_order(cuda, n):
     """The exported tree order is exactly the order of (Morton code, caller
     index) -- the device radix sort checked end to end at odd sizes around the
-    4,096-key sort tile -- and the compaction scan kept exactly the nodes that
-    hold more than leaf_size photons."""
+    2,048-key sort tile, and above 2,048 tiles (4,194,304 keys), where a pass
+    scans the whole digit-major array instead of one row per digit -- and the
+    compaction scan kept exactly the nodes that hold more than leaf_size
+    photons."""
     ph = gen.photons(n, seed=600 + n, caustic_frac=0.3)
     ph.pos[: n // 3, :3] = np.round(ph.pos[: n // 3, :3] * 64) / 64   # many equal codes: ties by index
     pm = PhotonMap(n, global_q_radius_max=0.1)
@@ -295,8 +297,9 @@ def test_radix_sort_and_scan_through_tree_order(cuda, n):
     scale = np.float32(65536.0) / ext if ext > 0 else np.float32(0)
     idx = tpos[:, 3].view(np.uint32)
     codes = _morton48(ph.pos[idx], lo, scale)
-    key = codes.astype(object) * (1 << 32) + idx.astype(object)
-    assert all(key[i] < key[i + 1] for i in range(len(key) - 1)), "tree order is not (code, index) order"
+    dc = np.diff(codes.astype(np.int64))
+    di = np.diff(idx.astype(np.int64))
+    assert ((dc > 0) | ((dc == 0) & (di > 0))).all(), "tree order is not (code, index) order"
     # every kept node holds more than leaf_size photons: leaves of at most 16, internal slots otherwise
     cnts = nodes[:, [7, 15]]
     assert (cnts <= 16).all()
