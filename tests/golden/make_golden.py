@@ -6,11 +6,12 @@ The reference ships no golden vectors, known-answer tests or fixtures for the
 photon-map path, so these are the project's own: seeded inputs of the small
 configuration's shape (room photons, wall queries) with the expected exact
 neighbour lists, counts, r^2 and FP64 radiance for the box, cone and
-Epanechnikov filters, plus the packed direction bits of reference-layout
-(azimuth / polar angle) photons.  Every expected array is computed twice, by
-the C++ oracle (oracle/pm_oracle.cpp) and by the independent numpy
-restatement (tests/np_restate.py); the script refuses to write a fixture on
-which they disagree.
+Epanechnikov filters, the FP64 adjoint (dL/dpower, dL/dposition of a
+squared-error loss) for each filter, plus the packed direction bits of
+reference-layout (azimuth / polar angle) photons.  Every expected array is
+computed twice, by the C++ oracle (oracle/pm_oracle.cpp) and by the
+independent numpy restatement (tests/np_restate.py); the script refuses to
+write a fixture on which they disagree.
 """
 from __future__ import annotations
 
@@ -59,6 +60,30 @@ def make_case(name: str, c: dict) -> dict:
     return out
 
 
+def make_adjoint() -> dict:
+    """dL/dpower and dL/dposition for L = sum |E - T|^2, T the estimate of
+    powers scaled by seeded U[0.5, 1.5] on the same neighbour sets."""
+    ph = gen.photons(1024, seed=540, caustic_frac=0.2, power_mean=1.0 / 65536)
+    q = gen.queries(128, seed=541)
+    k, r = 16, 0.25
+    idx, _d2, cnt, _r2 = oracle.knn_brute(ph.pos, q.pos, k, r)
+    tpow = ph.pow.copy()
+    tpow[:, :3] *= np.random.default_rng(542).uniform(0.5, 1.5, size=(ph.n, 3)).astype(np.float32)
+    out = dict(pos=ph.pos, pow=ph.pow, qpos=q.pos, qnrm=q.nrm, k=np.uint32(k), r_max=np.float32(r), idx=idx,
+               count=cnt)
+    for filt in ("box", "cone", "epanechnikov"):
+        e = oracle.radiance_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, filt, 1.0, 0)
+        t = oracle.radiance_fp64(ph.pos, tpow, q.pos, q.nrm, idx, cnt, k, r, filt, 1.0, 0)
+        g = (2.0 * (e - t)).astype(np.float32).astype(np.float64)   # dL/dE as the engine takes it, FP32
+        a = oracle.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, g, filt, 1.0, 0)
+        b = np_restate.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, g, filt, 1.0, 0)
+        for x, y, what in ((a[0], b[0], "power"), (a[1], b[1], "position")):
+            if np.abs(x - y).max() > 1e-12 * np.abs(y).max():
+                raise SystemExit(f"adjoint ({filt}, {what}): oracle and numpy restatement disagree")
+        out[f"g_{filt}"], out[f"gpow_{filt}"], out[f"gpos_{filt}"] = g.astype(np.float32), a[0], a[1]
+    return out
+
+
 def make_ingest() -> dict:
     ph = gen.photons(512, seed=530, layout="reference")
     pos, pw = oracle.pack_reference(ph.pos, ph.pow)
@@ -71,6 +96,8 @@ def main() -> int:
         print("wrote", name)
     np.savez_compressed(OUT / "reference_ingest.npz", **make_ingest())
     print("wrote reference_ingest")
+    np.savez_compressed(OUT / "adjoint_k16_r025.npz", **make_adjoint())
+    print("wrote adjoint_k16_r025")
     return 0
 
 

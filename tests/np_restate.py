@@ -83,6 +83,57 @@ def radiance_fp64(pos4, pow4, q4, n4, nbr, cnt, k, r_max, filt="box", cone_k=1.0
     return out
 
 
+
+def backward_fp64(pos4, pow4, q4, n4, nbr, cnt, k, r_max, grad, filt="box", cone_k=1.0, min_found=0):
+    """dL/dpower and dL/dposition (n, 3) of L given dL/dE (grad, (nq, 3)) for
+    the estimate E_q = norm(r2_q) * sum_p f_qp w(d2_qp, r2_q) power_p, where
+    r2_q is the k-th neighbour's d2 (a function of its position) when k were
+    found, else R^2.  Derived from that formula: dE/dpower_p = norm f w;
+    dE/dx_p = norm f power_p dw/dd2 * 2 (x_p - q), plus, for the k-th
+    neighbour, (dnorm/dr2 S + norm sum_p' f power_p' dw/dr2) * 2 (x_k - q)."""
+    n = pos4.shape[0]
+    gpow = np.zeros((n, 3))
+    gpos = np.zeros((n, 3))
+    dirbits = pow4[:, 3].view(np.uint32)
+    kc = float(np.float32(cone_k))
+    for q in range(q4.shape[0]):
+        c = int(cnt[q])
+        qp = q4[q, :3].astype(np.float64)
+        if not np.isfinite(qp).all():
+            continue
+        r2 = float(np.float64(np.float32(r_max)) ** 2)
+        if c == k:
+            dv = pos4[nbr[q, k - 1], :3].astype(np.float64) - qp
+            r2 = float(dv @ dv)
+        if c == 0 or c < min_found or not r2 > 0:
+            continue
+        sel = nbr[q, :c].astype(np.int64)
+        fr = front(np.repeat(n4[q:q + 1], c, axis=0), dirbits[sel]).astype(np.float64)
+        dx = pos4[sel, :3].astype(np.float64) - qp
+        d2 = (dx * dx).sum(1)
+        phi = pow4[sel, :3].astype(np.float64)
+        if filt == "cone":
+            d, r = np.sqrt(d2), np.sqrt(r2)
+            w = 1.0 - d / (kc * r)
+            dw_dd2 = np.where(d > 0, -1.0 / (2.0 * kc * np.where(d > 0, d, 1.0) * r), 0.0)
+            dw_dr2 = d / (2.0 * kc * r2 * r)
+            norm = 1.0 / ((1.0 - 2.0 / (3.0 * kc)) * np.pi * r2)
+        elif filt == "epanechnikov":
+            w, dw_dd2, dw_dr2 = 1.0 - d2 / r2, np.full_like(d2, -1.0 / r2), d2 / (r2 * r2)
+            norm = 2.0 / (np.pi * r2)
+        else:
+            w, dw_dd2, dw_dr2 = np.ones_like(d2), np.zeros_like(d2), np.zeros_like(d2)
+            norm = 1.0 / (np.pi * r2)
+        g = grad[q].astype(np.float64)
+        np.add.at(gpow, sel, (fr * w)[:, None] * (norm * g)[None, :])
+        coef = fr * dw_dd2 * norm * (phi @ g)
+        if c == k:
+            S = ((fr * w)[:, None] * phi).sum(0)
+            T = ((fr * dw_dr2)[:, None] * phi).sum(0)
+            coef[k - 1] += g @ (-norm / r2 * S + norm * T)
+        np.add.at(gpos, sel, 2.0 * coef[:, None] * dx)
+    return gpow, gpos
+
 # ---------------------------------------------------------------------------
 # Illumination cuts (GPU/illumcut.cu, PhotonMap.cpp:287-452,
 # GPU/photon_knn.cu:338-433) on a tree in the engine's node layout.  This
