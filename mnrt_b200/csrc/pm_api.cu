@@ -539,8 +539,9 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
     // normals are always copied in: read in place as well, they queue behind
     // the posted radiance writes on the link (12.76 ms with both in place;
     // 9.57 ms with the normals alone).
-    const bool rad_in_place = nq > 0 && aligned16(h_rad4) && host_mapped(h_rad4) != nullptr;
-    if (rad_in_place) drad = reinterpret_cast<float4*>(host_mapped(h_rad4));
+    void* const rad_mapped = (nq > 0 && aligned16(h_rad4)) ? host_mapped(h_rad4) : nullptr;
+    const bool rad_in_place = rad_mapped != nullptr;
+    if (rad_in_place) drad = reinterpret_cast<float4*>(rad_mapped);
     cudaEvent_t ev_photons = m->hs_ev[0], ev_done = m->hs_ev[1];
     // photons in, then the queries in pieces behind them on the copy stream
     if (n) {
