@@ -267,8 +267,10 @@ QueryParams params_of(const pm_query_desc* d) {
 }
 
 // Hilbert order of the queries (returns the permutation or nullptr).
-const uint32_t* sort_queries(pm_map* m, const float4* qpos, uint32_t nq, cudaStream_t st, int* launches) {
-    *launches += query_order_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint32_t>(m->qkeys0), P<uint32_t>(m->qvals0), st);
+const uint32_t* sort_queries(pm_map* m, const float4* qpos, uint32_t nq, cudaStream_t st, int* launches,
+                             bool hilbert = true) {
+    *launches += query_order_keys(qpos, nq, P<MapHeader>(m->hdr), P<uint32_t>(m->qkeys0), P<uint32_t>(m->qvals0), st,
+                                  hilbert);
     uint32_t* keys[2] = {P<uint32_t>(m->qkeys0), P<uint32_t>(m->qkeys1)};
     uint32_t* vals[2] = {P<uint32_t>(m->qvals0), P<uint32_t>(m->qvals1)};
     const int cur = radix_sort_pairs32(keys, vals, nq, kQueryKeyBits, P<uint32_t>(m->qscratch), st, launches);
@@ -839,7 +841,8 @@ static pm_status icut_interp_run(pm_map* m, float r_max, const float4* qpos, con
                                  bool sorted, float4* out, cudaStream_t st, int* nl) {
     pm_status s = ensure_query_capacity(m, nq, st);
     if (s != PM_OK) return s;
-    const uint32_t* order = sorted ? sort_queries(m, qpos, nq, st, nl) : nullptr;
+    // Morton order: the interpolation is a thread per query (see k_query_order)
+    const uint32_t* order = sorted ? sort_queries(m, qpos, nq, st, nl, false) : nullptr;
     *nl += icut_interpolate(view_of(m), icut_of(m), qpos, qnrm, order, nq, r_max * r_max, out, st);
     return PM_OK;
 }

@@ -236,6 +236,12 @@ __device__ __forceinline__ uint32_t hilbert30(float x, float y, float z, const f
     return (spread3_10(X[0]) << 2) | (spread3_10(X[1]) << 1) | spread3_10(X[2]);
 }
 
+// 30-bit Morton code of the same 10-bit cells (the cut interpolation's query order).
+__device__ __forceinline__ uint32_t morton30(float x, float y, float z, const float* lo, float scale) {
+    return (spread3_10(quantize16(x, lo[0], scale) >> 6) << 2) | (spread3_10(quantize16(y, lo[1], scale) >> 6) << 1) |
+           spread3_10(quantize16(z, lo[2], scale) >> 6);
+}
+
 __device__ __forceinline__ uint64_t morton48(float x, float y, float z, const float* lo, float scale) {
     return (spread3_16(quantize16(x, lo[0], scale)) << 2) | (spread3_16(quantize16(y, lo[1], scale)) << 1) |
            spread3_16(quantize16(z, lo[2], scale));

@@ -109,7 +109,7 @@ struct QueryOutputs {
 };
 
 int query_order_keys(const float4* qpos, uint32_t nq, const MapHeader* hdr, uint32_t* keys, uint32_t* vals,
-                       cudaStream_t st);
+                       cudaStream_t st, bool hilbert = true);
 constexpr int kQueryKeyBits = 30;         // bits of the query Hilbert keys (sorted as uint32)
 constexpr int kBatchQueryMapShift = 30;   // batch query keys: (map id << 30) | 30-bit Hilbert index in the map's cell
 struct QueryTuning {
