@@ -61,10 +61,11 @@ def make_inputs(cfg: dict, rank: int):
 # ------------------------------------------------------------- CPU legs --
 
 def cpu_reference_step(ph, q, cfg, sample: int, threads: int, rng: np.random.Generator):
-    """One CPU step: full kd-tree build + a bounded query sample, scaled to Q."""
+    """One CPU step: full kd-tree build (multithreaded) + a bounded query
+    sample, scaled to Q."""
     from oracle import oracle
     t0 = time.perf_counter()
-    tree = oracle.KdTree(ph.pos)
+    tree = oracle.KdTree(ph.pos, threads=threads)
     t1 = time.perf_counter()
     sel = rng.choice(q.n, size=min(sample, q.n), replace=False)
     qp, qn = q.pos[sel], q.nrm[sel]
@@ -101,9 +102,12 @@ def run_reference(args, cfg) -> dict:
         vals.append(v)
         builds.append(b)
     wall = time.perf_counter() - t0
+    tb = time.perf_counter()
+    oracle.KdTree(ph.pos, threads=1)   # the build on one thread, for the record
+    build_1t_ms = 1000.0 * (time.perf_counter() - tb)
     value = float(np.mean(vals))
-    sample_desc = (f"kd-tree build over all {cfg['n']:,} photons + {sample:,} of {cfg['nq']:,} queries per step "
-                   f"(random subset), query time scaled to all queries")
+    sample_desc = (f"kd-tree build over all {cfg['n']:,} photons ({threads} threads) + {sample:,} of {cfg['nq']:,} "
+                   f"queries per step (random subset), query time scaled to all queries")
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * cfg["nq"] / value,
@@ -112,7 +116,8 @@ def run_reference(args, cfg) -> dict:
                    "r_max": cfg["r_max"], "filter": cfg["filter"], "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample_desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "build_ms_cpu": 1000.0 * float(np.mean(builds)), "wall_s": wall,
+        "build_ms_cpu": 1000.0 * float(np.mean(builds)), "build_ms_cpu_threads": threads,
+        "build_ms_cpu_1_thread": build_1t_ms, "wall_s": wall,
         "note": "the reference ships no CPU path and cannot be built here; this is the oracle's port of its "
                 "algorithm (exact kNN, multithreaded kd-tree)",
     }
@@ -414,8 +419,8 @@ def run_ours(args, cfg) -> dict | None:
         v, b, per = cpu_reference_step(ph, q, cfg, sample, threads, np.random.default_rng(11))
         result["cpu_baseline"] = {
             "value": v, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"kd-tree build over all {N:,} photons ({1000 * b:.0f} ms) + {sample:,} random queries of "
-                      f"{Q:,}, query time scaled to all queries"}
+            "sample": f"kd-tree build over all {N:,} photons ({1000 * b:.0f} ms on {threads} threads) + {sample:,} "
+                      f"random queries of {Q:,}, query time scaled to all queries"}
     return result
 
 

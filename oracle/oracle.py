@@ -47,6 +47,8 @@ def load() -> C.CDLL:
         "orc_pack_reference_photons": (None, [P, P, u32, P, P]),
         "orc_knn_brute": (None, [P, u32, P, u32, u32, f32, P, P, P, P, i32]),
         "orc_kdtree_build": (P, [P, u32]),
+        "orc_kdtree_build_mt": (P, [P, u32, C.c_int]),
+        "orc_kdtree_order": (None, [P, P]),
         "orc_kdtree_free": (None, [P]),
         "orc_knn_kdtree": (None, [P, P, u32, u32, f32, P, P, P, P, i32]),
         "orc_radiance_fp64": (None, [P, P, P, P, u32, P, P, u32, f32, i32, f32, u32, P, i32]),
@@ -99,10 +101,21 @@ def knn_brute(pos4, q4, k: int, r_max: float, threads: int = 0):
 class KdTree:
     """The CPU baseline: median-split point kd-tree + bounded-heap kNN."""
 
-    def __init__(self, pos4: np.ndarray):
+    def __init__(self, pos4: np.ndarray, threads: int = 1):
+        """threads = 1: the sequential build; otherwise the top levels' halves
+        build on their own threads (0 = every hardware thread), same tree."""
         self._lib = load()
         self._pos = _c(pos4, np.float32)
-        self._h = self._lib.orc_kdtree_build(self._pos.ctypes.data, self._pos.shape[0])
+        if threads == 1:
+            self._h = self._lib.orc_kdtree_build(self._pos.ctypes.data, self._pos.shape[0])
+        else:
+            self._h = self._lib.orc_kdtree_build_mt(self._pos.ctypes.data, self._pos.shape[0], int(threads))
+
+    def order(self) -> np.ndarray:
+        """Caller indices of the points in tree order."""
+        out = np.empty(self._pos.shape[0], np.uint32)
+        self._lib.orc_kdtree_order(self._h, out.ctypes.data)
+        return out
 
     def knn(self, q4, k: int, r_max: float, threads: int = 0):
         q4 = _c(q4, np.float32)

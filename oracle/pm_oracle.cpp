@@ -265,6 +265,46 @@ int kd_build_rec(KdTree& t, std::vector<uint32_t>& ord, const float* pos4, int b
     return me;
 }
 
+// The same tree built with the two halves of every split of the top `depth`
+// levels on their own threads: each half is a disjoint range of ord, so the
+// splits, and with them the points' tree order, are those of kd_build_rec;
+// only the node numbering differs (each half's nodes follow its parent's).
+// Returns the subtree's nodes with the subtree root first, child links local.
+std::vector<KdNode> kd_build_par(std::vector<uint32_t>& ord, const float* pos4, int b, int e, int depth) {
+    std::vector<KdNode> out;
+    if (depth <= 0 || e - b <= kLeaf) {
+        KdTree sub;
+        kd_build_rec(sub, ord, pos4, b, e);
+        return std::move(sub.nodes);
+    }
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = b; i < e; ++i)
+        for (int a = 0; a < 3; ++a) { float v = pos4[4 * (size_t)ord[i] + a]; lo[a] = std::min(lo[a], v); hi[a] = std::max(hi[a], v); }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a) if (hi[a] - lo[a] > hi[axis] - lo[axis]) axis = a;
+    const int mid = b + (e - b) / 2;
+    std::nth_element(ord.begin() + b, ord.begin() + mid, ord.begin() + e, [&](uint32_t u, uint32_t v) {
+        float fu = pos4[4 * (size_t)u + axis], fv = pos4[4 * (size_t)v + axis];
+        return fu < fv || (fu == fv && u < v);
+    });
+    const float split = pos4[4 * (size_t)ord[mid] + axis];   // before the halves reorder their ranges
+    std::vector<KdNode> left, right;
+    std::thread th([&] { left = kd_build_par(ord, pos4, b, mid, depth - 1); });
+    right = kd_build_par(ord, pos4, mid, e, depth - 1);
+    th.join();
+    out.reserve(1 + left.size() + right.size());
+    out.push_back(KdNode{split, axis, 1, (int32_t)(1 + left.size()), b, e});
+    auto append = [&](const std::vector<KdNode>& sub, int32_t off) {
+        for (KdNode nd : sub) {
+            if (nd.axis >= 0) { nd.left += off; nd.right += off; }
+            out.push_back(nd);
+        }
+    };
+    append(left, 1);
+    append(right, (int32_t)(1 + left.size()));
+    return out;
+}
+
 void kd_query(const KdTree& t, float qx, float qy, float qz, float R2, KHeap& h) {
     struct Ent { int32_t node; float lb; };
     Ent stack[128];
@@ -354,6 +394,33 @@ void* orc_kdtree_build(const float* pos4, uint32_t n) {
         t->idx[i] = ord[i];
     }
     return t;
+}
+
+// Multithreaded build (the top levels' halves on their own threads, up to
+// nthreads in flight; 0 = one per hardware thread): the same splits and tree
+// order of the points as orc_kdtree_build.
+void* orc_kdtree_build_mt(const float* pos4, uint32_t n, int nthreads) {
+    if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+    int depth = 0;
+    while ((1 << depth) < nthreads && depth < 16) ++depth;
+    KdTree* t = new KdTree();
+    t->n = n;
+    std::vector<uint32_t> ord(n);
+    std::iota(ord.begin(), ord.end(), 0u);
+    if (n > 0) t->nodes = kd_build_par(ord, pos4, 0, (int)n, depth);
+    else t->nodes.push_back(KdNode{0.f, -1, -1, -1, 0, 0});
+    t->x.resize(n); t->y.resize(n); t->z.resize(n); t->idx.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        t->x[i] = pos4[4 * (size_t)ord[i]]; t->y[i] = pos4[4 * (size_t)ord[i] + 1]; t->z[i] = pos4[4 * (size_t)ord[i] + 2];
+        t->idx[i] = ord[i];
+    }
+    return t;
+}
+
+// The points in tree order (caller indices), for tests.
+void orc_kdtree_order(const void* h, uint32_t* out) {
+    const KdTree& t = *(const KdTree*)h;
+    std::copy(t.idx.begin(), t.idx.end(), out);
 }
 
 void orc_kdtree_free(void* h) { delete (KdTree*)h; }

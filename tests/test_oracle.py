@@ -115,3 +115,16 @@ def test_radiance_fp64_matches_numpy(oracle_mod, filt):
     b = np_restate.radiance_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, filt, ck, 8)
     assert np.allclose(a, b, rtol=1e-12, atol=0)
     assert (a > 0).any()
+
+
+@pytest.mark.parametrize("n", [1, 33, 1000, 20011])
+def test_kdtree_multithreaded_build_matches_sequential(oracle_mod, n):
+    """The CPU baseline's multithreaded build makes the same splits: the same
+    tree order of the points and the same exact kNN answers."""
+    from mnrt_b200 import gen
+    ph = gen.photons(n, seed=70 + n, caustic_frac=0.3)
+    q = gen.queries(300, seed=71)
+    a, b = oracle_mod.KdTree(ph.pos), oracle_mod.KdTree(ph.pos, threads=4)
+    assert np.array_equal(a.order(), b.order())
+    for x, y in zip(a.knn(q.pos, 24, 0.15, threads=2), b.knn(q.pos, 24, 0.15, threads=2)):
+        assert np.array_equal(x, y)
