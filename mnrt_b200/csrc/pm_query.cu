@@ -7,21 +7,24 @@
 // refinements, gather) with one thread and a local-memory stack per query,
 // this kernel finds the exact k nearest photons in one pass:
 //
-//   * queries are processed in Hilbert order; one warp owns 32 consecutive
-//     queries (one per lane) and traverses the tree jointly: a child is
-//     visited when any lane's box lower bound passes its threshold, so
-//     control flow is warp-uniform and a leaf's photons are fetched once per
-//     warp with one coalesced load and broadcast by shuffles;
-//   * each lane keeps a max-heap of (d^2, tree position) keys in shared
-//     memory (k <= 128), ties broken by the photon's caller index;
-//   * a warp walks a chunk of consecutive rounds; the previous round's
-//     k-th distances bound the next round's search (triangle inequality:
-//     r_k(q) <= r_k(q') + |q - q'|), so most queries start with a tight
-//     radius instead of R;
+//   * queries are processed in Hilbert order (k_query_order + the radix
+//     sort), and warps take chunks of consecutive queries by guided
+//     self-scheduling (long chunks first, short ones last);
+//   * each query starts from a radius bound given by the previous query of
+//     its warp (triangle inequality: r_k(q) <= r_k(q') + |q - q'|), so most
+//     searches start tight instead of at R;
+//   * the default layout (PM_KBUF_WIDE, k_knn_group<32, *, *, true>) gives
+//     each query a whole warp over the 32-wide tree: lane i tests child i,
+//     passing leaves are scanned a photon per lane, candidates go to a
+//     shared-memory buffer, and an exact selection keeps the k smallest
+//     (d^2, caller index) keys; PM_KBUF_GROUP runs groups of lanes per query
+//     over the binary tree, and PM_KBUF_HEAP (k_knn_tree) a lane per query
+//     with a max-heap in shared memory, the warp traversing jointly;
 //   * the cone / Epanechnikov / box filter and the 1/(pi r^2)
 //     normalisation are fused into the epilogue; the weighted flux sum is
 //     accumulated in 64-bit fixed point, so the result does not depend on
-//     the order in which neighbours were found.
+//     the order in which neighbours were found, and every layout gives the
+//     same bits.
 #include "pm_internal.h"
 
 namespace pm {
@@ -52,7 +55,7 @@ struct KnnArgs {
     const uint32_t* fix_in;   // fix pass: the list it works through
     uint32_t* fix_count;
     const uint32_t* nq_dev;   // fix pass: query count read on the device
-    uint32_t rounds_per_chunk;
+    uint32_t rounds_per_chunk;   // smallest chunk of the guided schedule, in rounds
     uint32_t cap;             // group kernel: candidate buffer entries per query
     uint32_t smem_per_warp;   // group kernel: shared bytes per warp
     unsigned long long* stats;   // optional traversal counters (kStat*), nullptr = off
@@ -62,7 +65,7 @@ struct KnnArgs {
     uint64_t nbr_off;         // batch: first neighbour slot of the map's rows
     uint32_t q_off;           // batch: first query of the map
     uint32_t ph_off;          // batch: first photon of the map (caller indices are batch-global)
-    const uint64_t* qkeys;    // batch: sorted query keys, map id in bits 48..63
+    const uint64_t* qkeys;    // batch: sorted query keys, map id from bit kBatchQueryMapShift up
     const BatchGeom* bgeom;   // batch: per-map geometry (built)
     const BatchQuery* bq;     // batch: per-map query parameters
 };
