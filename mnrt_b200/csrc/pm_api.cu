@@ -1084,7 +1084,7 @@ pm_status pm_export_tree(pm_map* m, uint32_t* host_nodes, uint32_t max_nodes, fl
 // host applications hand the engine a fixed memory budget up front and let
 // nothing grow afterwards.  This entry point runs the same kernels as
 // pm_query, but the scratch they need beyond the caller's inputs and outputs
-// (query Morton keys, radix-sort histograms, the list of queries re-evaluated
+// (query Hilbert keys, radix-sort histograms, the list of queries re-evaluated
 // with FP64 distances, the work counters) is carved from
 // one file-scope device array of a fixed size.  The map itself must already
 // be built.  Nothing here calls cudaMalloc, cudaFree or any allocating
