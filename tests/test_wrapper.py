@@ -62,3 +62,20 @@ def test_tuning_is_validated_by_the_engine(pm):
         pm.set_tuning(leaf_size=16, warps_per_block=9)
     with pytest.raises(L.PMError):
         pm.set_tuning(leaf_size=16, rounds_per_chunk=0)
+
+
+def test_batch_offsets_and_descriptors(engine_lib):
+    from mnrt_b200.batch import PhotonMapBatch, _offsets, make_desc
+    assert _offsets([0, 5, 5, 9]).tolist() == [0, 5, 5, 9]
+    for bad in ([5, 9], [0], [[0, 1], [1, 2]]):
+        with pytest.raises(ValueError, match="offsets"):
+            _offsets(bad)
+    d = make_desc(16, 0.05, filter="epanechnikov", min_found=8)
+    assert d.k == 16 and d.filter == L.PM_FILTER_EPANECHNIKOV and d.min_found == 8 and d.mode == L.PM_MODE_EXACT
+    arr = PhotonMapBatch._descs([d, dict(k=4, r_max=0.1, filter="cone")])
+    assert arr[0].k == 16 and arr[1].k == 4 and arr[1].filter == L.PM_FILTER_CONE
+    b = PhotonMapBatch()
+    with pytest.raises(L.PMError):
+        b.set_tuning(leaf_size=0)
+    b.close()
+    b.close()   # closing twice is harmless
