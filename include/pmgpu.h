@@ -56,7 +56,8 @@ enum {
     PM_ERR_OOM = -3,         /* device allocation failed */
     PM_ERR_STATE = -4,       /* call not valid in this state (no map built, capture growth) */
     PM_ERR_DEVICE = -5,      /* a kernel reported an error (stack overflow, NaN input, ...) */
-    PM_ERR_UNSUPPORTED = -6  /* parameter outside what this build supports (k > PM_MAX_K) */
+    PM_ERR_UNSUPPORTED = -6  /* parameter outside what this build supports (k > PM_MAX_K, 2^31 or more
+                                photons or queries in one call) */
 };
 
 enum { PM_PHOTONS_REFERENCE = 0, PM_PHOTONS_PACKED = 1 };

@@ -144,6 +144,10 @@ template <class T> T* P(const DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Query counts stay below 2^31: slot, round and grid arithmetic in the
+// kernels is 32-bit.
+constexpr uint32_t kMaxQueries = 0x7fffffffu;
+
 size_t sort_words(uint32_t n) { return sort_scratch_words(n) + 1 + scan_scratch_words(n) + 64; }
 
 pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
@@ -417,6 +421,7 @@ static pm_status query_common(pm_map* m, const pm_query_desc* desc, const float*
     if (!m) return PM_ERR_INVALID;
     pm_status s = validate_desc(m, desc, exact_only);
     if (s != PM_OK) return s;
+    if (nq > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "nq = %u exceeds 2^31 - 1 queries", nq);
     if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
     if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_rad4))
         return fail(m, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
@@ -510,6 +515,7 @@ pm_status pm_build_query_host(pm_map* m, const float* h_pos4, const float* h_pow
     if (chunks == 0) chunks = 1;
     if (chunks > 16) return fail(m, PM_ERR_INVALID, "chunks must be at most 16");
     if (n > 0 && (!h_pos4 || !h_pow4)) return fail(m, PM_ERR_INVALID, "photon arrays must be non-NULL when n > 0");
+    if (nq > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "nq = %u exceeds 2^31 - 1 queries", nq);
     if (nq > 0 && (!h_qpos4 || !h_qnrm4 || !h_rad4))
         return fail(m, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
     if (m->max_photons && n > m->max_photons)
@@ -664,6 +670,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     if (!d_grad_pow4 && !d_grad_pos4) return fail(m, PM_ERR_INVALID, "both gradient outputs are NULL");
     if ((d_grad_pow4 && !aligned16(d_grad_pow4)) || (d_grad_pos4 && !aligned16(d_grad_pos4)))
         return fail(m, PM_ERR_INVALID, "gradient arrays must be 16-byte aligned");
+    if (nq > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "nq = %u exceeds 2^31 - 1 queries", nq);
     if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_grad_rad4))
         return fail(m, PM_ERR_INVALID, "query positions, normals and dL/dE must be non-NULL");
     if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_grad_rad4)))
@@ -744,6 +751,7 @@ pm_status pm_gather_for(pm_map* m, const pm_query_desc* desc, const float* d_hit
     const bool icut = desc->mode == PM_MODE_ICUT;
     if (icut && m->icut_gen != m->build_gen)
         return fail(m, PM_ERR_STATE, "PM_MODE_ICUT needs an illumination cut of the current tree (pm_icut_build)");
+    if (n > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "n = %u exceeds 2^31 - 1 shading points", n);
     if (n > 0 && (!d_hit_pos4 || !d_hit_nrm4 || !d_ray_dir4 || !d_ray_influence4 || !d_io_radiance4))
         return fail(m, PM_ERR_INVALID, "hit positions, normals, ray directions, influences and radiance must be non-NULL");
     if (n > 0 && d_io_recip_dist && !d_ray_origin4)
@@ -918,6 +926,7 @@ pm_status pm_icut_interpolate(pm_map* m, float r_max, const float* d_qpos4, cons
     if (!m) return PM_ERR_INVALID;
     if (!(r_max > 0.0f) || !std::isfinite(r_max))
         return fail(m, PM_ERR_INVALID, "r_max must be finite and > 0 (got %g)", (double)r_max);
+    if (nq > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "nq = %u exceeds 2^31 - 1 queries", nq);
     if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_irr4))
         return fail(m, PM_ERR_INVALID, "query positions, normals and output must be non-NULL");
     if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_irr4)))
@@ -974,6 +983,7 @@ pm_status pm_compute_query_radii(pm_map* m, const pm_query_desc* desc, const flo
     pm_status s = validate_desc(m, desc, false);
     if (s != PM_OK) return s;
     if (!m->built) return fail(m, PM_ERR_STATE, "no photon map has been built");
+    if (nq > kMaxQueries) return fail(m, PM_ERR_UNSUPPORTED, "nq = %u exceeds 2^31 - 1 queries", nq);
     if (nq > 0 && (!d_qpos4 || !d_radii)) return fail(m, PM_ERR_INVALID, "query positions and radii must be non-NULL");
     if (nq > 0 && !aligned16(d_qpos4)) return fail(m, PM_ERR_INVALID, "query positions must be 16-byte aligned");
     return compat_run(m, desc, d_qpos4, d_qpos4, nq, d_radii, nullptr, nullptr, nullptr,
@@ -1331,6 +1341,7 @@ pm_status batch_check_query_args(pm_batch* b, const uint32_t* offsets, const flo
     if (!b->built) return batch_fail(b, PM_ERR_STATE, "the batch has not been built");
     if (!offsets) return batch_fail(b, PM_ERR_INVALID, "query offsets are NULL");
     const uint32_t nq = offsets[b->num_maps];
+    if (nq > kMaxQueries) return batch_fail(b, PM_ERR_UNSUPPORTED, "more than 2^31 - 1 queries in a batch");
     if (nq > 0 && (!d_qpos4 || !d_qnrm4 || !d_rad4))
         return batch_fail(b, PM_ERR_INVALID, "query positions, normals and radiance output must be non-NULL");
     if (nq > 0 && (!aligned16(d_qpos4) || !aligned16(d_qnrm4) || !aligned16(d_rad4)))

@@ -159,6 +159,20 @@ def test_icut_validation_without_gpu(engine_lib):
     lib.pm_destroy(h)
 
 
+def test_counts_of_2_pow_31_are_unsupported(engine_lib):
+    """Query counts stay below 2^31 (32-bit slot arithmetic in the kernels):
+    larger calls are refused before any CUDA call."""
+    lib = engine_lib
+    h = _create(lib)
+    d = L.QueryDesc(k=10, r_max=0.1, filter=L.PM_FILTER_BOX, cone_k=1.0, mode=0, min_found=0, order=0, refine_iters=2)
+    big = 1 << 31
+    assert lib.pm_query(h, C.byref(d), 16, 16, big, 16, None, None, None, None) == L.PM_ERR_UNSUPPORTED
+    assert lib.pm_build_query_host(h, None, None, 0, L.PM_PHOTONS_PACKED, C.byref(d), 16, 16, big, 16, 1,
+                                   None) == L.PM_ERR_UNSUPPORTED
+    assert lib.pm_query(h, C.byref(d), 16, 16, big - 1, 16, None, None, None, None) == L.PM_ERR_STATE   # next check
+    lib.pm_destroy(h)
+
+
 def test_build_query_host_validation_without_gpu(engine_lib):
     lib = engine_lib
     h = _create(lib)
