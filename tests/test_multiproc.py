@@ -165,3 +165,17 @@ def test_query_divided_adjoint_all_reduce_matches_single_rank():
     assert (np.abs(out[0][0][:, :3] - hp) <= bp).all()
     assert (np.abs(out[0][1][:, :3] - hx) <= bx).all()
     assert np.abs(hp).max() > 0 and np.abs(hx).max() > 0
+
+
+def test_bench_reads_the_committed_profiles():
+    """bench.py's roofline object takes the DRAM and L2 bytes per launch from
+    the committed ncu summaries; both are present and plausible."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    dram = bench.profiled_traffic("k_knn_group", "plain")
+    l2 = bench.profiled_traffic("k_knn_group", "plain", "l2_bytes_per_launch")
+    assert dram is not None and 1e8 < dram < 1e10
+    assert l2 is not None and l2 > dram
+    assert bench.profiled_traffic("k_knn_group", "no_such_workload") is None
+    peak, kind = bench.measured_peaks()
+    assert peak > 1000 and kind in ("measured", "fallback")
