@@ -224,13 +224,17 @@ PM_API pm_status pm_query_bruteforce(pm_map* map, const pm_query_desc* desc, con
  *     output buffer, as for pm_query.
  *   - The query scratch (Hilbert sort keys, the list of queries re-evaluated
  *     with FP64 distances, the work counters) lives in one fixed array of
- *     about 7.2 MiB inside this library.  Every GPU that loads
+ *     about 5.1 MiB inside this library.  Every GPU that loads
  *     the library holds it until the process exits.
  *   - nq > PM_NOALLOC_MAX_QUERIES is rejected with PM_ERR_INVALID; split
  *     larger query sets into several calls.
  *   - The first call on each device looks up the array's device address,
  *     with that device current.  Make that first call before any stream
- *     capture.
+ *     capture: a first call on a capturing stream returns PM_ERR_STATE.
+ *     The address is kept for the life of the process; after
+ *     cudaDeviceReset on a device, do not call this entry point there again.
+ *   - pm_last_timings after this call reports its launch count but no phase
+ *     times, and pm_query_stats does not count it.
  *   - Every call, on every handle and stream, shares the one array.  Calls
  *     that overlap on the GPU (two streams, two threads) race and give wrong
  *     results.  Serialise them, e.g. on one stream.

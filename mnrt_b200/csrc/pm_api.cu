@@ -1110,9 +1110,11 @@ constexpr uint32_t kNoallocMaxQ = PM_NOALLOC_MAX_QUERIES;
 constexpr size_t kNoallocSortWords = 33024;   // >= sort_scratch_words(kNoallocMaxQ) = 33024, checked at set-up
 constexpr size_t kNoallocAlign = 256;
 constexpr size_t noalloc_round(size_t b) { return (b + kNoallocAlign - 1) / kNoallocAlign * kNoallocAlign; }
+// The single-map query sorts 32-bit Hilbert keys: 4 bytes per query for each
+// key and value buffer.
 constexpr size_t kNoallocKeys0 = 0;
-constexpr size_t kNoallocKeys1 = kNoallocKeys0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint64_t));
-constexpr size_t kNoallocVals0 = kNoallocKeys1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint64_t));
+constexpr size_t kNoallocKeys1 = kNoallocKeys0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
+constexpr size_t kNoallocVals0 = kNoallocKeys1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
 constexpr size_t kNoallocVals1 = kNoallocVals0 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
 constexpr size_t kNoallocSort = kNoallocVals1 + noalloc_round((size_t)kNoallocMaxQ * sizeof(uint32_t));
 constexpr size_t kNoallocFix = kNoallocSort + noalloc_round(kNoallocSortWords * sizeof(uint32_t));
@@ -1128,14 +1130,21 @@ std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
 
 // Device address of the scratch array on the current device (looked up on
-// the first call per device, with that device current).
-pm_status noalloc_scratch(pm_map* m, unsigned char** out) {
+// the first call per device, with that device current).  The lookup may load
+// the module, which must not happen inside a stream capture: a first call on
+// a capturing stream is refused with PM_ERR_STATE before any runtime call
+// that could invalidate the capture.  The cached address is never refreshed;
+// after cudaDeviceReset it no longer names the array (the header says so).
+pm_status noalloc_scratch(pm_map* m, cudaStream_t st, unsigned char** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return check_cuda(m, "pm_query_noalloc: cudaGetDevice");
     if (dev < 0 || dev >= kNoallocMaxDevices)
         return fail(m, PM_ERR_UNSUPPORTED, "pm_query_noalloc supports device ordinals below %d", kNoallocMaxDevices);
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
+        if (capturing(st))
+            return fail(m, PM_ERR_STATE, "the first pm_query_noalloc call on a device must come before any stream "
+                                         "capture (it looks up the scratch array's address)");
         if (sort_scratch_words(kNoallocMaxQ) > kNoallocSortWords)
             return fail(m, PM_ERR_STATE, "pm_query_noalloc: sort scratch of the fixed array is too small");
         void* p = nullptr;
@@ -1164,10 +1173,10 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
         return fail(m, PM_ERR_INVALID, "nq = %u exceeds PM_NOALLOC_MAX_QUERIES = %u; split the queries", nq,
                     kNoallocMaxQ);
     if (nq == 0) return PM_OK;
-    unsigned char* base = nullptr;
-    s = noalloc_scratch(m, &base);
-    if (s != PM_OK) return s;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* base = nullptr;
+    s = noalloc_scratch(m, st, &base);
+    if (s != PM_OK) return s;
     const float4* qpos = reinterpret_cast<const float4*>(d_qpos4);
     int nl = 0;
     const uint32_t* order = nullptr;
@@ -1187,6 +1196,10 @@ extern "C" pm_status pm_query_noalloc(pm_map* m, const pm_query_desc* desc, cons
     nl += query_knn(view_of(m), params_of(desc), qpos, reinterpret_cast<const float4*>(d_qnrm4), order, nq, out,
                     reinterpret_cast<uint32_t*>(base + kNoallocCounter), reinterpret_cast<uint32_t*>(base + kNoallocFix),
                     t, st);
+    // no phase events and no traversal counters here: pm_last_timings then
+    // reports this call's launch count and no query times
+    m->have_query_ev = false;
+    m->query_launches = (uint32_t)nl;
     m->launches += (uint64_t)nl;
     return check_cuda(m, "pm_query_noalloc");
 }

@@ -8,6 +8,7 @@ import torch
 from mnrt_b200 import gen
 from mnrt_b200 import _lib as L
 from mnrt_b200.photon_map import PhotonMap
+from tests.test_gpu_parity import format_errors, radiance_errors
 
 pytestmark = pytest.mark.gpu
 
@@ -37,10 +38,8 @@ def test_compat_matches_oracle(cuda, oracle_mod, n, nq, k, r, iters, filt, leaf)
     assert np.array_equal(radii.cpu().numpy(), o_radius)
     assert np.array_equal(out["count"].cpu().numpy().view(np.uint32), o_count)
     assert np.array_equal(out["r2"].cpu().numpy(), o_r2)
-    got = out["rad"].cpu().numpy()
-    floor = 1e-6 * max(np.abs(o_rad).mean(), 1e-30)
-    rel = np.abs(got[:, :3] - o_rad) / np.maximum(np.abs(o_rad), floor)
-    assert rel.max() <= 1e-5, rel.max()
+    e = radiance_errors(out["rad"].cpu().numpy()[:, :3], o_rad)
+    assert e["max"] <= 1e-5, format_errors(e)
     assert (o_count >= 0).all() and (o_radius <= np.float32(r)).all()
     assert pm.info().device_errors == 0
     # roughly k photons inside the refined radius (the reference's intent)

@@ -1,13 +1,14 @@
-"""The differentiation workload at full size: 1,048,576
-photons (80 % walls, 20 % caustic), 1,048,576 wall queries, k = 64,
-Epanechnikov filter, target from powers scaled by seeded U[0.5, 1.5], loss
-= sum |E - T|^2.  Gradient check on 1,024 sampled photons:
+"""The differentiation workload at full size: 1,048,576 photons (80 % walls,
+20 % caustic), 1,048,576 wall queries, k = 64, Epanechnikov filter, target
+from powers scaled by seeded U[0.5, 1.5], loss = sum |E - T|^2.  Gradient
+check on 1,024 sampled photons:
   * the engine's dL/dpower and dL/dposition against the oracle's FP64 host
     gradient on the same neighbour sets: relative 1e-5 (floor 1e-6 of max);
-  * the host gradient against FP64 central finite differences with h = 1e-4
-    (Richardson-combined with h/2): relative 1e-3 (floor 1e-3 of max),
-    samples whose neighbour set or k-th neighbour changes within +-h
-    excluded and counted (printed)."""
+  * the host gradient against plain FP64 central finite differences with
+    h = 1e-4: relative 1e-3 (floor 1e-3 of max), samples whose neighbour set
+    or k-th neighbour changes within +-h excluded and counted (printed); the
+    Richardson combination with h/2 is checked to the same bar as a second
+    figure."""
 import numpy as np
 import pytest
 import torch
@@ -73,5 +74,6 @@ def test_config4_gradient_check(cuda, oracle_mod):
     # boundaries on average (query density x 2 pi r_k x 2 h), so about half the samples sit on a
     # kink and are excluded; the rest must be plentiful
     assert ok.sum() >= 500
+    assert err_plain.max() <= 1e-3
     assert err_rich.max() <= 1e-3
     assert err_pow.max() <= 1e-3

@@ -2,9 +2,11 @@
 
 Bars (stated per test):
   * neighbour index sets, their order, counts and r^2: bit-exact;
-  * radiance: max relative error <= 1e-5 against the FP64 oracle on the same
-    neighbour sets, where the FP64 value is above 1e-6 of the map's mean
-    estimate (smaller values are checked with that absolute floor).
+  * radiance: relative error <= 1e-5 against the FP64 oracle on the same
+    neighbour sets for every nonzero FP64 value, however small (no absolute
+    floor), and exactly 0 where the FP64 value is 0.  The count of values
+    below 1e-6 of the mean estimate (where a floored bar would have judged
+    absolute error instead) is reported beside the relative errors.
 """
 import numpy as np
 import pytest
@@ -37,22 +39,51 @@ def run(ph, q, dev, k, r_max, filt="box", cone_k=1.0, min_found=0, brute=False, 
     return res
 
 
-def check_against_oracle(oracle_mod, ph, q, res, k, r_max, filt, cone_k=1.0, min_found=0, pos_ref=None, pow_ref=None):
+def radiance_errors(got, ref):
+    """Relative radiance errors of FP32 results against FP64 values, per
+    channel, with no absolute floor: |got - ref| / |ref| where ref != 0, and
+    0 / inf where ref == 0 and got is / is not exactly 0.  Returns a dict of
+    the max and mean relative error, the count of zero references, and the
+    count of nonzero references below 1e-6 of the mean |ref| (the values a
+    floored bar would have judged on absolute error) with their max error."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    nz = ref != 0.0
+    rel = np.zeros_like(ref)
+    rel[nz] = np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])
+    rel[~nz] = np.where(got[~nz] == 0.0, 0.0, np.inf)
+    floor = 1e-6 * np.abs(ref).mean() if ref.size else 0.0
+    small = nz & (np.abs(ref) < floor)
+    return {"max": float(rel.max()) if rel.size else 0.0, "mean": float(rel.mean()) if rel.size else 0.0,
+            "values": int(ref.size), "zero": int((~nz).sum()), "below_floor": int(small.sum()),
+            "below_floor_max": float(rel[small].max()) if small.any() else 0.0}
+
+
+def format_errors(e):
+    return (f"max rel err {e['max']:.2e}, mean {e['mean']:.2e} over {e['values']:,} values "
+            f"({e['zero']:,} exact zeros; {e['below_floor']:,} below 1e-6 of the mean, max {e['below_floor_max']:.2e})")
+
+
+def check_against_oracle(oracle_mod, ph, q, res, k, r_max, filt, cone_k=1.0, min_found=0, pos_ref=None, pow_ref=None,
+                         oracle_knn=None, threads=0):
+    """Bit-exact neighbour lists, counts and r^2, and radiance within RTOL of
+    the FP64 oracle (no floor); returns the error summary of radiance_errors."""
     pos_ref = ph.pos if pos_ref is None else pos_ref
     pow_ref = ph.pow if pow_ref is None else pow_ref
-    idx, d2, cnt, r2 = oracle_mod.KdTree(pos_ref).knn(q.pos, k, r_max)
+    if oracle_knn is None:
+        oracle_knn = oracle_mod.KdTree(pos_ref, threads=threads).knn(q.pos, k, r_max, threads=threads)
+    idx, _d2, cnt, r2 = oracle_knn
     nbr = res["nbr"].view(np.uint32)
     assert np.array_equal(res["count"].view(np.uint32), cnt), "neighbour counts differ"
     bad = np.where((nbr != idx).any(1))[0]
     assert bad.size == 0, f"{bad.size} queries with different neighbour lists, first {bad[:5]}"
     assert np.array_equal(res["r2"], r2), "r^2 differs"
-    ref = oracle_mod.radiance_fp64(pos_ref, pow_ref, q.pos, q.nrm, idx, cnt, k, r_max, filt, cone_k, min_found)
-    got = res["rad"][:, :3].astype(np.float64)
-    floor = 1e-6 * max(np.abs(ref).mean(), 1e-30)
-    rel = np.abs(got - ref) / np.maximum(np.abs(ref), floor)
-    assert rel.max() <= RTOL, f"max relative radiance error {rel.max():.3e}"
+    ref = oracle_mod.radiance_fp64(pos_ref, pow_ref, q.pos, q.nrm, idx, cnt, k, r_max, filt, cone_k, min_found,
+                                   threads=threads)
+    e = radiance_errors(res["rad"][:, :3], ref)
+    assert e["max"] <= RTOL, f"radiance: {format_errors(e)}"
     assert np.array_equal(res["rad"][:, 3], cnt.astype(np.float32))
-    return rel.max()
+    return e
 
 
 @pytest.mark.parametrize("filt", ["box", "cone", "epanechnikov"])
@@ -64,7 +95,7 @@ def test_small_config_parity(cuda, oracle_mod, filt):
     res = run(ph, q, cuda, cfg["k"], cfg["r_max"], filt)
     assert res["info"].device_errors == 0
     err = check_against_oracle(oracle_mod, ph, q, res, cfg["k"], cfg["r_max"], filt)
-    print(f"small config {filt}: max rel err {err:.2e}")
+    print(f"small config {filt}: {format_errors(err)}")
 
 
 KERNELS = [dict(kbuf_layout=0), dict(kbuf_layout=1, queries_per_warp=1), dict(kbuf_layout=1, queries_per_warp=2),
@@ -226,10 +257,8 @@ def test_engine_reproduces_golden(cuda, name, filt):
     assert np.array_equal(res["nbr"].view(np.uint32), g["idx"])
     assert np.array_equal(res["count"].view(np.uint32), g["count"])
     assert np.array_equal(res["r2"], g["r2"])
-    ref = g[f"rad_{filt}"]
-    floor = 1e-6 * max(np.abs(ref).mean(), 1e-30)
-    rel = np.abs(res["rad"][:, :3] - ref) / np.maximum(np.abs(ref), floor)
-    assert rel.max() <= RTOL, rel.max()
+    e = radiance_errors(res["rad"][:, :3], g[f"rad_{filt}"])
+    assert e["max"] <= RTOL, format_errors(e)
 
 
 @pytest.mark.parametrize("filt", ["box", "cone", "epanechnikov"])

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from mnrt_b200 import gen
-from tests.test_gpu_parity import check_against_oracle, run
+from tests.test_gpu_parity import check_against_oracle, format_errors, radiance_errors, run
 
 pytestmark = pytest.mark.gpu
 
@@ -138,9 +138,8 @@ def test_random_compat(cuda, oracle_mod, seed):
     assert np.array_equal(radii.cpu().numpy(), o_radius)
     assert np.array_equal(out["count"].cpu().numpy().view(np.uint32), o_count)
     assert np.array_equal(out["r2"].cpu().numpy(), o_r2)
-    got = out["rad"].cpu().numpy()
-    floor = 1e-6 * max(np.abs(o_rad).mean(), 1e-30)
-    assert (np.abs(got[:, :3] - o_rad) / np.maximum(np.abs(o_rad), floor)).max() <= 1e-5
+    e = radiance_errors(out["rad"].cpu().numpy()[:, :3], o_rad)
+    assert e["max"] <= 1e-5, format_errors(e)
     assert pm.info().device_errors == 0
     pm.close()
 

@@ -8,8 +8,10 @@ in one fixed array inside the library, shared by every call.
 
 This test calls it through the C ABI twice in a row, on different query sets
 and parameters, and checks each result against pm_query on the same map:
-neighbour lists, counts and r^2 bit-exact, radiance within RTOL.  A counting
-allocator on the handle shows that no call reaches the handle's allocator.
+neighbour lists, counts, r^2 and radiance bit for bit (the header promises
+identical results; that is stricter than the parity tests' RTOL, which the
+radiance also meets).  A counting allocator on the handle shows that no call
+reaches the handle's allocator.
 
 The file is named so that pytest collects it last.
 """
@@ -91,6 +93,9 @@ def test_query_noalloc_matches_query(cuda):
             out = _outputs(nq, k, dev)
             _call(lib, lib.pm_query_noalloc, h, d, qpos, qnrm, out)
             torch.cuda.synchronize()
+            tm = L.Timings()
+            assert lib.pm_last_timings(h, C.byref(tm)) == L.PM_OK
+            assert tm.query_launches > 0 and tm.query_ms == 0.0   # this call's launches, no phase times
             results.append((d, qpos, qnrm, {key: v.cpu().numpy() for key, v in out.items()}))
         assert len(allocs) == after_build, "pm_query_noalloc reached the handle's allocator"
 
@@ -102,6 +107,7 @@ def test_query_noalloc_matches_query(cuda):
             for key in ("nbr", "count", "r2"):
                 assert np.array_equal(got[key], ref[key]), key
             np.testing.assert_allclose(got["rad"], ref["rad"], rtol=RTOL, atol=0.0)
+            assert np.array_equal(got["rad"].view(np.uint32), ref["rad"].view(np.uint32)), "radiance bits"
             assert (got["count"] > 0).all()
 
         info = L.MapInfo()
