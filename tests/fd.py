@@ -40,6 +40,7 @@ class FDResult:
     fd: np.ndarray          # (s, 3) finite differences (nan where excluded)
     excluded: np.ndarray    # (s, 3) bool
     num_excluded: int
+    scale: np.ndarray = None   # (s,) smallest (k+1)-th neighbour distance of the queries the photon moves
 
 
 class LossFD:
@@ -155,12 +156,14 @@ class LossFD:
         out = np.full((len(photons), 3), np.nan)
         plain = np.full((len(photons), 3), np.nan)
         excl = np.zeros((len(photons), 3), bool)
+        scale = np.full(len(photons), np.inf)
         for s, p in enumerate(photons):
             p = int(p)
             qsel = self._affected(p, h)
             if qsel.size == 0:
                 out[s] = plain[s] = 0.0
                 continue
+            scale[s] = self.rk[qsel].min()
             base = self._rows(qsel, p, self.pos[p, :3])
             for a in range(3):
                 d1 = self._central(p, qsel, base, a, h)
@@ -170,7 +173,7 @@ class LossFD:
                     continue
                 plain[s, a] = d1
                 out[s, a] = (4.0 * d2 - d1) / 3.0
-        r = FDResult(out, excl, int(excl.sum()))
+        r = FDResult(out, excl, int(excl.sum()), scale)
         r.plain = plain
         return r
 

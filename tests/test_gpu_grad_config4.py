@@ -5,10 +5,17 @@ check on 1,024 sampled photons:
   * the engine's dL/dpower and dL/dposition against the oracle's FP64 host
     gradient on the same neighbour sets: relative 1e-5 (floor 1e-6 of max);
   * the host gradient against plain FP64 central finite differences with
-    h = 1e-4: relative 1e-3 (floor 1e-3 of max), samples whose neighbour set
-    or k-th neighbour changes within +-h excluded and counted (printed); the
-    Richardson combination with h/2 is checked to the same bar as a second
-    figure."""
+    h = 1e-4: relative 1e-3 (floor 1e-3 of max) on every sample whose
+    neighbour distances are large against h (the smallest k-th-neighbour
+    distance of the queries the photon moves at least 20 h); samples whose
+    neighbour set or k-th neighbour changes within +-h are excluded and
+    counted (printed);
+  * the Richardson combination of h and h/2 (fourth order) to the same bar on
+    every sample, the caustic's included.
+In the caustic blob (sigma = 0.01, 200k photons) the k-th-neighbour distance
+falls to about 3e-4 = 3 h, where the plain difference's h^2 term is of the
+order of the gradient itself: there the plain difference is no measurement
+of the gradient, and those samples are counted and printed, not asserted."""
 import numpy as np
 import pytest
 import torch
@@ -62,18 +69,27 @@ def test_config4_gradient_check(cuda, oracle_mod):
                                           "epanechnikov")
     fd = LossFD(oracle_mod, ph.pos, ph.pow, q.pos, q.nrm, t, k, r, "epanechnikov")
     f = fd.position(sample)
+    h = 1e-4
     ok = ~f.excluded
+    smooth = ok & (f.scale[:, None] >= 20 * h)   # neighbour distances >= 20 h: plain FD resolves the gradient
     err_rich = rel_err(hx64[sample][ok], f.fd[ok], 1e-3)
-    err_plain = rel_err(hx64[sample][ok], f.plain[ok], 1e-3)
+    err_plain_all = rel_err(hx64[sample][ok], f.plain[ok], 1e-3)   # floor: 1e-3 of the largest sampled gradient
+    err_plain = err_plain_all[smooth[ok]]
     fp = fd.power(sample[:256])
     err_pow = rel_err(hp64[sample[:256]], fp, 1e-3)
-    print(f"config 4: FD position check on {ok.sum()} of {ok.size} samples ({f.num_excluded} excluded: set change "
-          f"within +-h): max rel err {err_rich.max():.2e} (Richardson), {err_plain.max():.2e} (plain h=1e-4), "
-          f"within 1e-3 plain: {(err_plain <= 1e-3).mean() * 100:.1f} %; power FD max rel err {err_pow.max():.2e}")
+    print(f"config 4: FD position check, plain h=1e-4: max rel err {err_plain.max():.2e} on {smooth.sum()} samples "
+          f"with neighbour distances >= 20 h; over all {ok.sum()} included samples {(err_plain_all <= 1e-3).sum()} "
+          f"within 1e-3 (the rest in the caustic, distances {f.scale[(ok & ~smooth).any(1)].min():.1e} .. "
+          f"{f.scale[(ok & ~smooth).any(1)].max():.1e}); Richardson (h, h/2): max rel err {err_rich.max():.2e} on all "
+          f"{ok.sum()}; {f.num_excluded} of {ok.size} excluded (set change within +-h); "
+          f"power FD max rel err {err_pow.max():.2e}")
     # at this density an in-plane move of 1e-4 crosses about 2.8 queries' k-th-neighbour
     # boundaries on average (query density x 2 pi r_k x 2 h), so about half the samples sit on a
     # kink and are excluded; the rest must be plentiful
-    assert ok.sum() >= 500
+    assert ok.sum() >= 500 and smooth.sum() >= 500
     assert err_plain.max() <= 1e-3
+    near = np.broadcast_to(f.scale[:, None] < 20 * h, ok.shape)[ok]
+    assert (err_plain_all[near] > 1e-3).sum() == (err_plain_all > 1e-3).sum(), \
+        "a plain-FD miss outside the caustic"
     assert err_rich.max() <= 1e-3
     assert err_pow.max() <= 1e-3
