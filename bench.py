@@ -10,14 +10,24 @@ R = 0.05, cone filter, FP32.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun (one rank per GPU) the plain, final-gather and icut
-workloads run an independent replica per rank (its own seeded map and query
-set, no data exchange): scaling is weak and value is the total queries/s of
-all ranks.  The batch workload divides its maps over the ranks by LPT; the
+Under torchrun (one rank per GPU) the plain and final-gather workloads build
+the same map on every rank and divide its queries into contiguous ranges
+(mnrt_b200/shard.py query_range; no data exchange, the radiance stays on the
+rank that computed it): scaling is strong and value is all queries over the
+slowest rank's step.  --division replicas instead gives every rank its own
+seeded map and query set (weak scaling); the icut workload always runs
+replicas.  The batch workload divides its maps over the ranks by LPT; the
 diff workload builds the map on every rank, divides the queries and sums the
 adjoint's partial gradients with one all-reduce (mnrt_b200/shard.py).
 --impl reference times the CPU port of the reference algorithm (oracle/,
 multithreaded kd-tree) on the same workload.
+
+The default run (plain workload, one GPU) adds three sub-objects measured
+after its own timed region, in the same process: "final_gather" (4,194,304
+photons, 8,388,608 queries, k = 64: Hilbert-sorted against as-given query
+order), "batch" (64 maps in one CUDA graph against 64 sequential per-map
+calls) and "diff" (forward and forward + adjoint times, gradient descent on
+the powers).  --no-extras skips them.
 """
 from __future__ import annotations
 
@@ -282,16 +292,31 @@ def barrier(world: int) -> None:
     torch.cuda.synchronize()
 
 
-def run_ours(args, cfg) -> dict | None:
+def run_ours(args, cfg, light: bool = False) -> dict | None:
+    """The plain one-map step.  light: the device-resident step only (no
+    end-to-end leg, no build median, no CPU baseline): the form the default
+    run uses for its final-gather sub-measurement."""
     import torch
     import torch.distributed as dist
 
     world, rank, local, dev = init_ranks()
 
+    from mnrt_b200 import gen
     from mnrt_b200.photon_map import PhotonMap
+    from mnrt_b200.shard import query_range
 
-    ph, q = make_inputs(cfg, rank)
-    N, Q, k, R = cfg["n"], cfg["nq"], cfg["k"], cfg["r_max"]
+    # N > 1: one map, its queries divided into contiguous ranges (every rank
+    # builds the same map); --division replicas gives every rank its own map
+    division = args.division or ("queries" if world > 1 else "replicas")
+    if division == "queries":
+        ph, q_all = make_inputs(cfg, 0)
+        qa, qb = query_range(q_all.n, rank, world)
+        q = gen.QuerySet(np.ascontiguousarray(q_all.pos[qa:qb]), np.ascontiguousarray(q_all.nrm[qa:qb]))
+        Q_job = q_all.n
+    else:
+        ph, q = make_inputs(cfg, rank)
+        Q_job = world * q.n
+    N, Q, k, R = cfg["n"], q.n, cfg["k"], cfg["r_max"]
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     h_pos, h_pow, h_qpos, h_qnrm = pin(ph.pos), pin(ph.pow), pin(q.pos), pin(q.nrm)
     h_rad = torch.empty((Q, 4), dtype=torch.float32).pin_memory()
@@ -350,7 +375,17 @@ def run_ours(args, cfg) -> dict | None:
     info = pm.info()
     total_ms = rank_max([float(np.sum(steps_ms))], dev)[0]
     ms_per_step = total_ms / args.steps
-    value = world * Q / (ms_per_step / 1000.0)
+    value = Q_job / (ms_per_step / 1000.0)
+
+    if light:
+        kern_ms = float(np.mean(kernels))
+        res = {"value": value, "ms_per_step": ms_per_step, "build_ms": float(np.mean(builds)),
+               "query_sort_ms": float(np.mean(sorts)), "query_kernel_ms": kern_ms,
+               "query_kernel_queries_per_s": Q / (kern_ms / 1000.0), "clocks": clocks,
+               "device_errors": info.device_errors, "gpu_launches": int(launches), "tuning": tuning}
+        pm.close()
+        close_ranks(world)
+        return res if rank == 0 else None
 
     # end to end through the public API: pinned host in, host radiance out.
     # pm_build_query_host copies the photons in and builds while the queries
@@ -366,7 +401,7 @@ def run_ours(args, cfg) -> dict | None:
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_total = rank_max([float(np.sum(e2e_ms))], dev)[0]
-    e2e_value = world * Q / (e2e_total / args.steps / 1000.0)
+    e2e_value = Q_job / (e2e_total / args.steps / 1000.0)
     if not torch.equal(h_rad.view(torch.int32), d_rad.cpu().view(torch.int32)):
         raise RuntimeError("host-buffer path and device path disagree")
 
@@ -386,12 +421,17 @@ def run_ours(args, cfg) -> dict | None:
     build_bytes = 68 * N + 64 * (nodes + 1)
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if division == "queries" and world > 1 else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R,
+        "config": {"workload": cfg["workload"], "photons": N, "queries": Q_job, "k": k, "r_max": R,
                    "filter": cfg["filter"], "query_order": "as given" if args.unsorted else "Hilbert-sorted",
                    "l2": "flushed between steps (256 MiB write, untimed)",
-                   "parallelism": f"{world} independent replica(s), one per GPU", "tuning": tuning},
+                   "parallelism": (f"one map built on each of {world} GPUs, its queries divided into {world} "
+                                   f"contiguous ranges (rank 0: {Q:,}), no exchange"
+                                   if division == "queries" and world > 1 else
+                                   f"{world} independent replica(s), one per GPU"),
+                   "tuning": tuning},
         "build_ms": build_ms, "build_ms_median_of_20_warm": build_median_ms, "query_ms": float(np.mean(queries)), "query_sort_ms": float(np.mean(sorts)),
         "query_kernel_ms": kern_ms, "query_only_mqueries_per_s": Q / (float(np.mean(queries)) / 1000.0) / 1e6,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -402,6 +442,7 @@ def run_ours(args, cfg) -> dict | None:
                            "unit": "GB/s", "frac": build_bytes / (build_ms / 1000.0) / 1e9 / peak,
                            "algorithmic_bytes": build_bytes},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 32 * N + 32 * Q,
+                "per_rank_bytes": world > 1,
                 "d2h_bytes_per_step": 16 * Q, "call": "pm_build_query_host (pinned host buffers)",
                 "chunks": args.chunks, "ms_per_step": e2e_total / args.steps},
         "gpu_launches": int(launches),
@@ -476,13 +517,15 @@ def run_diff(args, cfg) -> dict | None:
         fwd(out_plain); fwd(out); bwd()
     t_fwd, t_bwd = [], []
     barrier(world)
-    for _ in range(args.steps):
-        flush.zero_()
-        ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
-        flush.zero_()
-        ev[0].record(); fwd(out); ev[2].record(); bwd(); ev[3].record(); ev[3].synchronize()
-        t_fwd.append(ev[0].elapsed_time(ev[2]))
-        t_bwd.append(ev[2].elapsed_time(ev[3]))
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            ev[0].record(); fwd(out_plain); ev[1].record(); ev[1].synchronize()
+            flush.zero_()
+            ev[0].record(); fwd(out); ev[2].record(); bwd(); ev[3].record(); ev[3].synchronize()
+            t_fwd.append(ev[0].elapsed_time(ev[2]))
+            t_bwd.append(ev[2].elapsed_time(ev[3]))
+    clocks = clk.summary()
     # forward without neighbour lists, timed on its own
     plain = []
     for _ in range(args.steps):
@@ -533,6 +576,7 @@ def run_diff(args, cfg) -> dict | None:
                    "l2": "flushed between steps (256 MiB write, untimed)",
                    "parallelism": "one GPU" if world == 1 else
                    f"map on every rank, queries divided over {world} ranks, gradient all-reduce (NCCL, f64)"},
+        "clocks": clocks,
         "forward_ms": fwd_ms, "forward_no_lists_ms": plain_ms, "backward_ms": bwd_ms,
         "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms, "fwd_bwd_over_fwd_no_lists": (fwd_ms + bwd_ms) / plain_ms,
         "gradient_descent": {"steps": steps, "loss_first": losses[0], "loss_last": losses[-1],
@@ -669,15 +713,19 @@ def run_batch(args) -> dict | None:
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
+    clock_runs = []
+
     def timed(fn):
         for _ in range(args.warmup):
             fn()
         barrier(world)
         ts = []
-        for _ in range(args.steps):
-            flush.zero_()
-            e0.record(); fn(); e1.record(); e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                e0.record(); fn(); e1.record(); e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        clock_runs.append(clk.summary())
         barrier(world)
         return float(np.mean(ts))
 
@@ -735,10 +783,43 @@ def run_batch(args) -> dict | None:
         "batched_graph_ms": graph_ms, "batched_eager_ms": eager_ms, "sequential_per_map_ms": seq_ms,
         "sequential_queries_per_s": Q_all / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q_all / (eager_ms / 1000.0),
         "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": int(errors),
+        "clocks": clock_runs[-1] if clock_runs else None,
         "batch_tuning": None if bt is None else {
             "leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block, "rounds_per_chunk": bt.rounds_per_chunk,
             "wide_tree": bt.kbuf_layout == 2, "chosen_by": "pm_batch_autotune (rank 0)"},
     }
+
+
+def run_extras(args) -> dict:
+    """The other workloads' headline figures, measured after the default
+    line's own timed region in the same process (one GPU):
+      final_gather  config-2 queries Hilbert-sorted against taken as given
+      batch         the 64-map batch (one graph) against 64 sequential per-map calls
+      diff          forward and forward + adjoint of the differentiation workload,
+                    then the gradient-descent run on the powers
+    Each keeps its own clocks record."""
+    import copy
+    out = {}
+    fg_cfg = workload_config("final_gather")
+    a = copy.copy(args)
+    a.no_cpu_baseline = True
+    a.unsorted = False
+    srt = run_ours(a, fg_cfg, light=True)
+    a.unsorted = True
+    uns = run_ours(a, fg_cfg, light=True)
+    out["final_gather"] = {
+        "workload": fg_cfg["workload"], "metric": "queries/s (build + query per step)",
+        "sorted_queries_per_s": srt["value"], "unsorted_queries_per_s": uns["value"],
+        "speedup_sorted_over_unsorted": srt["value"] / uns["value"],
+        "sorted": srt, "unsorted": uns}
+    b = run_batch(copy.copy(args))
+    out["batch"] = {k: b[k] for k in ("config", "value", "unit", "batched_graph_ms", "batched_eager_ms",
+                                      "sequential_per_map_ms", "sequential_queries_per_s",
+                                      "speedup_graph_over_sequential", "device_errors", "clocks", "batch_tuning")}
+    d = run_diff(copy.copy(args), workload_config("diff"))
+    out["diff"] = {k: d[k] for k in ("config", "forward_ms", "forward_no_lists_ms", "backward_ms",
+                                     "fwd_bwd_over_fwd", "fwd_bwd_over_fwd_no_lists", "gradient_descent", "clocks")}
+    return out
 
 
 def main(argv=None) -> int:
@@ -750,7 +831,12 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="plain", choices=["small", "plain", "final_gather", "diff", "batch", "icut"])
     ap.add_argument("--maps", type=int, default=64, help="maps of the batch workload")
     ap.add_argument("--unsorted", action="store_true", help="keep the queries in the given order")
+    ap.add_argument("--division", choices=["queries", "replicas"], default=None,
+                    help="N > 1, plain / final-gather workloads: divide one map's queries over the ranks "
+                         "(the default) or run an independent replica per rank")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the final-gather, batch and diff sub-measurements")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel setting")
     ap.add_argument("--gd-steps", type=int, default=200, help="gradient-descent steps of the diff workload")
     ap.add_argument("--leaf", type=int, default=0)
@@ -784,6 +870,8 @@ def main(argv=None) -> int:
             print(json.dumps(res), flush=True)
         return 0
     res = run_ours(args, cfg)
+    if res is not None and args.config == "plain" and res["n_gpus"] == 1 and not args.no_extras:
+        res.update(run_extras(args))
     if res is not None:
         print(json.dumps(res), flush=True)
     return 0

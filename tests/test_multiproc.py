@@ -1,7 +1,8 @@
-"""The N-GPU path of bench.py on CPU: two gloo ranks.  Each rank runs an
-independent replica (its own seeded photons and queries, no exchange on the
-data path); the only collective is the max over ranks of the timed region's
-device time, and rank 0 alone prints."""
+"""The N-GPU path of bench.py on CPU: two gloo ranks.  The plain workload
+divides one map's queries into contiguous ranges (every rank builds the same
+map, no exchange on the data path); --division replicas gives every rank its
+own seeded photons and queries.  The only collective of the timed region is
+the max over ranks of its device time, and rank 0 alone prints."""
 import os
 import subprocess
 import sys
@@ -49,7 +50,7 @@ def test_rank_max_without_process_group():
     assert bench.rank_max([3.0, 1.5]) == [3.0, 1.5]
 
 
-def test_replicas_have_their_own_inputs():
+def test_replica_division_gives_ranks_their_own_inputs():
     sys.path.insert(0, str(ROOT))
     import bench
     cfg = bench.workload_config("small")
@@ -100,6 +101,72 @@ def test_query_range_partitions_contiguously():
             assert all(r[i][1] == r[i + 1][0] for i in range(world - 1))
             sizes = [b - a for a, b in r]
             assert max(sizes) - min(sizes) <= 1
+
+
+def _forward_worker(rank, world, port, q):
+    """Each rank: the oracle's exact kNN and FP64 estimate over its own query
+    range of one map, then an all-gather of the per-range answers."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from mnrt_b200.shard import query_range
+    from oracle import oracle
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        cfg = bench.workload_config("small")
+        ph, qs = bench.make_inputs(cfg, 0)          # every rank: the same map and query set
+        a, b = query_range(qs.n, rank, world)
+        idx, _d2, cnt, r2 = oracle.KdTree(ph.pos).knn(qs.pos[a:b], cfg["k"], cfg["r_max"])
+        rad = oracle.radiance_fp64(ph.pos, ph.pow, qs.pos[a:b], qs.nrm[a:b], idx, cnt, cfg["k"], cfg["r_max"],
+                                   cfg["filter"])
+        mine = [torch.from_numpy(idx.view(np.int32).copy()), torch.from_numpy(cnt.view(np.int32).copy()),
+                torch.from_numpy(r2.copy()), torch.from_numpy(rad.copy())]
+        # ranges differ by at most one query: pad to the largest, gather, trim
+        size = max(query_range(qs.n, i, world)[1] - query_range(qs.n, i, world)[0] for i in range(world))
+        parts = []
+        for t in mine:
+            pad = torch.zeros((size,) + tuple(t.shape[1:]), dtype=t.dtype)
+            pad[:t.shape[0]] = t
+            got = [torch.empty_like(pad) for _ in range(world)]
+            dist.all_gather(got, pad)
+            parts.append(torch.cat([g[:query_range(qs.n, i, world)[1] - query_range(qs.n, i, world)[0]]
+                                    for i, g in enumerate(got)]).numpy())
+        q.put((rank, parts))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_query_divided_forward_assembles_the_undivided_answer():
+    """One map, queries divided over two gloo ranks: the per-range answers,
+    gathered in rank order, are the undivided answer bit for bit."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from oracle import oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + os.getpid() % 1000
+    world = 2
+    procs = [ctx.Process(target=_forward_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    cfg = bench.workload_config("small")
+    ph, qs = bench.make_inputs(cfg, 0)
+    idx, _d2, cnt, r2 = oracle.KdTree(ph.pos).knn(qs.pos, cfg["k"], cfg["r_max"])
+    rad = oracle.radiance_fp64(ph.pos, ph.pow, qs.pos, qs.nrm, idx, cnt, cfg["k"], cfg["r_max"], cfg["filter"])
+    for rank in range(world):
+        g_idx, g_cnt, g_r2, g_rad = out[rank]
+        assert np.array_equal(g_idx.view(np.uint32), idx)
+        assert np.array_equal(g_cnt.view(np.uint32), cnt)
+        assert np.array_equal(g_r2.view(np.uint32), r2.view(np.uint32))
+        assert np.array_equal(g_rad.view(np.uint64), rad.view(np.uint64))
 
 
 def _adjoint_worker(rank, world, port, q):
