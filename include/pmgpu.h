@@ -73,6 +73,7 @@ enum { PM_ORDER_SORTED = 0, PM_ORDER_AS_GIVEN = 1 };
 #define PM_DEVERR_STACK 0x1u     /* traversal stack overflow (query result invalid) */
 #define PM_DEVERR_NONFINITE 0x2u /* non-finite photon position at build */
 #define PM_DEVERR_QNONFINITE 0x4u/* non-finite query position */
+#define PM_DEVERR_WAIT 0x8u      /* a bounded inter-block wait gave up (that call's results are invalid) */
 
 typedef struct pm_map pm_map;
 
@@ -112,7 +113,9 @@ PM_API pm_status pm_create(pm_map** out, uint32_t max_photons, const float* aabb
 PM_API pm_status pm_destroy(pm_map* map);
 
 /* Routes this handle's device allocations through alloc/free (NULL, NULL
- * restores cudaMalloc/cudaFree).  Must be set before the first build. */
+ * restores cudaMalloc/cudaFree).  Must be set before the first build.  Blocks
+ * must be at least 16-byte aligned (cudaMalloc gives 256); a misaligned block
+ * is freed again and the call fails with PM_ERR_INVALID. */
 PM_API pm_status pm_set_allocator(pm_map* map, pm_alloc_fn alloc, pm_free_fn free_fn, void* user);
 
 /* k-buffer layouts of the query kernel. */

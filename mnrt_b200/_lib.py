@@ -18,7 +18,7 @@ PM_MODE_EXACT, PM_MODE_ZHOU_COMPAT, PM_MODE_ICUT = 0, 1, 2
 PM_ORDER_SORTED, PM_ORDER_AS_GIVEN = 0, 1
 PM_MAX_K = 128
 PM_NOALLOC_MAX_QUERIES = 262144
-PM_DEVERR_STACK, PM_DEVERR_NONFINITE, PM_DEVERR_QNONFINITE = 0x1, 0x2, 0x4
+PM_DEVERR_STACK, PM_DEVERR_NONFINITE, PM_DEVERR_QNONFINITE, PM_DEVERR_WAIT = 0x1, 0x2, 0x4, 0x8
 PM_KBUF_HEAP, PM_KBUF_GROUP, PM_KBUF_WIDE = 0, 1, 2
 
 FILTERS = {"box": PM_FILTER_BOX, "cone": PM_FILTER_CONE, "epanechnikov": PM_FILTER_EPANECHNIKOV}

@@ -52,7 +52,7 @@ struct pm_map {
     DevBuf stats;           // query counters (profiling level 2)
     // backward (pm_query_backward): pair sort, per-query records, segments,
     // FP64 running sums, and the forward outputs when the kNN is recomputed
-    DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, qr2, qcnt, seg_start, seg_end, acc;
+    DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, seg_start, seg_end, acc;
     DevBuf rnbr, rcnt, rr2, rrad;
     DevBuf gnrm, gest;        // pm_gather_for: flipped normals, estimates
     // PM_MODE_ZHOU_COMPAT: node radius estimates of the current tree, kept
@@ -119,6 +119,8 @@ void buf_free(pm_map* m, DevBuf& b) {
     b.bytes = 0;
 }
 
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 pm_status buf_ensure(pm_map* m, DevBuf& b, size_t bytes, const char* name) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return PM_OK;
@@ -127,6 +129,11 @@ pm_status buf_ensure(pm_map* m, DevBuf& b, size_t bytes, const char* name) {
     if (m->alloc) {
         if (m->alloc(&p, bytes, m->alloc_user) != 0 || !p)
             return fail(m, PM_ERR_OOM, "allocation of %zu bytes for %s failed (caller allocator)", bytes, name);
+        if (!aligned16(p)) {   // float4 records and 64-bit scan words need it
+            if (m->free_fn) m->free_fn(p, m->alloc_user);
+            return fail(m, PM_ERR_INVALID, "the caller allocator returned a block for %s that is not 16-byte aligned",
+                        name);
+        }
     } else {
         const cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) {
@@ -142,7 +149,6 @@ pm_status buf_ensure(pm_map* m, DevBuf& b, size_t bytes, const char* name) {
 
 template <class T> T* P(const DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
 
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // Query counts stay below 2^31: slot, round and grid arithmetic in the
 // kernels is 32-bit.
@@ -181,7 +187,7 @@ pm_status ensure_photon_capacity(pm_map* m, uint32_t n, cudaStream_t st) {
     ENSURE(wfirst, cap * sizeof(uint32_t));
     ENSURE(wchild, (cap + 1) * 2 * sizeof(ChildSlot));
     ENSURE(wroot, sizeof(ChildSlot));
-    ENSURE(wscan, (scan_scratch_words((uint32_t)cap) + 2) * sizeof(uint32_t));
+    ENSURE(wscan, wide_scan_words((uint32_t)cap) * sizeof(uint32_t));
     ENSURE(rootmark, (cap + 1) * sizeof(uint32_t));
 #undef ENSURE
     m->cap_photons = (uint32_t)cap;
@@ -325,7 +331,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wcnt, &m->wfirst,
                      &m->wchild, &m->wroot, &m->wscan, &m->rootmark, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
                      &m->qscratch, &m->counter, &m->fixq, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
-                     &m->bscratch, &m->qrec, &m->qr2, &m->qcnt, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
+                     &m->bscratch, &m->qrec, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
                      &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
                      &m->ic_normal, &m->ic_est, &m->ic_exact, &m->ic_coarse, &m->ic_fin, &m->ic_work0, &m->ic_work1,
@@ -639,9 +645,7 @@ static pm_status ensure_bwd_capacity(pm_map* m, uint32_t chunk_q, uint32_t k, bo
     ENSURE(bvals0, pc * sizeof(uint32_t));
     ENSURE(bvals1, pc * sizeof(uint32_t));
     ENSURE(bscratch, bwd_sort_scratch_words(pc) * sizeof(uint32_t));
-    ENSURE(qrec, qc * sizeof(double4));
-    ENSURE(qr2, qc * sizeof(double));
-    ENSURE(qcnt, qc * sizeof(uint32_t));
+    ENSURE(qrec, qc * sizeof(BwdQuery));
     ENSURE(seg_start, (size_t)n * sizeof(uint32_t));
     ENSURE(seg_end, (size_t)n * sizeof(uint32_t));
     if (chunked) ENSURE(acc, (size_t)n * 6 * sizeof(double));
@@ -700,7 +704,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     a.n = m->n; a.k = k; a.r_max = desc->r_max; a.filter = desc->filter;
     a.cone_k = desc->filter == PM_FILTER_CONE ? desc->cone_k : 1.0f;
     a.min_found = desc->min_found;
-    a.qrec = P<double4>(m->qrec); a.qr2 = P<double>(m->qr2); a.qcnt = P<uint32_t>(m->qcnt);
+    a.qrec = P<BwdQuery>(m->qrec);
     a.keys = nullptr; a.vals = nullptr;
     a.nbr = nullptr; a.count_in = nullptr; a.order = nullptr;
     BwdBuffers b;
@@ -1285,6 +1289,7 @@ pm_status batch_upload_queries(pm_batch* b, const pm_query_desc* descs, const ui
         q.r2max = descs[i].r_max * descs[i].r_max;
         q.filter = descs[i].filter;
         q.cone_k = descs[i].filter == PM_FILTER_CONE ? descs[i].cone_k : 1.0f;
+        q.norm_c = filter_norm_const(q.filter, q.cone_k);
         nbr += (uint64_t)q.q_n * q.k;
         kmax = q.k > kmax ? q.k : kmax;
     }
@@ -1314,9 +1319,11 @@ pm_status batch_build_device(pm_batch* b, const float* d_pos4, const float* d_po
                                    P<BatchGeom>(b->geom), P<MapHeader>(m->hdr), bb.keys[0], bb.vals[0], st);
     uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
     uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
-    const int cur = n > 1 ? radix_sort_pairs(keys, vals, n, 48 + map_id_bits(maps), bb.scratch, st, &nl) : 0;
+    const SortGather g{pos, pw, format, P<float4>(m->pos), P<float4>(m->pow), P<uint32_t>(m->inv)};
+    const int cur = n > 1 ? radix_sort_pairs(keys, vals, n, 48 + map_id_bits(maps), bb.scratch, st, &nl, &g) : 0;
     nl += build_from_sorted(pos, pw, n, format, m->leaf_size, keys[cur], vals[cur], P<float4>(m->pos),
-                            P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes), P<MapHeader>(m->hdr), bb, st);
+                            P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes), P<MapHeader>(m->hdr), bb, st,
+                            n > 1);
     nl += batch_roots(P<uint32_t>(b->ph_off), maps, n, m->leaf_size, P<float4>(m->pos), P<Node>(m->nodes), bb,
                       P<BatchGeom>(b->geom), st);
     nl += batch_wide(n, maps, P<Node>(m->nodes), P<uint32_t>(m->parent), P<MapHeader>(m->hdr), P<uint32_t>(m->rootmark),

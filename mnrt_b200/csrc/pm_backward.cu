@@ -17,13 +17,13 @@
 //
 // Scatter without float atomics, deterministic by construction:
 //   1. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
-//                   -> per-query record (g * norm, G), count, r^2
-//   2. k_bwd_pairs  one (photon tree position, pair id) key-value per
+//                   -> per-query record (g * norm, G, r^2, position, normal),
+//                   and one (photon tree position, pair id) key-value per
 //                   neighbour slot; empty slots get the sentinel key n
-//   3. stable LSD radix sort by photon (pair ids of one photon stay in
+//   2. stable LSD radix sort by photon (pair ids of one photon stay in
 //      query order)
-//   4. k_bwd_bounds segment [start, end) of every photon in the sorted array
-//   5. k_bwd_reduce thread per photon: walks its segment in order and sums
+//   3. k_bwd_bounds segment [start, end) of every photon in the sorted array
+//   4. k_bwd_reduce thread per photon: walks its segment in order and sums
 //                   the FP64 contributions; the running sum carries across
 //                   query chunks, so chunked and single-pass runs give the
 //                   same bits
@@ -75,8 +75,12 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 
 // One warp per query of the chunk, taken in Hilbert order when a.order is
 // set: neighbouring warps then gather neighbouring photons, which L1 and L2
-// serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records stay at the caller's
-// index, so the results do not depend on the order.
+// serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records and pairs stay at the
+// caller's index, so the results do not depend on the order.  The warp also
+// writes the query's k (photon tree position, pair id) keys and values for
+// the sort by photon (empty slots and queries without gradient get the
+// sentinel key n, which sorts after every photon): the neighbour rows and
+// the inverse permutation are read once, here.
 __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -103,48 +107,44 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     if (cnt == k) r2 = dist2_d(a.pos[a.inv[row[k - 1]]], qp);
     const bool active = cnt > 0 && cnt >= a.min_found && r2 > 0.0 && isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
     double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
-    if (active) {
-        for (uint32_t j = lane; j < cnt; j += 32) {
+    const uint64_t pair0 = (uint64_t)ql * k;
+    for (uint32_t j = lane; j < k; j += 32) {
+        uint32_t key = a.n;
+        if (active && j < cnt) {
             const uint32_t p = a.inv[row[j]];
+            key = p;
             const float4 pp = a.pos[p], pw = a.pow[p];
-            if (!front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) continue;
-            double w, dwd, dwr;
-            weight_terms(a.filter, dist2_d(pp, qp), r2, (double)a.cone_k, w, dwd, dwr);
-            S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
-            T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
+            if (front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
+                double w, dwd, dwr;
+                weight_terms(a.filter, dist2_d(pp, qp), r2, (double)a.cone_k, w, dwd, dwr);
+                S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
+                T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
+            }
         }
+        a.keys[pair0 + j] = key;
+        a.vals[pair0 + j] = (uint32_t)(pair0 + j);
     }
     S0 = warp_sum_d(S0); S1 = warp_sum_d(S1); S2 = warp_sum_d(S2);
     T0 = warp_sum_d(T0); T1 = warp_sum_d(T1); T2 = warp_sum_d(T2);
     if (lane != 0) return;
-    double4 rec = make_double4(0.0, 0.0, 0.0, 0.0);
+    BwdQuery rec;
+    rec.gx = rec.gy = rec.gz = rec.G = 0.0;
+    rec.r2 = active ? r2 : 0.0;
+    rec.qx = qp.x; rec.qy = qp.y; rec.qz = qp.z;
+    rec.nx = qn.x; rec.ny = qn.y; rec.nz = qn.z;
     if (active) {
         const float4 g = a.grad[q];
         const double nrm = norm_of(a.filter, r2, (double)a.cone_k);
-        rec.x = (double)g.x * nrm;
-        rec.y = (double)g.y * nrm;
-        rec.z = (double)g.z * nrm;
+        rec.gx = (double)g.x * nrm;
+        rec.gy = (double)g.y * nrm;
+        rec.gz = (double)g.z * nrm;
         if (cnt == k) {
             const double dn = -nrm / r2;
-            rec.w = (double)g.x * (dn * S0 + nrm * T0) + (double)g.y * (dn * S1 + nrm * T1) +
+            rec.G = (double)g.x * (dn * S0 + nrm * T0) + (double)g.y * (dn * S1 + nrm * T1) +
                     (double)g.z * (dn * S2 + nrm * T2);
         }
     }
     a.qrec[ql] = rec;
-    a.qr2[ql] = active ? r2 : 0.0;
-    a.qcnt[ql] = active ? cnt : 0u;
-}
-
-// One thread per neighbour slot of the chunk.
-__global__ void k_bwd_pairs(BwdArgs a, uint32_t nq_chunk) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t total = (uint64_t)nq_chunk * a.k;
-    if (i >= total) return;
-    const uint32_t ql = (uint32_t)(i / a.k), j = (uint32_t)(i % a.k);
-    uint32_t key = a.n;   // sentinel: sorts after every photon
-    if (j < a.qcnt[ql]) key = a.inv[a.nbr[i]];
-    a.keys[i] = key;
-    a.vals[i] = (uint32_t)i;
 }
 
 // Segment bounds of every photon in the sorted keys (start = end = 0 when
@@ -179,25 +179,22 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
         for (uint32_t i = b; i < e; ++i) {
             const uint32_t v = sorted_vals[i];
             const uint32_t ql = v / k, j = v % k;
-            const uint32_t q = q0 + ql;
-            const double4 rec = a.qrec[ql];
-            const double r2 = a.qr2[ql];
+            const BwdQuery rec = a.qrec[ql];
+            const double r2 = rec.r2;
             if (!(r2 > 0.0)) continue;
-            const float4 qp = a.qpos[q];
-            const float4 qn = a.qnrm[q];
-            const double dx = (double)pp.x - (double)qp.x, dy = (double)pp.y - (double)qp.y,
-                         dz = (double)pp.z - (double)qp.z;
+            const double dx = (double)pp.x - (double)rec.qx, dy = (double)pp.y - (double)rec.qy,
+                         dz = (double)pp.z - (double)rec.qz;
             const double d2 = dx * dx + dy * dy + dz * dz;
             double coef = 0.0;
-            if (front_rn(qn.x, qn.y, qn.z, dir)) {
+            if (front_rn(rec.nx, rec.ny, rec.nz, dir)) {
                 double w, dwd, dwr;
                 weight_terms(a.filter, d2, r2, (double)a.cone_k, w, dwd, dwr);
-                g0 += w * rec.x;
-                g1 += w * rec.y;
-                g2 += w * rec.z;
-                coef = (rec.x * pw.x + rec.y * pw.y + rec.z * pw.z) * dwd;
+                g0 += w * rec.gx;
+                g1 += w * rec.gy;
+                g2 += w * rec.gz;
+                coef = (rec.gx * pw.x + rec.gy * pw.y + rec.gz * pw.z) * dwd;
             }
-            if (j == k - 1) coef += rec.w;   // the k-th neighbour sets r^2 of q
+            if (j == k - 1) coef += rec.G;   // the k-th neighbour sets r^2 of q
             x0 += 2.0 * coef * dx;
             x1 += 2.0 * coef * dy;
             x2 += 2.0 * coef * dz;
@@ -233,8 +230,7 @@ int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first,
     if (nq_chunk > 0) {
         const uint32_t warps_per_block = 8;
         k_bwd_prep<<<(nq_chunk + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
-        k_bwd_pairs<<<(uint32_t)((pairs + 255) / 256), 256, 0, st>>>(x, nq_chunk);
-        nl += 2;
+        ++nl;
     }
     uint32_t* keys[2] = {b.keys[0], b.keys[1]};
     uint32_t* vals[2] = {b.vals[0], b.vals[1]};

@@ -34,6 +34,10 @@ constexpr int kBoundsThreads = 256;
 constexpr int kBoundsBlocksMax = 1184;   // 8 per SM on 148 SMs
 constexpr int kLeafBoxBlocks = 1184;     // 8 blocks of 8 warps per SM, grid-stride over the nodes
 
+// The wide tree's child-count scan in WideBuffers::scratch: ticket, total,
+// one uint64 look-back word per tile of 256 nodes.
+size_t wide_scan_words(uint32_t n) { return 2 + 2 * (size_t)((n + 255) / 256); }
+
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -161,6 +165,8 @@ __device__ __forceinline__ int delta(const uint64_t* __restrict__ keys, int64_t 
     return 64 + __clz((uint32_t)i ^ (uint32_t)j);
 }
 
+// Thread per radix-tree node i (Karras 2012): direction, range [first, last],
+// split, and the keep flag (more than leaf_size photons).
 __global__ void k_radix_tree(const uint64_t* __restrict__ keys, uint32_t n, uint32_t leaf_size,
                              uint32_t* __restrict__ kfirst, uint32_t* __restrict__ klast,
                              uint32_t* __restrict__ ksplit, uint32_t* __restrict__ kkeep) {
@@ -360,18 +366,23 @@ void scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr, cudaStream_
     k_scale_flux<<<blocks, 256, 0, st>>>(pw, n, scale, hdr);
 }
 
-// Everything after the sort: photons into tree order, radix tree, compaction
-// into 64-byte nodes, refit.  keys/vals are the sorted (code, caller index)
-// pairs; any code whose prefix separates groups (e.g. a map id in the top
-// bits) yields one subtree per group.
+// Everything after the sort: photons into tree order (unless the sort's last
+// pass already moved them: gathered), radix tree, compaction into 64-byte
+// nodes, refit.  keys/vals are the sorted (code, caller index) pairs; any
+// code whose prefix separates groups (e.g. a map id in the top bits) yields
+// one subtree per group.
 int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
                       const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
-                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st) {
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered) {
     const uint32_t tb = 256;
     if (n > 0) {
-        k_gather<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, in_pow, vals, n, format, out_pos, out_pow, inv);
+        if (!gathered) k_gather<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, in_pow, vals, n, format, out_pos, out_pow, inv);
+        const int ng = gathered ? 0 : 1;
         if (n > 1) {
             const uint32_t ni = n - 1, gi = (ni + tb - 1) / tb;
+            // the keep flags' exclusive scan (a single-pass scan with look-back inside
+            // k_radix_tree measured 87 us against 46 + 13 us: one slow tile holds up
+            // every later one, where separate kernels let blocks finish independently)
             k_radix_tree<<<gi, tb, 0, st>>>(keys, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep);
             uint32_t* total = bb.scratch + sort_scratch_words(n);
             const int ns = exclusive_scan(bb.kkeep, bb.krank, ni, total + 1, total, st);
@@ -379,7 +390,7 @@ int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, in
                                       total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
             k_leaf_boxes<<<kLeafBoxBlocks, 256, 0, st>>>(out_pos, nodes, hdr);
             k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
-            return 6 + ns;
+            return ng + 5 + ns;
         }
     }
     k_emit<<<1, 32, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank, nullptr,
@@ -404,11 +415,13 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
         const uint32_t tb = 256;
         k_morton<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, n, hdr, bb.keys[0], bb.vals[0]);
         ++nl;
-        cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl);
+        // the last pass moves the photons into tree order (n >= 2; one photon is not sorted)
+        const SortGather g{in_pos, in_pow, format, out_pos, out_pow, inv};
+        cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl, n > 1 ? &g : nullptr);
     }
     if (sort_done) cudaEventRecord(sort_done, st);
     return nl + build_from_sorted(in_pos, in_pow, n, format, leaf_size, keys[cur], vals[cur], out_pos, out_pow, inv,
-                                  nodes, hdr, bb, st);
+                                  nodes, hdr, bb, st, n > 1);
 }
 
 
@@ -416,22 +429,6 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
 
 __device__ __forceinline__ bool is_marked_root(const uint32_t* rootmark, uint32_t id) {
     return id == 1 || (rootmark && rootmark[id]);
-}
-
-// wflag[t] = 1 when compacted node t + 1 lies a multiple of kWideLevels below
-// its root (node 1, or a node marked in rootmark).
-__global__ void k_wide_flags(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ rootmark,
-                             const MapHeader* __restrict__ hdr, uint32_t bound, uint32_t* __restrict__ wflag) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= bound) return;
-    const uint32_t m = hdr->num_nodes;
-    uint32_t f = 0;
-    if (t < m) {
-        uint32_t c = t + 1, d = 0;
-        while (!is_marked_root(rootmark, c) && d < 4096) { c = parent[c] >> 1; ++d; }
-        f = (d % kWideLevels == 0) ? 1u : 0u;
-    }
-    wflag[t] = f;
 }
 
 // Warp-cooperative expansion of wide node `id`: the slots reached by expanding
@@ -484,18 +481,33 @@ __device__ uint32_t wide_expand_warp(const Node* __restrict__ nodes, const uint3
     return count;
 }
 
-// Warp per 32 consecutive compacted nodes: the child count of every wide
-// node among them (0 for the others).
-__global__ void k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
-                             const uint32_t* __restrict__ wflag, const MapHeader* __restrict__ hdr, uint32_t bound,
-                             uint32_t* __restrict__ wcnt) {
+// Block of 8 warps per 256 consecutive compacted nodes, taken by ticket: each
+// lane marks its node as wide when the node lies a multiple of kWideLevels
+// below its root (node 1, or a node marked in rootmark), the warps expand
+// their wide nodes to count the children, and the block's exclusive scan of
+// the counts plus a decoupled look-back gives every wide node its first
+// child slot (one launch for flags, counts and scan).  scan: [0] ticket, [1]
+// total child slots (last tile), look-back words from word 2; cleared before.
+__global__ void __launch_bounds__(256) k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ parent,
+                                                     const uint32_t* __restrict__ rootmark,
+                                                     const MapHeader* __restrict__ hdr, uint32_t bound,
+                                                     uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
+                                                     uint32_t* __restrict__ wfirst, uint32_t* scan, uint32_t* err) {
     __shared__ uint32_t s_buf[8][64];
+    __shared__ uint32_t s_tile, s_warp[32];
+    __shared__ uint64_t s_before;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&scan[0], 1u);
+    __syncthreads();
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    const uint32_t t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
-    if (t0 >= bound) return;
+    const uint32_t t0 = s_tile * 256u + wib * 32u;
     const uint32_t m = hdr->num_nodes;
     const uint32_t t = t0 + lane;
-    const bool wide = t < m && t < bound && wflag[t];
+    bool wide = false;
+    if (t < m && t < bound) {
+        uint32_t c = t + 1, d = 0;
+        while (!is_marked_root(rootmark, c) && d < 4096) { c = parent[c] >> 1; ++d; }
+        wide = d % kWideLevels == 0;
+    }
     uint32_t mine = 0;
     uint32_t todo = __ballot_sync(0xffffffffu, wide);
     while (todo) {
@@ -505,15 +517,38 @@ __global__ void k_wide_count(const Node* __restrict__ nodes, const uint32_t* __r
         const uint32_t c = wide_expand_warp(nodes, rootmark, t0 + b + 1u, lane, s_buf[wib], slot, state);
         if (lane == b) mine = c;
     }
-    if (t < bound) wcnt[t] = mine;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(mine, s_warp, total);
+    if (threadIdx.x < 32) {
+        const uint64_t b = warp_lookback_exclusive(reinterpret_cast<uint64_t*>(scan + 2), s_tile, total, err);
+        if (threadIdx.x == 0) s_before = b;
+    }
+    __syncthreads();
+    if (t < bound) {
+        wflag[t] = wide ? 1u : 0u;
+        wcnt[t] = mine;
+        wfirst[t] = (uint32_t)s_before + ex;
+    }
+    if (threadIdx.x == 0 && s_tile + 1 == (bound + 255u) / 256u) scan[1] = (uint32_t)s_before + total;
 }
 
+// Warp per 32 consecutive compacted nodes: every wide node's child slots;
+// thread 0 of block 0 also writes the traversal's start slot (the
+// super-root's slot, pointing at the root wide node).
 __global__ void k_wide_emit(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
                             const uint32_t* __restrict__ wflag, const uint32_t* __restrict__ wcnt,
                             const uint32_t* __restrict__ wfirst, const MapHeader* __restrict__ hdr, uint32_t bound,
-                            ChildSlot* __restrict__ wchild) {
+                            ChildSlot* __restrict__ wchild, ChildSlot* __restrict__ wroot) {
     __shared__ uint32_t s_buf[8][64];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ChildSlot s = nodes[0].c[0];
+        if (s.ref != kInvalid && s.cnt == 0) {
+            s.ref = wfirst[0];
+            s.cnt = kWideFlag | wcnt[0];
+        }
+        *wroot = s;
+    }
     const uint32_t t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
     if (t0 >= bound) return;
     const uint32_t m = hdr->num_nodes;
@@ -537,32 +572,18 @@ __global__ void k_wide_emit(const Node* __restrict__ nodes, const uint32_t* __re
     }
 }
 
-// The traversal's start slot: the super-root's slot, pointing at the wide node.
-__global__ void k_wide_root(const Node* __restrict__ nodes, const uint32_t* __restrict__ wcnt,
-                            const uint32_t* __restrict__ wfirst, ChildSlot* __restrict__ wroot) {
-    ChildSlot s = nodes[0].c[0];
-    if (s.ref != kInvalid && s.cnt == 0) {
-        s.ref = wfirst[0];
-        s.cnt = kWideFlag | wcnt[0];
-    }
-    *wroot = s;
-}
-
 int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint32_t* rootmark, MapHeader* hdr,
                const WideBuffers& wb, cudaStream_t st) {
-    int nl = 0;
     const uint32_t bound = n > 1 ? n - 1 : 1;   // internal nodes are at most n - 1
-    const uint32_t tb = 128, grid = (bound + tb - 1) / tb;
     const uint32_t wgrid = (bound + 32u * 8u - 1u) / (32u * 8u);   // 8 warps per block, 32 nodes per warp
     if (n > 1) {
-        k_wide_flags<<<grid, tb, 0, st>>>(parent, rootmark, hdr, bound, wb.wflag);
-        k_wide_count<<<wgrid, 256, 0, st>>>(nodes, rootmark, wb.wflag, hdr, bound, wb.wcnt);
-        nl += 2 + exclusive_scan(wb.wcnt, wb.wfirst, bound, wb.scratch + 1, wb.scratch, st);
-        k_wide_emit<<<wgrid, 256, 0, st>>>(nodes, rootmark, wb.wflag, wb.wcnt, wb.wfirst, hdr, bound, wb.wchild);
-        ++nl;
+        cudaMemsetAsync(wb.scratch, 0, wide_scan_words(n) * sizeof(uint32_t), st);
+        k_wide_count<<<wgrid, 256, 0, st>>>(nodes, parent, rootmark, hdr, bound, wb.wflag, wb.wcnt, wb.wfirst,
+                                            wb.scratch, &hdr->errors);
     }
-    k_wide_root<<<1, 1, 0, st>>>(nodes, wb.wcnt, wb.wfirst, wb.wroot);
-    return nl + 1;
+    k_wide_emit<<<n > 1 ? wgrid : 1, 256, 0, st>>>(nodes, rootmark, wb.wflag, wb.wcnt, wb.wfirst, hdr,
+                                                  n > 1 ? bound : 0, wb.wchild, wb.wroot);
+    return n > 1 ? 2 : 1;
 }
 
 }  // namespace pm

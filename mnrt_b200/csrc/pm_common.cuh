@@ -19,6 +19,7 @@ constexpr uint32_t kInvalid = 0xffffffffu;
 constexpr uint32_t kErrStack = 0x1u;
 constexpr uint32_t kErrNonFinite = 0x2u;
 constexpr uint32_t kErrQueryNonFinite = 0x4u;
+constexpr uint32_t kErrWait = 0x8u;        // a bounded wait gave up (the launch's results are invalid)
 
 // Child slot of a tree node: refitted AABB of the child's photons plus a
 // reference.  cnt > 0: leaf holding photons [ref, ref + cnt) in tree order;

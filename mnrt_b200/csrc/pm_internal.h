@@ -9,13 +9,116 @@
 
 namespace pm {
 
+// ------------------------------------------------ device-side helpers --
+
+// Exclusive scan of one value per thread over the block (blockDim.x a
+// multiple of 32, at most 1024); total = the block's sum.  s_warp: 32 words
+// of shared memory.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = (lane < nwarps) ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nwarps) s_warp[lane] = w;
+    }
+    __syncthreads();
+    total = s_warp[nwarps - 1];
+    const uint32_t warp_prefix = warp ? s_warp[warp - 1] : 0u;
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+// Relaxed 64-bit loads and stores of the look-back words (status and value
+// in one word, so no other data is ordered by them).
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Polls of one look-back word before a wait gives up (sets kErrWait).
+constexpr uint32_t kLookbackWaitLimit = 1u << 22;
+
+// Decoupled look-back over one value per tile (D. Merrill and M. Garland,
+// "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016), called
+// by all 32 lanes of one warp of the block that holds tile `tile`.  The tile
+// publishes its aggregate; lane l then reads the word of tile base - l, 32
+// earlier tiles per step, waits until all 32 have published, and adds their
+// values up to the nearest one holding an inclusive prefix (or all 32
+// aggregates, then the next 32).  The tile publishes its own inclusive
+// prefix; every lane returns the exclusive prefix.  words: one uint64 per
+// tile, cleared before the launch; status in bits 62-63 (1 aggregate, 2
+// inclusive prefix).  Tiles must be taken in the order blocks start (an
+// atomic ticket), so that a tile only waits for tiles whose blocks are
+// running and publish their aggregates before they wait themselves.
+__device__ __forceinline__ uint64_t warp_lookback_exclusive(uint64_t* words, uint32_t tile, uint64_t agg,
+                                                            uint32_t* err) {
+    constexpr uint64_t kAgg = 1ull << 62, kPrefix = 2ull << 62, kValue = (1ull << 62) - 1ull;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(words, kPrefix | agg);
+        return 0;
+    }
+    if (lane == 0) st_relaxed_u64(words + tile, kAgg | agg);
+    uint64_t before = 0;
+    int64_t base = (int64_t)tile - 1;
+    uint32_t polls = 0;
+    for (;;) {
+        const int64_t t = base - (int64_t)lane;
+        uint64_t w = t >= 0 ? ld_relaxed_u64(words + t) : kPrefix;   // before tile 0: a zero prefix
+        bool gave_up = false;
+        while (__any_sync(0xffffffffu, (w >> 62) == 0)) {
+            if (++polls > kLookbackWaitLimit) { gave_up = true; break; }   // never expected
+            if (polls > 32) __nanosleep(64);
+            if ((w >> 62) == 0) w = ld_relaxed_u64(words + t);
+        }
+        if (gave_up) {
+            if (lane == 0 && err) atomicOr(err, kErrWait);
+            break;
+        }
+        const uint32_t pm = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+        uint64_t v = w & kValue;
+        if (pm && lane > (uint32_t)(__ffs(pm) - 1)) v = 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        before += v;
+        if (pm) break;
+        base -= 32;
+    }
+    if (lane == 0) st_relaxed_u64(words + tile, kPrefix | (before + agg));
+    return before;
+}
+
 // pm_sort.cu
 size_t scan_scratch_words(uint32_t n);
 int exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch, uint32_t* total_out,
                    cudaStream_t st);
 size_t sort_scratch_words(uint32_t n);
+struct SortGather {   // the last pass moves the photons, not the values (n >= 2 only)
+    const float4* in_pos;
+    const float4* in_pow;
+    int format;           // PM_PHOTONS_*: 0 = reference angles, converted to the packed direction
+    float4* out_pos;      // tree order: xyz, w = caller index bits
+    float4* out_pow;      // tree order: rgb, w = packed direction
+    uint32_t* inv;        // caller index -> tree position
+};
 int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
-                     cudaStream_t st, int* launches = nullptr);
+                     cudaStream_t st, int* launches = nullptr, const SortGather* gather = nullptr);
 int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
                        cudaStream_t st, int* launches = nullptr);
 
@@ -37,6 +140,7 @@ struct __align__(16) BatchQuery {
     uint32_t k, min_found;
     float r2max, rmax, cone_k;
     int filter;
+    double norm_c;         // filter normalisation constant (the estimate's factor is norm_c / r^2)
 };
 
 // Device buffers describing one built map (the build writes them, the
@@ -74,11 +178,12 @@ struct WideBuffers {
     uint32_t* wfirst;      // scan of wcnt: first child slot
     ChildSlot* wchild;     // child slots of all wide nodes
     ChildSlot* wroot;      // start slot of the wide traversal
-    uint32_t* scratch;     // scan scratch (total at [0])
+    uint32_t* scratch;     // child-count scan: ticket, total, look-back words (wide_scan_words)
 };
 
 // pm_build.cu
 size_t build_bytes_needed(uint32_t n);
+size_t wide_scan_words(uint32_t n);   // WideBuffers::scratch
 // Returns the number of kernels launched; sort_done (if set) is recorded on
 // the stream right after the radix sort.
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
@@ -89,7 +194,7 @@ int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint
                const WideBuffers& wb, cudaStream_t st);
 int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
                       const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
-                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st);
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered = false);
 
 // pm_query.cu
 struct QueryParams {
@@ -125,6 +230,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
 int query_bruteforce(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                       uint32_t nq, const QueryOutputs& out, cudaStream_t st);
 int query_smem_bytes_per_warp(uint32_t k);
+double filter_norm_const(int filter, float cone_k);
 
 int query_knn_batch(const MapView& m, const BatchQuery* bq, const BatchGeom* bg, uint32_t kmax, const float4* qpos,
                     const float4* qnrm, const uint32_t* order, const uint64_t* qkeys, uint32_t nq,
@@ -192,6 +298,17 @@ int merge_scatter(const float4* pos, const float4* pw, const uint32_t* flags, co
 int scale_rgb(float4* pw, uint32_t n, float scale, cudaStream_t st);
 
 // pm_backward.cu
+// Per-query record of the adjoint, 64 bytes: everything the per-photon pass
+// needs about one query in one aligned load.
+struct __align__(16) BwdQuery {
+    double gx, gy, gz;        // dL/dE * norm per channel
+    double G;                 // the k-th neighbour's r^2 path (0 unless k were found)
+    double r2;                // r^2 of the filter (0 = the query carries no gradient)
+    float qx, qy, qz;         // position
+    float nx, ny, nz;         // normal
+};
+static_assert(sizeof(BwdQuery) == 64, "one 64-byte record per query");
+
 struct BwdArgs {
     const float4* pos;        // tree order
     const float4* pow;
@@ -206,9 +323,7 @@ struct BwdArgs {
     int filter;
     float cone_k;
     uint32_t min_found;
-    double4* qrec;            // per chunk query: g * norm (xyz), G (w)
-    double* qr2;              // per chunk query: r^2 (0 = no gradient)
-    uint32_t* qcnt;           // per chunk query: neighbours carrying gradient
+    BwdQuery* qrec;           // per chunk query: the record the per-photon pass reads
     uint32_t* keys;           // pair keys / values (set by backward_chunk)
     uint32_t* vals;
     const uint32_t* order;    // the chunk's queries in Hilbert order (chunk-local ids), or nullptr

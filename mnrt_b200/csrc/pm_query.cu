@@ -27,6 +27,7 @@
 //     same bits.
 #include "pm_internal.h"
 
+
 namespace pm {
 
 constexpr uint32_t kFull = 0xffffffffu;
@@ -68,6 +69,9 @@ struct KnnArgs {
     const uint64_t* qkeys;    // batch: sorted query keys, map id from bit kBatchQueryMapShift up
     const BatchGeom* bgeom;   // batch: per-map geometry (built)
     const BatchQuery* bq;     // batch: per-map query parameters
+    double norm_c;            // the filter's normalisation constant (filter_norm_const)
+    const ChildSlot* s_top;   // staged root children (shared memory) or nullptr
+    uint32_t top_first;       // wchild index of the staged children
 };
 
 // Counters of the group kernel, accumulated when KnnArgs::stats is set.
@@ -167,13 +171,6 @@ __device__ __forceinline__ double filter_r2(const float4* __restrict__ pos, bool
     return d2_64(qx, qy, qz, __ldg(pos + kth));
 }
 
-__device__ __forceinline__ double filter_norm(int filter, double r2, double cone_k) {
-    const double pi = 3.14159265358979323846;
-    if (filter == 1) return 1.0 / ((1.0 - 2.0 / (3.0 * cone_k)) * pi * r2);
-    if (filter == 2) return 2.0 / (pi * r2);
-    return 1.0 / (pi * r2);
-}
-
 __device__ __forceinline__ long long fixed_term(float w, float phi, float scale) {
     return __float2ll_rn(__fmul_rn(__fmul_rn(w, phi), scale));
 }
@@ -252,19 +249,22 @@ __device__ __forceinline__ void est_add64(const KnnArgs& a, uint32_t t, const Fi
 // channel must pass on its own (a channel whose flux sits in low-weight
 // neighbours, e.g. the k-th at weight zero, would otherwise slip through).
 // The unweighted sums are kept in 32 bits at 2^24 / max flux with every term
-// rounded up, which can only send more queries to FP64.
+// rounded up, which can only send more queries to FP64.  The comparison
+// 6 sum(w flux) < sum(flux) is exact in 64-bit integers: the weighted sums are
+// below 2^60 (6 times that below 2^63), the unweighted ones below 2^31.
 __device__ __forceinline__ bool est_needs_fp64(int filter, const EstAcc& acc) {
     if (filter == 0) return false;
-    const double k29 = 536870912.0;   // 2^29: the unweighted sums' scale to the weighted sums'
-    return 6.0 * (double)acc.c0 < (double)acc.f0 * k29 || 6.0 * (double)acc.c1 < (double)acc.f1 * k29 ||
-           6.0 * (double)acc.c2 < (double)acc.f2 * k29;
+    return 6ll * acc.c0 < (long long)((uint64_t)acc.f0 << 29) || 6ll * acc.c1 < (long long)((uint64_t)acc.f1 << 29) ||
+           6ll * acc.c2 < (long long)((uint64_t)acc.f2 << 29);
 }
 
-__device__ __forceinline__ float4 est_result(const EstAcc& acc, int filter, double r2, float cone_k, float scale,
-                                             uint32_t n) {
+// The estimate from the fixed-point sums: c / (r^2 scale) per unit of sum, c
+// the filter's normalisation constant (filter_norm_const, one FP64 division
+// per query).
+__device__ __forceinline__ float4 est_result(const EstAcc& acc, double r2, float scale, uint32_t n, double norm_c) {
     float4 rad = make_float4(0.0f, 0.0f, 0.0f, (float)n);
     if (scale > 0.0f) {
-        const double f = filter_norm(filter, r2, (double)cone_k) / (double)scale;
+        const double f = norm_c / __dmul_rn(r2, (double)scale);
         rad.x = __double2float_rn((double)acc.c0 * f);
         rad.y = __double2float_rn((double)acc.c1 * f);
         rad.z = __double2float_rn((double)acc.c2 * f);
@@ -332,7 +332,7 @@ __device__ void finish_query(const KnnArgs& a, uint64_t* h, uint32_t stride, uin
         }
         double r2d = (double)r2;
         if (est_needs_fp64(a.filter, acc)) r2d = est_fp64_heap(a, h, stride, hn, hn == k, kth, qx, qy, qz, nx, ny, nz, acc);
-        rad = est_result(acc, a.filter, r2d, a.cone_k, scale, hn);
+        rad = est_result(acc, r2d, scale, hn, a.norm_c);
     }
     a.out_rad[qo] = rad;
     if (a.out_r2) a.out_r2[qo] = r2;
@@ -910,7 +910,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
                 a.fix_list[atomicAdd(a.fix_count, 1u)] = slot;
             }
         }
-        rad = est_result(acc, a.filter, r2d, a.cone_k, scale, n);
+        rad = est_result(acc, r2d, scale, n, a.norm_c);
     }
     if (s == 0) {
         a.out_rad[qo] = rad;
@@ -927,7 +927,11 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
 // tests child i of a wide node, passing internal children are pushed with the
 // nearest on top, passing leaves are scanned in tree order (one photon per
 // lane).  Candidates go to buf as in the binary traversal.
-constexpr int kWideStack = 192;   // entries of 3 words: first child, child count, lower bound
+constexpr int kWideStack = 192;   // entries of 2 words: first child slot, stack_word(lower bound, child count)
+// Single-map wide instances stage the root wide node's child slots (the top
+// kWideLevels binary levels of the tree) in shared memory, once per block:
+// every query visits them first.
+constexpr int kTopBytes = 32 * (int)sizeof(ChildSlot);
 
 __device__ __forceinline__ void scan_leaf32(const KnnArgs& a, uint32_t ref, uint32_t cnt, float qx, float qy, float qz,
                                             uint32_t k, uint32_t C, uint64_t* buf, uint32_t& n, bool& selected,
@@ -951,18 +955,12 @@ __device__ __forceinline__ void scan_leaf32(const KnnArgs& a, uint32_t ref, uint
     __syncwarp();
 }
 
-// Lane holding the smallest v among the lanes in mask (ties: lowest lane).
-__device__ __forceinline__ uint32_t warp_argmin(float v, uint32_t mask, uint32_t lane) {
-    float bv = ((mask >> lane) & 1u) ? v : INFINITY;
-    uint32_t bl = ((mask >> lane) & 1u) ? lane : 32u;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        const float ov = __shfl_xor_sync(kFull, bv, o);
-        const uint32_t ol = __shfl_xor_sync(kFull, bl, o);
-        if (ov < bv || (ov == bv && ol < bl)) { bv = ov; bl = ol; }
-    }
-    return bl;
-}
+// Stack entry of the wide traversal: two words, the wide node's first child
+// slot and its lower bound with the 6 low mantissa bits replaced by the child
+// count (<= 32).  Clearing those bits rounds the non-negative bound toward
+// zero, so it stays a lower bound: a pop may visit a node the exact bound
+// would skip, never the reverse.
+__device__ __forceinline__ uint32_t stack_word(float lb, uint32_t kids) { return (__float_as_uint(lb) & ~63u) | kids; }
 
 __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float qy, float qz, uint32_t k, uint32_t C, uint64_t* buf,
                               uint32_t& n, bool& selected, float& thr, uint32_t* hist, uint32_t* stack, uint32_t lane,
@@ -976,7 +974,7 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         const float lb = box_lb(qx, qy, qz, lo, hi);
         if (!(selected ? lb <= thr : lb < thr)) return;
         if (cnt & kWideFlag) {
-            if (lane == 0) { stack[0] = ref; stack[1] = cnt & kWideCount; stack[2] = __float_as_uint(lb); }
+            if (lane == 0) { stack[0] = ref; stack[1] = stack_word(lb, cnt & kWideCount); }
             sp = 1;
             __syncwarp();
         } else if (cnt > 0) {
@@ -986,13 +984,23 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
     }
     while (sp > 0) {
         --sp;
-        const uint32_t first = stack[3 * sp], kids = stack[3 * sp + 1];
-        const float plb = __uint_as_float(stack[3 * sp + 2]);
+        const uint32_t first = stack[2 * sp], e1 = stack[2 * sp + 1];
+        const uint32_t kids = e1 & 63u;
+        const float plb = __uint_as_float(e1 & ~63u);
         __syncwarp();
         if (!(selected ? plb <= thr : plb < thr)) continue;
         float lo[3], hi[3];
         uint32_t ref = kInvalid, cnt = 0;
-        if (lane < kids) load_root(a.wchild + first + lane, lo, hi, ref, cnt);
+        if (lane < kids) {
+            if (first == a.top_first) {   // the root wide node: staged in shared memory
+                const float4* tp = reinterpret_cast<const float4*>(a.s_top + lane);
+                const float4 ta = tp[0], tb = tp[1];
+                lo[0] = ta.x; lo[1] = ta.y; lo[2] = ta.z; hi[0] = ta.w;
+                hi[1] = tb.x; hi[2] = tb.y; ref = __float_as_uint(tb.z); cnt = __float_as_uint(tb.w);
+            } else {
+                load_root(a.wchild + first + lane, lo, hi, ref, cnt);
+            }
+        }
         float lb = INFINITY;
         bool pass = false;
         if (ref != kInvalid) {
@@ -1007,17 +1015,17 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
             if (sp + (int)np > kWideStack) {
                 if (lane == 0) atomicOr(&a.hdr->errors, kErrStack);
             } else {
-                // A child whose box holds the query (lower bound 0) is the nearest,
-                // and the lowest such lane is what the reduction would pick: the
-                // shuffle reduction only runs when none does (7.29 -> 7.14 ms).
-                const uint32_t inside = __ballot_sync(kFull, ((intm >> lane) & 1u) && lb == 0.0f);
-                const uint32_t near = inside ? (uint32_t)(__ffs(inside) - 1) : warp_argmin(lb, intm, lane);
+                // The nearest passing child (smallest lower bound, ties to the
+                // lowest lane) goes on top: the bounds are non-negative, so their
+                // bits order as the values, and one warp min-reduction finds it.
+                const uint32_t lbb = ((intm >> lane) & 1u) ? __float_as_uint(lb) : 0xffffffffu;
+                const uint32_t mn = __reduce_min_sync(kFull, lbb);
+                const uint32_t near = (uint32_t)(__ffs(__ballot_sync(kFull, lbb == mn)) - 1);
                 const uint32_t others = intm & ~(1u << near);
                 if ((intm >> lane) & 1u) {
                     const uint32_t at = (uint32_t)sp + (lane == near ? np - 1 : __popc(others & lt));
-                    stack[3 * at] = ref;
-                    stack[3 * at + 1] = cnt & kWideCount;
-                    stack[3 * at + 2] = __float_as_uint(lb);
+                    stack[2 * at] = ref;
+                    stack[2 * at + 1] = stack_word(lb, cnt & kWideCount);
                 }
                 sp += (int)np;
                 __syncwarp();
@@ -1031,10 +1039,15 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         uint32_t rest = leafm;
         if (rest) {
             uint32_t b = __ffs(rest) - 1;
+            const float thr0 = thr;
             for (;;) {
                 const uint32_t lref = __shfl_sync(kFull, ref, b), lcnt = __shfl_sync(kFull, cnt, b);
-                const float llb = __shfl_sync(kFull, lb, b);
-                if (selected ? llb <= thr : llb < thr)
+                bool go = true;
+                if (thr != thr0) {   // a selection tightened the threshold since the ballot
+                    const float llb = __shfl_sync(kFull, lb, b);
+                    go = llb <= thr;
+                }
+                if (go)
                     scan_leaf32(a, lref, lcnt, qx, qy, qz, k, C, buf, n, selected, thr, hist, lane, lt);
                 rest &= ~(1u << b);
                 if (!rest) break;
@@ -1045,8 +1058,9 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
 }
 
 // The wide instances are held to 64 registers (4 blocks of 256 per SM, 32
-// warps): measured fastest, and without a bound ptxas holds them to 48
-// registers and spills.
+// warps): measured fastest.  Without a bound ptxas holds them to 48
+// registers and spills; with 3 blocks (80 registers, no spills, 24 warps) the
+// plain workload's kernel took 8.19 ms against 6.95.
 template <int G, bool kFix, bool kBatch, bool kWide>
 __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
     constexpr int QW = 32 / G;
@@ -1058,7 +1072,17 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
     const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << gbase);
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t C = a0.cap;
-    unsigned char* wb = smem + (size_t)warp * a0.smem_per_warp;
+    constexpr size_t top_off = (kWide && !kBatch) ? kTopBytes : 0;
+    if constexpr (kWide && !kBatch) {   // stage the root wide node's children
+        ChildSlot* st = reinterpret_cast<ChildSlot*>(smem);
+        const ChildSlot r = *a0.root;
+        const bool w = r.ref != kInvalid && (r.cnt & kWideFlag);
+        if (w && threadIdx.x < (r.cnt & kWideCount)) st[threadIdx.x] = a0.wchild[r.ref + threadIdx.x];
+        __syncthreads();
+        a0.s_top = st;
+        a0.top_first = w ? r.ref : kInvalid;
+    }
+    unsigned char* wb = smem + top_off + (size_t)warp * a0.smem_per_warp;
     uint64_t* buf = reinterpret_cast<uint64_t*>(wb) + (size_t)g * C;
     uint32_t* hist = reinterpret_cast<uint32_t*>(wb + (size_t)QW * C * sizeof(uint64_t)) + g * 256;
     uint32_t* stack = reinterpret_cast<uint32_t*>(wb + (size_t)QW * (C * sizeof(uint64_t) + 256 * sizeof(uint32_t)));
@@ -1090,6 +1114,7 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
                 const BatchQuery bq = a0.bq[map];
                 a.k = bq.k; a.r2max = bq.r2max; a.rmax = bq.rmax; a.filter = bq.filter; a.cone_k = bq.cone_k;
                 a.min_found = bq.min_found; a.nbr_off = bq.nbr_off; a.q_off = bq.q_off; a.ph_off = bq.ph_off;
+                a.norm_c = bq.norm_c;
                 a.scale_ptr = &a0.bgeom[map].fix_scale;
                 a.root = kWide ? &a0.bgeom[map].wroot : &a0.bgeom[map].root;
             }
@@ -1105,8 +1130,9 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
             if (inrange) {
                 qo = a.order ? a.order[slot_main] : slot_main;
                 const float4 q = a.qpos[qo];
+                qx = q.x; qy = q.y; qz = q.z;
                 const float4 nn = a.qnrm[qo];
-                qx = q.x; qy = q.y; qz = q.z; nx = nn.x; ny = nn.y; nz = nn.z;
+                nx = nn.x; ny = nn.y; nz = nn.z;
                 active = isfinite(qx) && isfinite(qy) && isfinite(qz);
                 if (!active && s == 0) atomicOr(&a.hdr->errors, kErrQueryNonFinite);
             }
@@ -1361,6 +1387,15 @@ int query_smem_bytes_per_warp(uint32_t k) {
     return (int)(32 * k * sizeof(uint64_t) + kStackDepth * sizeof(uint32_t));
 }
 
+// The filter's normalisation constant c, the estimate's factor being c / r^2:
+// 1 / ((1 - 2 / (3 k_c)) pi) (cone), 2 / pi (Epanechnikov), 1 / pi (box).
+double filter_norm_const(int filter, float cone_k) {
+    const double pi = 3.14159265358979323846;
+    if (filter == 1) return 1.0 / ((1.0 - 2.0 / (3.0 * (double)cone_k)) * pi);
+    if (filter == 2) return 2.0 / pi;
+    return 1.0 / pi;
+}
+
 static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
                          const uint32_t* order, uint32_t nq, const QueryOutputs& out) {
     KnnArgs a;
@@ -1376,13 +1411,15 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.nbr_off = 0; a.q_off = 0; a.ph_off = 0;
     a.qkeys = nullptr; a.bgeom = nullptr; a.bq = nullptr;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
+    a.norm_c = filter_norm_const(p.filter, p.cone_k);
+    a.s_top = nullptr; a.top_first = kInvalid;
     return a;
 }
 
 uint32_t group_capacity(uint32_t k) { return ((k + 31u) & ~31u) + 64u; }
 
 int wide_smem_bytes_per_warp(uint32_t k) {
-    return (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) + 3 * kWideStack * (int)sizeof(uint32_t);
+    return (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) + 2 * kWideStack * (int)sizeof(uint32_t);
 }
 
 int group_smem_bytes_per_warp(uint32_t k, int qpw) {
@@ -1427,7 +1464,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         a.root = m.wroot;
         a.fix_list = fix_list;
         a.fix_count = work_counter + 1;
-        const int smem = (int)a.smem_per_warp * t.warps_per_block;
+        const int smem = (int)a.smem_per_warp * t.warps_per_block + kTopBytes;
         const uint32_t nchunks = (nq + a.rounds_per_chunk - 1) / a.rounds_per_chunk;
         KnnArgs fx = a;
         fx.fix_in = fix_list;

@@ -23,32 +23,6 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 // ------------------------------------------------------------------ scan --
 
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = (lane < nwarps) ? s_warp[lane] : 0u;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < nwarps) s_warp[lane] = w;
-    }
-    __syncthreads();
-    total = s_warp[nwarps - 1];
-    const uint32_t warp_prefix = warp ? s_warp[warp - 1] : 0u;
-    __syncthreads();
-    return warp_prefix + x - v;
-}
-
 // Per-tile sums of in[0, n).
 __global__ void k_scan_reduce(const uint32_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ tile_sums) {
     __shared__ uint32_t s_warp[32];
@@ -188,14 +162,17 @@ __global__ void __launch_bounds__(kScanThreads) k_digit_rowscan(uint32_t* __rest
     if (threadIdx.x == 0) digit_total[blockIdx.x] = carry;
 }
 
-template <class Key>
+// kGather (the build's last pass): instead of the values, the photons
+// themselves go to their sorted positions (tree order), with the caller index
+// in pos.w, the packed direction in pow.w, and the inverse permutation.
+template <class Key, bool kGather>
 __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __restrict__ keys_in,
                                                                   const uint32_t* __restrict__ vals_in, uint32_t n,
                                                                   int shift, uint32_t ntiles,
                                                                   const uint32_t* __restrict__ offsets,
                                                                   const uint32_t* __restrict__ digit_total,
                                                                   Key* __restrict__ keys_out,
-                                                                  uint32_t* __restrict__ vals_out) {
+                                                                  uint32_t* __restrict__ vals_out, SortGather gather) {
     __shared__ uint32_t s_cnt[kSortWarps][256];   // per-warp digit counts, then per-warp starts within the digit
     __shared__ uint32_t s_start[256];             // tile-local start of each digit
     __shared__ uint32_t s_global[256];            // global position of the tile's first key of each digit
@@ -275,7 +252,17 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
         const uint32_t digit = (uint32_t)(kk >> shift) & 0xffu;
         const uint32_t dst = s_global[digit] + (i - s_start[digit]);
         keys_out[dst] = kk;
-        vals_out[dst] = s_val[i];
+        if (kGather) {
+            const uint32_t src = s_val[i];
+            const float4 p = gather.in_pos[src];
+            const float4 w = gather.in_pow[src];
+            const uint32_t dir = (gather.format == 0) ? spherical_to_oct(p.w, w.w) : __float_as_uint(w.w);
+            gather.out_pos[dst] = make_float4(p.x, p.y, p.z, __uint_as_float(src));
+            gather.out_pow[dst] = make_float4(w.x, w.y, w.z, __uint_as_float(dir));
+            gather.inv[src] = dst;
+        } else {
+            vals_out[dst] = s_val[i];
+        }
     }
 }
 
@@ -297,7 +284,7 @@ size_t sort_scratch_words(uint32_t n) {
 // index are clobbered.
 template <class Key>
 static int radix_sort_impl(Key* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
-                           cudaStream_t st, int* launches) {
+                           cudaStream_t st, int* launches, const SortGather* gather) {
     if (n <= 1) return 0;
     int nl = 0;
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
@@ -313,8 +300,13 @@ static int radix_sort_impl(Key* keys[2], uint32_t* vals[2], uint32_t n, int key_
         } else {
             nl += 2 + exclusive_scan(hist, hist, tiles * 256u, tail, nullptr, st);
         }
-        k_digit_scatter<Key><<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
-                                                              rows ? tail : nullptr, keys[cur ^ 1], vals[cur ^ 1]);
+        const uint32_t* dtot = rows ? tail : nullptr;
+        if (gather && shift + 8 >= key_bits)
+            k_digit_scatter<Key, true><<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
+                                                                       dtot, keys[cur ^ 1], vals[cur ^ 1], *gather);
+        else
+            k_digit_scatter<Key, false><<<tiles, kSortThreads, 0, st>>>(keys[cur], vals[cur], n, shift, tiles, hist,
+                                                                        dtot, keys[cur ^ 1], vals[cur ^ 1], SortGather{});
         cur ^= 1;
     }
     if (launches) *launches += nl;
@@ -322,13 +314,13 @@ static int radix_sort_impl(Key* keys[2], uint32_t* vals[2], uint32_t n, int key_
 }
 
 int radix_sort_pairs(uint64_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
-                     cudaStream_t st, int* launches) {
-    return radix_sort_impl<uint64_t>(keys, vals, n, key_bits, scratch, st, launches);
+                     cudaStream_t st, int* launches, const SortGather* gather) {
+    return radix_sort_impl<uint64_t>(keys, vals, n, key_bits, scratch, st, launches, gather);
 }
 
 int radix_sort_pairs32(uint32_t* keys[2], uint32_t* vals[2], uint32_t n, int key_bits, uint32_t* scratch,
                        cudaStream_t st, int* launches) {
-    return radix_sort_impl<uint32_t>(keys, vals, n, key_bits > 32 ? 32 : key_bits, scratch, st, launches);
+    return radix_sort_impl<uint32_t>(keys, vals, n, key_bits > 32 ? 32 : key_bits, scratch, st, launches, nullptr);
 }
 
 }  // namespace pm
