@@ -331,10 +331,11 @@ def _morton48(p, lo, scale):
 @pytest.mark.parametrize("n", [1, 2, 3, 2047, 2048, 2049, 4097, 65537, 100003, 4194305])
 def test_radix_sort_and_scan_through_tree_order(cuda, n):
     """The exported tree order is exactly the order of (Morton code, caller
-    index) -- the device radix sort (one launch per pass, tile offsets by
-    decoupled look-back) checked end to end at odd sizes around the 2,048-key
-    sort tile and up to 2,049 tiles -- and the compaction scan kept exactly the
-    nodes that hold more than leaf_size photons."""
+    index) -- the device radix sort, whose last pass moves the photons into
+    tree order, checked end to end at odd sizes around the 2,048-key sort tile,
+    and above 2,048 tiles (4,194,304 keys), where a pass scans the whole
+    digit-major array instead of one row per digit -- and the compaction scan
+    kept exactly the nodes that hold more than leaf_size photons."""
     ph = gen.photons(n, seed=600 + n, caustic_frac=0.3)
     ph.pos[: n // 3, :3] = np.round(ph.pos[: n // 3, :3] * 64) / 64   # many equal codes: ties by index
     pm = PhotonMap(n, global_q_radius_max=0.1)
