@@ -223,7 +223,9 @@ struct QueryTuning {
     int warps_per_block;
     int rounds_per_chunk;
     unsigned long long* stats;   // 8 traversal counters (group layout), nullptr = off
+    const float4* qsorted = nullptr;   // query records in sorted order (pos.xyz | caller index, normal), or nullptr
 };
+int gather_queries(const uint32_t* order, const float4* qpos, const float4* qnrm, uint32_t nq, float4* out, cudaStream_t st);
 int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const float4* qnrm,
               const uint32_t* order, uint32_t nq, const QueryOutputs& out, uint32_t* work_counter, uint32_t* fix_list,
               const QueryTuning& t, cudaStream_t st);

@@ -8,8 +8,9 @@
 // this kernel finds the exact k nearest photons in one pass:
 //
 //   * queries are processed in Hilbert order (k_query_order + the radix
-//     sort), and warps take chunks of consecutive queries by guided
-//     self-scheduling (long chunks first, short ones last);
+//     sort; for the wide layout k_gather_queries then lays their 32-byte
+//     records out in that order), and warps take chunks of consecutive
+//     queries by guided self-scheduling (long chunks first, short ones last);
 //   * each query starts from a radius bound given by the previous query of
 //     its warp (triangle inequality: r_k(q) <= r_k(q') + |q - q'|), so most
 //     searches start tight instead of at R;
@@ -26,7 +27,6 @@
 //     the order in which neighbours were found, and every layout gives the
 //     same bits.
 #include "pm_internal.h"
-
 
 namespace pm {
 
@@ -70,6 +70,7 @@ struct KnnArgs {
     const BatchGeom* bgeom;   // batch: per-map geometry (built)
     const BatchQuery* bq;     // batch: per-map query parameters
     double norm_c;            // the filter's normalisation constant (filter_norm_const)
+    const float4* qsorted;    // query records in sorted order (pos.xyz | caller index, normal), or nullptr
     const ChildSlot* s_top;   // staged root children (shared memory) or nullptr
     uint32_t top_first;       // wchild index of the staged children
 };
@@ -1128,10 +1129,17 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
             float qx = 0.f, qy = 0.f, qz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
             bool active = false;
             if (inrange) {
-                qo = a.order ? a.order[slot_main] : slot_main;
-                const float4 q = a.qpos[qo];
+                float4 q, nn;
+                if (!kFix && !kBatch && a.qsorted) {   // records already in processing order
+                    q = a.qsorted[2 * (size_t)slot_main];
+                    nn = a.qsorted[2 * (size_t)slot_main + 1];
+                    qo = __float_as_uint(q.w);
+                } else {
+                    qo = a.order ? a.order[slot_main] : slot_main;
+                    q = a.qpos[qo];
+                    nn = a.qnrm[qo];
+                }
                 qx = q.x; qy = q.y; qz = q.z;
-                const float4 nn = a.qnrm[qo];
                 nx = nn.x; ny = nn.y; nz = nn.z;
                 active = isfinite(qx) && isfinite(qy) && isfinite(qz);
                 if (!active && s == 0) atomicOr(&a.hdr->errors, kErrQueryNonFinite);
@@ -1354,6 +1362,26 @@ __global__ void __launch_bounds__(kBruteThreads) k_knn_brute(KnnArgs a, uint32_t
     if (valid) finish_query(a, heap, kBruteThreads, hn, q, qx, qy, qz, nx, ny, nz);
 }
 
+// Query records in processing order: rec[2i] = (position xyz, caller index
+// bits), rec[2i + 1] = normal of query order[i].
+__global__ void k_gather_queries(const uint32_t* __restrict__ order, const float4* __restrict__ qpos,
+                                 const float4* __restrict__ qnrm, uint32_t nq, float4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const uint32_t o = order[i];
+    float4 p = qpos[o];
+    p.w = __uint_as_float(o);
+    out[2 * (size_t)i] = p;
+    out[2 * (size_t)i + 1] = qnrm[o];
+}
+
+int gather_queries(const uint32_t* order, const float4* qpos, const float4* qnrm, uint32_t nq, float4* out,
+                   cudaStream_t st) {
+    if (!nq) return 0;
+    k_gather_queries<<<(nq + 255) / 256, 256, 0, st>>>(order, qpos, qnrm, nq, out);
+    return 1;
+}
+
 // Processing-order keys of the queries: a 30-bit Hilbert index (the kNN
 // query, a warp per query, profits from consecutive queries being neighbours)
 // or a 30-bit Morton code (the cut interpolation, a thread per query, profits
@@ -1412,6 +1440,7 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     a.qkeys = nullptr; a.bgeom = nullptr; a.bq = nullptr;
     a.cap = 0; a.smem_per_warp = 0; a.stats = nullptr;
     a.norm_c = filter_norm_const(p.filter, p.cone_k);
+    a.qsorted = nullptr;
     a.s_top = nullptr; a.top_first = kInvalid;
     return a;
 }
@@ -1459,6 +1488,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         return 1;
     }
     if (t.layout == 2) {   // one query per warp over the 32-wide tree
+        a.qsorted = t.qsorted;
         a.cap = group_capacity(p.k);
         a.smem_per_warp = (uint32_t)wide_smem_bytes_per_warp(p.k);
         a.root = m.wroot;
@@ -1470,6 +1500,7 @@ int query_knn(const MapView& m, const QueryParams& p, const float4* qpos, const 
         fx.fix_in = fix_list;
         fx.nq_dev = work_counter + 1;
         fx.work_counter = work_counter + 2;
+        fx.qsorted = nullptr;
         const uint32_t grid = grid_for(k_knn_group<32, false, false, true>, threads, smem, nchunks, t.warps_per_block);
         k_knn_group<32, false, false, true><<<grid, threads, smem, st>>>(a);
         const uint32_t gfix = grid_for(k_knn_group<32, true, false, true>, threads, smem, nchunks, t.warps_per_block);
