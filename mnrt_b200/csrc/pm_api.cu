@@ -409,12 +409,11 @@ pm_status pm_build(pm_map* m, const float* d_pos4, const float* d_pow4, uint32_t
     if (prof) cudaEventRecord(m->ev[0], st);
     const int nl = build_map(reinterpret_cast<const float4*>(d_pos4), reinterpret_cast<const float4*>(d_pow4), n,
                              format, m->leaf_size, P<float4>(m->pos), P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes),
-                             P<MapHeader>(m->hdr), bb, st, prof ? m->ev[1] : nullptr);
-    const int nw = build_wide(n, P<Node>(m->nodes), P<uint32_t>(m->parent), nullptr, P<MapHeader>(m->hdr), wide_of(m), st);
+                             P<MapHeader>(m->hdr), bb, wide_of(m), st, prof ? m->ev[1] : nullptr);
     if (prof) cudaEventRecord(m->ev[2], st);
     m->have_build_ev = prof;
-    m->build_launches = (uint32_t)(nl + nw);
-    m->launches += (uint64_t)(nl + nw);
+    m->build_launches = (uint32_t)nl;
+    m->launches += (uint64_t)nl;
     s = check_cuda(m, "pm_build");
     if (s != PM_OK) return s;
     m->n = n;

@@ -316,10 +316,10 @@ __global__ void k_leaf_boxes(const float4* __restrict__ pos, Node* __restrict__ 
 // Thread per compacted node: nodes whose two children are leaves start a
 // climb; each climber writes its box into the parent's slot and the second
 // arrival at a parent continues upwards.
-__global__ void k_refit(Node* nodes, const uint32_t* __restrict__ parent, uint32_t* arrive,
-                        const uint32_t* __restrict__ nleaf, const MapHeader* __restrict__ hdr, uint32_t max_nodes) {
+__device__ __forceinline__ void refit_thread(Node* nodes, const uint32_t* __restrict__ parent, uint32_t* arrive,
+                                             const uint32_t* __restrict__ nleaf, const MapHeader* __restrict__ hdr,
+                                             uint32_t max_nodes, uint32_t t) {
     const uint32_t m = hdr->num_nodes;
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= m || t >= max_nodes) return;
     uint32_t id = 1 + t;
     if (nleaf[id] != 2) return;
@@ -347,6 +347,11 @@ __global__ void k_refit(Node* nodes, const uint32_t* __restrict__ parent, uint32
     }
 }
 
+__global__ void k_refit(Node* nodes, const uint32_t* __restrict__ parent, uint32_t* arrive,
+                        const uint32_t* __restrict__ nleaf, const MapHeader* __restrict__ hdr, uint32_t max_nodes) {
+    refit_thread(nodes, parent, arrive, nleaf, hdr, max_nodes, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 __global__ void k_scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -371,9 +376,21 @@ void scale_flux(float4* pw, uint32_t n, float scale, MapHeader* hdr, cudaStream_
 // nodes, refit.  keys/vals are the sorted (code, caller index) pairs; any
 // code whose prefix separates groups (e.g. a map id in the top bits) yields
 // one subtree per group.
+// k_refit_wide_count is defined with the wide tree below.
+__global__ void k_refit_wide_count(Node* nodes, const uint32_t* __restrict__ parent, uint32_t* arrive,
+                                   const uint32_t* __restrict__ nleaf, const MapHeader* __restrict__ hdr,
+                                   uint32_t max_nodes, uint32_t refit_blocks, uint32_t bound,
+                                   uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
+                                   uint32_t* __restrict__ wfirst, uint32_t* scan, uint32_t* err);
+__global__ void k_wide_emit(const Node* __restrict__ nodes, const uint32_t* __restrict__ rootmark,
+                            const uint32_t* __restrict__ wflag, const uint32_t* __restrict__ wcnt,
+                            const uint32_t* __restrict__ wfirst, const MapHeader* __restrict__ hdr, uint32_t bound,
+                            ChildSlot* __restrict__ wchild, ChildSlot* __restrict__ wroot);
+
 int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
                       const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
-                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered) {
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered,
+                      const WideBuffers* wide) {
     const uint32_t tb = 256;
     if (n > 0) {
         if (!gathered) k_gather<<<(n + tb - 1) / tb, tb, 0, st>>>(in_pos, in_pow, vals, n, format, out_pos, out_pow, inv);
@@ -389,6 +406,16 @@ int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, in
             k_emit<<<gi, tb, 0, st>>>(out_pos, n, leaf_size, bb.kfirst, bb.klast, bb.ksplit, bb.kkeep, bb.krank,
                                       total, nodes, bb.parent, bb.arrive, bb.nleaf, hdr);
             k_leaf_boxes<<<kLeafBoxBlocks, 256, 0, st>>>(out_pos, nodes, hdr);
+            if (wide) {   // the single-map build: refit and the wide tree's counts in one launch
+                const uint32_t wgrid = (ni + 255u) / 256u;
+                cudaMemsetAsync(wide->scratch, 0, wide_scan_words(n) * sizeof(uint32_t), st);
+                k_refit_wide_count<<<gi + wgrid, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n, gi, ni,
+                                                             wide->wflag, wide->wcnt, wide->wfirst, wide->scratch,
+                                                             &hdr->errors);
+                k_wide_emit<<<wgrid, 256, 0, st>>>(nodes, nullptr, wide->wflag, wide->wcnt, wide->wfirst, hdr, ni,
+                                                   wide->wchild, wide->wroot);
+                return ng + 6 + ns;
+            }
             k_refit<<<gi, tb, 0, st>>>(nodes, bb.parent, bb.arrive, bb.nleaf, hdr, n);
             return ng + 5 + ns;
         }
@@ -400,7 +427,7 @@ int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, in
 
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
               float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
-              cudaStream_t st, cudaEvent_t sort_done) {
+              const WideBuffers& wide, cudaStream_t st, cudaEvent_t sort_done) {
     int nl = 0;
     const uint32_t nb = (uint32_t)((n + kBoundsThreads - 1) / kBoundsThreads);
     const uint32_t bblocks = nb < 1 ? 1 : (nb > (uint32_t)kBoundsBlocksMax ? (uint32_t)kBoundsBlocksMax : nb);
@@ -420,8 +447,10 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
         cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl, n > 1 ? &g : nullptr);
     }
     if (sort_done) cudaEventRecord(sort_done, st);
-    return nl + build_from_sorted(in_pos, in_pow, n, format, leaf_size, keys[cur], vals[cur], out_pos, out_pow, inv,
-                                  nodes, hdr, bb, st, n > 1);
+    nl += build_from_sorted(in_pos, in_pow, n, format, leaf_size, keys[cur], vals[cur], out_pos, out_pow, inv, nodes,
+                            hdr, bb, st, n > 1, &wide);
+    if (n <= 1) nl += build_wide(n, nodes, bb.parent, nullptr, hdr, wide, st);   // the start slot only
+    return nl;
 }
 
 
@@ -488,11 +517,11 @@ __device__ uint32_t wide_expand_warp(const Node* __restrict__ nodes, const uint3
 // the counts plus a decoupled look-back gives every wide node its first
 // child slot (one launch for flags, counts and scan).  scan: [0] ticket, [1]
 // total child slots (last tile), look-back words from word 2; cleared before.
-__global__ void __launch_bounds__(256) k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ parent,
-                                                     const uint32_t* __restrict__ rootmark,
-                                                     const MapHeader* __restrict__ hdr, uint32_t bound,
-                                                     uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
-                                                     uint32_t* __restrict__ wfirst, uint32_t* scan, uint32_t* err) {
+__device__ __forceinline__ void wide_count_block(const Node* __restrict__ nodes, const uint32_t* __restrict__ parent,
+                                                 const uint32_t* __restrict__ rootmark,
+                                                 const MapHeader* __restrict__ hdr, uint32_t bound,
+                                                 uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
+                                                 uint32_t* __restrict__ wfirst, uint32_t* scan, uint32_t* err) {
     __shared__ uint32_t s_buf[8][64];
     __shared__ uint32_t s_tile, s_warp[32];
     __shared__ uint64_t s_before;
@@ -530,6 +559,33 @@ __global__ void __launch_bounds__(256) k_wide_count(const Node* __restrict__ nod
         wfirst[t] = (uint32_t)s_before + ex;
     }
     if (threadIdx.x == 0 && s_tile + 1 == (bound + 255u) / 256u) scan[1] = (uint32_t)s_before + total;
+}
+
+__global__ void __launch_bounds__(256) k_wide_count(const Node* __restrict__ nodes, const uint32_t* __restrict__ parent,
+                                                     const uint32_t* __restrict__ rootmark,
+                                                     const MapHeader* __restrict__ hdr, uint32_t bound,
+                                                     uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
+                                                     uint32_t* __restrict__ wfirst, uint32_t* scan, uint32_t* err) {
+    wide_count_block(nodes, parent, rootmark, hdr, bound, wflag, wcnt, wfirst, scan, err);
+}
+
+// The refit and the wide tree's counts in one launch: they are independent
+// (the counts read only the tree's structure, which k_emit wrote; the refit
+// writes only boxes), and both are latency-bound walks along root-to-leaf
+// paths, so blocks [0, refit_blocks) climb while the others count.  The
+// counting blocks take their tiles by ticket and wait only on each other.
+__global__ void __launch_bounds__(256) k_refit_wide_count(Node* nodes, const uint32_t* __restrict__ parent,
+                                                           uint32_t* arrive, const uint32_t* __restrict__ nleaf,
+                                                           const MapHeader* __restrict__ hdr, uint32_t max_nodes,
+                                                           uint32_t refit_blocks, uint32_t bound,
+                                                           uint32_t* __restrict__ wflag, uint32_t* __restrict__ wcnt,
+                                                           uint32_t* __restrict__ wfirst, uint32_t* scan,
+                                                           uint32_t* err) {
+    if (blockIdx.x < refit_blocks) {
+        refit_thread(nodes, parent, arrive, nleaf, hdr, max_nodes, blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    wide_count_block(nodes, parent, nullptr, hdr, bound, wflag, wcnt, wfirst, scan, err);
 }
 
 // Warp per 32 consecutive compacted nodes: every wide node's child slots;

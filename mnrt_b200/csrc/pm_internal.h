@@ -186,15 +186,17 @@ size_t build_bytes_needed(uint32_t n);
 size_t wide_scan_words(uint32_t n);   // WideBuffers::scratch
 // Returns the number of kernels launched; sort_done (if set) is recorded on
 // the stream right after the radix sort.
+// The whole single-map build, binary and 32-wide tree.
 int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
               float4* out_pos, float4* out_pow, uint32_t* inv, Node* nodes, MapHeader* hdr, const BuildBuffers& bb,
-              cudaStream_t st, cudaEvent_t sort_done = nullptr);
+              const WideBuffers& wide, cudaStream_t st, cudaEvent_t sort_done = nullptr);
 void scale_flux(float4* pow, uint32_t n, float scale, MapHeader* hdr, cudaStream_t st);
 int build_wide(uint32_t n, const Node* nodes, const uint32_t* parent, const uint32_t* rootmark, MapHeader* hdr,
                const WideBuffers& wb, cudaStream_t st);
 int build_from_sorted(const float4* in_pos, const float4* in_pow, uint32_t n, int format, uint32_t leaf_size,
                       const uint64_t* keys, const uint32_t* vals, float4* out_pos, float4* out_pow, uint32_t* inv,
-                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered = false);
+                      Node* nodes, MapHeader* hdr, const BuildBuffers& bb, cudaStream_t st, bool gathered = false,
+                      const WideBuffers* wide = nullptr);   // wide: also the 32-wide tree (single map, n >= 2)
 
 // pm_query.cu
 struct QueryParams {
