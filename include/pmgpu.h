@@ -123,7 +123,7 @@ enum { PM_KBUF_HEAP = 0,   /* one lane per query, max-heap in shared memory */
        PM_KBUF_GROUP = 1,  /* a group of lanes per query, candidate buffer + exact selection */
        PM_KBUF_WIDE = 2    /* one query per warp over the 32-wide tree, candidate buffer + exact selection */ };
 
-/* Tuning knobs (chosen by the autotuner): photons per leaf (1..32), warps per
+/* Tuning knobs (chosen by the autotuner): photons per leaf (1..64), warps per
  * query block (1..8), rounds in the smallest work chunk (1..4096; warps take
  * chunks by guided self-scheduling: long chunks first, this size last), queries per warp
  * (1, 2, 4, 8; group layout) and the k-buffer layout (PM_KBUF_*). */

@@ -1525,7 +1525,7 @@ struct TuneCand {
 
 std::vector<TuneCand> tune_candidates(uint32_t k) {
     std::vector<TuneCand> c;
-    const uint32_t leaves[] = {16, 24, 32};
+    const uint32_t leaves[] = {16, 24, 32, 48, 64};
     const int wpbs[] = {2, 4, 8};
     const int rounds[] = {8, 32};
     for (uint32_t l : leaves)
@@ -1630,7 +1630,7 @@ extern "C" pm_status pm_batch_autotune(pm_batch* b, const float* d_pos4, const f
     uint32_t bl = saved_leaf;
     int bw = saved_wpb, br = saved_rounds;
     pm_status s = PM_OK;
-    const uint32_t leaves[] = {16, 24, 32};
+    const uint32_t leaves[] = {16, 24, 32, 48, 64};
     const int wpbs[] = {2, 4, 8};
     const int rounds[] = {8, 32};
     const int layouts[] = {PM_KBUF_GROUP, PM_KBUF_WIDE};

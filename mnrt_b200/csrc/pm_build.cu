@@ -298,6 +298,11 @@ __global__ void k_leaf_boxes(const float4* __restrict__ pos, Node* __restrict__ 
             float4 p = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
             float4 q = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
             if (lane < cnt) { p = pos[ref + lane]; q = p; }
+            if (lane + 32 < cnt) {   // leaves hold up to kLeafMax = 64 photons
+                const float4 r = pos[ref + 32 + lane];
+                p.x = fminf(p.x, r.x); p.y = fminf(p.y, r.y); p.z = fminf(p.z, r.z);
+                q.x = fmaxf(q.x, r.x); q.y = fmaxf(q.y, r.y); q.z = fmaxf(q.z, r.z);
+            }
             const uint32_t lx = __reduce_min_sync(0xffffffffu, ord_key(p.x));
             const uint32_t ly = __reduce_min_sync(0xffffffffu, ord_key(p.y));
             const uint32_t lz = __reduce_min_sync(0xffffffffu, ord_key(p.z));

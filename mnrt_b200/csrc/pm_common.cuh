@@ -11,7 +11,7 @@
 namespace pm {
 
 constexpr uint32_t kMaxK = 128;        // largest k a query supports
-constexpr uint32_t kLeafMax = 32;      // photons per leaf (upper bound)
+constexpr uint32_t kLeafMax = 64;      // photons per leaf (upper bound; two per lane where a warp scans a leaf)
 constexpr int kStackDepth = 128;       // traversal stack entries per warp
 constexpr uint32_t kInvalid = 0xffffffffu;
 

@@ -69,7 +69,8 @@ def test_build_validation_without_gpu(engine_lib):
     assert lib.pm_build(h, 17, 32, 10, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID   # misaligned
     assert lib.pm_build(h, 16, 32, 5000, L.PM_PHOTONS_PACKED, None) == L.PM_ERR_INVALID  # > max_photons
     assert lib.pm_set_tuning(h, 0, 4, 8, 4, 1) == L.PM_ERR_INVALID
-    assert lib.pm_set_tuning(h, 33, 4, 8, 4, 1) == L.PM_ERR_INVALID
+    assert lib.pm_set_tuning(h, 65, 4, 8, 4, 1) == L.PM_ERR_INVALID   # leaves hold at most 64 photons
+    assert lib.pm_set_tuning(h, 64, 4, 8, 4, 1) == L.PM_OK
     assert lib.pm_set_tuning(h, 16, 9, 8, 4, 1) == L.PM_ERR_INVALID
     assert lib.pm_set_tuning(h, 16, 4, 8, 3, 1) == L.PM_ERR_INVALID
     assert lib.pm_set_tuning(h, 16, 4, 8, 4, 3) == L.PM_ERR_INVALID

@@ -133,13 +133,28 @@ def test_tree_matches_bruteforce_and_order_invariance(cuda):
         assert np.array_equal(a[key], c[key]), key
 
 
-@pytest.mark.parametrize("leaf", [1, 4, 16, 32])
+@pytest.mark.parametrize("leaf", [1, 4, 16, 32, 33, 48, 64])
 def test_leaf_sizes_and_tuning(cuda, oracle_mod, leaf):
     ph = gen.photons(20000, seed=9, caustic_frac=0.3, caustic_sigma=0.005)
     q = gen.queries(3000, seed=10)
     res = run(ph, q, cuda, 32, 0.08, "epanechnikov", leaf=leaf,
               tuning=dict(warps_per_block=2, rounds_per_chunk=3))
     check_against_oracle(oracle_mod, ph, q, res, 32, 0.08, "epanechnikov")
+
+
+@pytest.mark.parametrize("leaf", [33, 64])
+@pytest.mark.parametrize("layout,qpw", [(0, 1), (1, 1), (1, 2), (1, 4), (1, 8), (2, 1)])
+def test_large_leaves_every_layout(cuda, oracle_mod, leaf, layout, qpw):
+    """Leaves of more than 32 photons (up to 64: two per lane) in every
+    k-buffer layout: the heap and group layouts scan them 32 photons at a
+    time, the wide layout in two halves."""
+    ph = gen.photons(30000, seed=31, caustic_frac=0.3, caustic_sigma=0.005)
+    q = gen.queries(2500, seed=32)
+    for k in (16, 100):
+        res = run(ph, q, cuda, k, 0.08, "cone", leaf=leaf,
+                  tuning=dict(warps_per_block=4, rounds_per_chunk=8, queries_per_warp=qpw, kbuf_layout=layout))
+        assert res["info"].leaf_size == leaf
+        check_against_oracle(oracle_mod, ph, q, res, k, 0.08, "cone")
 
 
 @pytest.mark.parametrize("k", [1, 2, 100, 128])
@@ -168,13 +183,15 @@ def test_duplicates_and_ties(cuda, oracle_mod):
         check_against_oracle(oracle_mod, ph, q, res, k, 0.3, "cone")
 
 
-def test_edge_maps(cuda, oracle_mod):
+@pytest.mark.parametrize("leaf", [16, 64])
+def test_edge_maps(cuda, oracle_mod, leaf):
+    """Empty and tiny maps, including single-leaf trees of up to 64 photons."""
     q = gen.queries(300, seed=15)
-    for n in (0, 1, 2, 5, 16, 17, 33):
+    for n in (0, 1, 2, 5, 16, 17, 33, 63, 64, 65):
         ph = gen.photons(n, seed=16 + n) if n else gen.PhotonSet(np.zeros((0, 4), np.float32),
                                                                   np.zeros((0, 4), np.float32),
                                                                   np.zeros((0, 3), np.float32), "packed")
-        res = run(ph, q, cuda, 8, 2.0, "box")
+        res = run(ph, q, cuda, 8, 2.0, "box", leaf=leaf)
         if n == 0:
             assert (res["count"] == 0).all() and (res["rad"] == 0).all()
             assert (res["nbr"].view(np.uint32) == 0xFFFFFFFF).all()
@@ -304,7 +321,7 @@ def test_autotune_keeps_results_exact(cuda, oracle_mod):
     pm = PhotonMap(ph.n, global_q_radius_max=0.05)
     d_pos, d_pow, d_qp, d_qn = (to_dev(x, cuda) for x in (ph.pos, ph.pow, q.pos, q.nrm))
     t = pm.autotune(d_pos, d_pow, d_qp, d_qn, max_sample=4096, k=64, r_max=0.05, filter="cone")
-    assert t.leaf_size in (16, 24, 32) and t.warps_per_block in (2, 4, 8) and t.rounds_per_chunk in (8, 32)
+    assert t.leaf_size in (16, 24, 32, 48, 64) and t.warps_per_block in (2, 4, 8) and t.rounds_per_chunk in (8, 32)
     assert t.queries_per_warp in (1, 2) and t.kbuf_layout in (0, 1, 2) and t.query_ms > 0
     out = pm.query(d_qp, d_qn, want_nbr=True, k=64, r_max=0.05, filter="cone")
     torch.cuda.synchronize()

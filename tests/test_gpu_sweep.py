@@ -87,7 +87,7 @@ def test_random_batch(cuda, seed):
     qoff = np.concatenate([[0], np.cumsum([q.n for q in qs])]).astype(np.uint32)
     cat = lambda xs: np.concatenate(xs).astype(np.float32)
     b = PhotonMapBatch()
-    b.set_tuning(leaf_size=int(rng.choice([4, 16, 32])), warps_per_block=4, rounds_per_chunk=int(rng.choice([1, 8, 32])),
+    b.set_tuning(leaf_size=int(rng.choice([4, 16, 32, 48, 64])), warps_per_block=4, rounds_per_chunk=int(rng.choice([1, 8, 32])),
                  wide=bool(rng.random() < 0.7))
     b.build(to_dev(cat([p.pos for p in phs]), cuda), to_dev(cat([p.pow for p in phs]), cuda), poff)
     if qoff[-1]:
@@ -127,7 +127,7 @@ def test_random_compat(cuda, oracle_mod, seed):
     ph = gen.photons(n, seed=int(rng.integers(1 << 30)), caustic_frac=0.2)
     q = gen.queries(nq, seed=int(rng.integers(1 << 30)))
     pm = PhotonMap(n, global_q_radius_max=r, knn_target_count=k)
-    pm.set_tuning(leaf_size=int(rng.choice([4, 16, 32])))
+    pm.set_tuning(leaf_size=int(rng.choice([4, 16, 32, 48, 64])))
     pm.build(to_dev(ph.pos, cuda), to_dev(ph.pow, cuda))
     out = pm.query(to_dev(q.pos, cuda), to_dev(q.nrm, cuda), mode=L.PM_MODE_ZHOU_COMPAT, refine_iters=iters,
                    filter=filt, min_found=8, k=k)
