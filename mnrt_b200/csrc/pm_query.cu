@@ -937,43 +937,39 @@ constexpr int kWideStack = 192;   // entries of 2 words: first child slot, stack
 // every query visits them first.
 constexpr int kTopBytes = 32 * (int)sizeof(ChildSlot);
 
-// One 32-photon half of a leaf: this lane's photon (px, py, pz; tree
-// position idx) when `have`.
-__device__ __forceinline__ void scan_half(const KnnArgs& a, float px, float py, float pz, bool have, uint32_t idx,
-                                          float qx, float qy, float qz, uint32_t k, uint32_t C, uint64_t* buf,
-                                          uint32_t& n, bool& selected, float& thr, uint32_t* hist, uint32_t lane,
-                                          uint32_t lt) {
+// One 32-photon half of a leaf: this lane's photon at tree position idx,
+// at squared distance d2 from the query, when `have`.
+__device__ __forceinline__ void scan_half(const KnnArgs& a, float d2, bool have, uint32_t idx, uint32_t k, uint32_t C,
+                                          uint64_t* buf, uint32_t& n, bool& selected, float& thr, uint32_t* hist,
+                                          uint32_t lane, uint32_t lt) {
     if (n + 32 > C) {   // make room: keep the k nearest, tighten the threshold
         const uint64_t T = group_select<32>(buf, n, k, hist, a.pos, lane, kFull, lt);
         selected = true;
         thr = __uint_as_float((uint32_t)(T >> 32));
     }
-    bool acc = false;
-    float d2 = 0.0f;
-    if (have) {
-        d2 = d2_rn(qx, qy, qz, px, py, pz);
-        acc = selected ? (d2 <= thr) : (d2 < thr);
-    }
+    const bool acc = have && (selected ? (d2 <= thr) : (d2 < thr));
     const uint32_t bal = __ballot_sync(kFull, acc);
     if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | idx;
     n += __popc(bal);
     __syncwarp();
 }
 
-// A leaf of up to 64 photons: both halves' loads are issued before the
-// first is tested, so a large leaf costs one load latency.  Leaves of 64
-// (the autotuned size of the plain workload) against 32: 12.5 -> about 7.7
-// leaves per query for 23 % more photons tested, kernel 6.91 -> 6.50 ms.
+// A leaf of up to 64 photons: both halves' loads are issued before either is
+// tested, so a large leaf costs one load latency, and both distances are
+// formed at once (the second half then holds one register, not a photon).
+// Leaves of 64 (the autotuned size of the plain workload) against 32:
+// 12.5 -> about 7.7 leaves per query for 23 % more photons tested, kernel
+// 6.90 -> 6.52 ms.
 __device__ __forceinline__ void scan_leaf(const KnnArgs& a, uint32_t ref, uint32_t cnt, float qx, float qy, float qz,
                                           uint32_t k, uint32_t C, uint64_t* buf, uint32_t& n, bool& selected,
                                           float& thr, uint32_t* hist, uint32_t lane, uint32_t lt) {
     float4 m0 = make_float4(0.f, 0.f, 0.f, 0.f), m1 = m0;
     if (lane < cnt) m0 = __ldg(a.pos + ref + lane);
     if (lane + 32 < cnt) m1 = __ldg(a.pos + ref + 32 + lane);
-    scan_half(a, m0.x, m0.y, m0.z, lane < cnt, ref + lane, qx, qy, qz, k, C, buf, n, selected, thr, hist, lane, lt);
-    if (cnt > 32)
-        scan_half(a, m1.x, m1.y, m1.z, lane + 32 < cnt, ref + 32 + lane, qx, qy, qz, k, C, buf, n, selected, thr, hist,
-                  lane, lt);
+    const float d0 = d2_rn(qx, qy, qz, m0.x, m0.y, m0.z);
+    const float d1 = d2_rn(qx, qy, qz, m1.x, m1.y, m1.z);
+    scan_half(a, d0, lane < cnt, ref + lane, k, C, buf, n, selected, thr, hist, lane, lt);
+    if (cnt > 32) scan_half(a, d1, lane + 32 < cnt, ref + 32 + lane, k, C, buf, n, selected, thr, hist, lane, lt);
 }
 
 // Stack entry of the wide traversal: two words, the wide node's first child
