@@ -490,8 +490,14 @@ def run_diff(args, cfg) -> dict | None:
     d_qpos = torch.from_numpy(np.ascontiguousarray(q.pos[qa:qb])).to(dev)
     d_qnrm = torch.from_numpy(np.ascontiguousarray(q.nrm[qa:qb])).to(dev)
     pm = PhotonMap(N, global_q_radius_max=R, knn_target_count=k)
-    pm.reserve(N, Qr)
     kw = dict(k=k, r_max=R, filter=filt)
+    tuning = "defaults"
+    if not args.no_autotune:   # untimed: the forward's kernel setting, as the plain workload picks it
+        t = pm.autotune(d_pos, d_pow, d_qpos, d_qnrm, max_sample=0, **kw)
+        tuning = {"leaf_size": t.leaf_size, "warps_per_block": t.warps_per_block,
+                  "rounds_per_chunk": t.rounds_per_chunk, "queries_per_warp": t.queries_per_warp,
+                  "kbuf_layout": t.kbuf_layout, "chosen_by": "pm_autotune over all queries"}
+    pm.reserve(N, Qr)
     pm.build(d_pos, d_tpow)
     target = pm.query(d_qpos, d_qnrm, **kw)["rad"][:, :3].clone()
     out = {"rad": torch.empty((Qr, 4), dtype=torch.float32, device=dev),
@@ -575,7 +581,8 @@ def run_diff(args, cfg) -> dict | None:
         "config": {"workload": cfg["workload"], "photons": N, "queries": Q, "k": k, "r_max": R, "filter": filt,
                    "l2": "flushed between steps (256 MiB write, untimed)",
                    "parallelism": "one GPU" if world == 1 else
-                   f"map on every rank, queries divided over {world} ranks, gradient all-reduce (NCCL, f64)"},
+                   f"map on every rank, queries divided over {world} ranks, gradient all-reduce (NCCL, f64)",
+                   "tuning": tuning},
         "clocks": clocks,
         "forward_ms": fwd_ms, "forward_no_lists_ms": plain_ms, "backward_ms": bwd_ms,
         "fwd_bwd_over_fwd": (fwd_ms + bwd_ms) / fwd_ms, "fwd_bwd_over_fwd_no_lists": (fwd_ms + bwd_ms) / plain_ms,
