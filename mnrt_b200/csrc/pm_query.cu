@@ -635,26 +635,47 @@ template <int G>
 __device__ uint32_t hist_round(const uint64_t* buf, uint32_t n, float scale, int shift, uint32_t prefix,
                                bool use_prefix, uint32_t& kk, uint32_t* hist, uint32_t s, uint32_t gmask) {
     constexpr int BPL = 256 / G;   // buckets per lane
+    uint4* own = reinterpret_cast<uint4*>(hist + s * BPL);   // this lane's buckets, 16-byte aligned
 #pragma unroll
-    for (int i = 0; i < BPL; ++i) hist[s * BPL + i] = 0;
+    for (int i = 0; i < BPL / 4; ++i) own[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncwarp(gmask);
     for (uint32_t e = s; e < n; e += G) {
         const uint32_t q = q16((uint32_t)(buf[e] >> 32), scale);
         if (!use_prefix || (q >> 8) == prefix) atomicAdd(&hist[(q >> shift) & 255u], 1u);
     }
     __syncwarp(gmask);
-    uint32_t local = 0;
+    uint32_t local = 0, digit = 0, below = 0;
+    bool mine;
+    if constexpr (BPL <= 8) {   // one warp per query: the lane's 8 buckets stay in registers
+        uint32_t h[BPL];
 #pragma unroll
-    for (int i = 0; i < BPL; ++i) local += hist[s * BPL + i];
-    const uint32_t base = gexscan_u32<G>(local, s, gmask);
-    uint32_t digit = 0, below = 0;
-    const bool mine = base < kk && kk <= base + local;
-    if (mine) {
+        for (int i = 0; i < BPL / 4; ++i) {
+            const uint4 v = own[i];
+            h[4 * i] = v.x; h[4 * i + 1] = v.y; h[4 * i + 2] = v.z; h[4 * i + 3] = v.w;
+        }
+#pragma unroll
+        for (int i = 0; i < BPL; ++i) local += h[i];
+        const uint32_t base = gexscan_u32<G>(local, s, gmask);
+        mine = base < kk && kk <= base + local;
         uint32_t run = base;
+        bool found = false;
+#pragma unroll
         for (int i = 0; i < BPL; ++i) {
-            const uint32_t h = hist[s * BPL + i];
-            if (run + h >= kk) { digit = s * BPL + i; below = run; break; }
-            run += h;
+            if (mine && !found && run + h[i] >= kk) { digit = s * BPL + i; below = run; found = true; }
+            run += h[i];
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < BPL; ++i) local += hist[s * BPL + i];
+        const uint32_t base = gexscan_u32<G>(local, s, gmask);
+        mine = base < kk && kk <= base + local;
+        if (mine) {
+            uint32_t run = base;
+            for (int i = 0; i < BPL; ++i) {
+                const uint32_t hv = hist[s * BPL + i];
+                if (run + hv >= kk) { digit = s * BPL + i; below = run; break; }
+                run += hv;
+            }
         }
     }
     const uint32_t who = __ffs(__ballot_sync(gmask, mine)) - 1;
@@ -741,11 +762,15 @@ __device__ __forceinline__ uint64_t gsort_bitonic(uint64_t v, uint32_t s, uint32
 // crowds the hot loop's instructions.
 template <int G>
 __device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32_t kk, uint32_t* hist,
-                                              const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt) {
-    uint32_t mx = 0;
-    for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
-    mx = gmax_u32<G>(mx, gmask);
-    const float dmax = __uint_as_float(mx);
+                                              const float4* __restrict__ pos, uint32_t s, uint32_t gmask, uint32_t lt,
+                                              float bound) {
+    float dmax = bound;   // every entry's d^2 is at most the acceptance threshold
+    if (!(dmax > 0.0f) || !(dmax < INFINITY)) {
+        uint32_t mx = 0;
+        for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+        mx = gmax_u32<G>(mx, gmask);
+        dmax = __uint_as_float(mx);
+    }
     if (!(dmax > 0.0f)) return group_select_general<G>(buf, n, kk, hist, pos, s, gmask, lt);
     const float scale = __fdiv_rn(255.0f, dmax);   // q in [0, 255], monotone in d^2
     uint32_t need = kk;
@@ -871,13 +896,13 @@ __device__ __noinline__ void write_neighbours(uint64_t* buf, uint32_t n, uint32_
 }
 
 template <int G, bool kFix>
-__device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, uint32_t s,
+__device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint32_t* hist, float thr, uint32_t s,
                               uint32_t gmask, uint32_t lt, uint32_t qo, uint32_t slot, float qx, float qy, float qz,
                               float nx, float ny, float nz) {
     const uint32_t k = a.k;
     float rk2 = a.r2max;
     if (n > k) {   // the selection returns the largest kept d^2, the k-th neighbour's
-        rk2 = __uint_as_float((uint32_t)(group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt) >> 32));
+        rk2 = __uint_as_float((uint32_t)(group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt, thr) >> 32));
     } else if (n == k) {
         uint32_t mx = 0;
         for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
@@ -943,7 +968,7 @@ __device__ __forceinline__ void scan_half(const KnnArgs& a, float d2, bool have,
                                           uint64_t* buf, uint32_t& n, bool& selected, float& thr, uint32_t* hist,
                                           uint32_t lane, uint32_t lt) {
     if (n + 32 > C) {   // make room: keep the k nearest, tighten the threshold
-        const uint64_t T = group_select<32>(buf, n, k, hist, a.pos, lane, kFull, lt);
+        const uint64_t T = group_select<32>(buf, n, k, hist, a.pos, lane, kFull, lt, thr);
         selected = true;
         thr = __uint_as_float((uint32_t)(T >> 32));
     }
@@ -1208,7 +1233,7 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
                                     const bool full = live && (n + G > C);
                                     if (__any_sync(kFull, full)) {
                                         if (full) {
-                                            const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt);
+                                            const uint64_t T = group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt, thr);
                                             ++st_sel;
                                             selected = true;
                                             thr = __uint_as_float((uint32_t)(T >> 32));
@@ -1300,7 +1325,7 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
                 atomicAdd(a.stats + kStatPhotons, (unsigned long long)st_photons);
             }
             if (active) {
-                const float r2 = group_finish<G, kFix>(a, buf, n, hist, s, gmask, lt, qo, slot_main, qx, qy, qz, nx, ny, nz);
+                const float r2 = group_finish<G, kFix>(a, buf, n, hist, thr, s, gmask, lt, qo, slot_main, qx, qy, qz, nx, ny, nz);
                 rk2 = r2;
             } else if (inrange && s == 0) {
                 a.out_rad[qo] = make_float4(0.f, 0.f, 0.f, 0.f);
