@@ -640,7 +640,7 @@ __device__ uint32_t hist_round(const uint64_t* buf, uint32_t n, float scale, int
     for (int i = 0; i < BPL / 4; ++i) own[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncwarp(gmask);
     for (uint32_t e = s; e < n; e += G) {
-        const uint32_t q = q16((uint32_t)(buf[e] >> 32), scale);
+        const uint32_t q = q16(reinterpret_cast<const uint32_t*>(buf)[2 * e + 1], scale);   // the d^2 word
         if (!use_prefix || (q >> 8) == prefix) atomicAdd(&hist[(q >> shift) & 255u], 1u);
     }
     __syncwarp(gmask);
@@ -807,14 +807,14 @@ __device__ __noinline__ uint64_t group_select(uint64_t* buf, uint32_t& n, uint32
             keep = q < B || (q == B && (all_b || exact_key(v, pos) <= T));
         }
         const uint32_t bal = __ballot_sync(gmask, keep);
-        __syncwarp(gmask);
+        __syncwarp(gmask);   // this round's reads before its writes (in place, never ahead of the reads)
         if (keep) {
             buf[out + __popc(bal & lt)] = v;
             kmax = max(kmax, (uint32_t)(v >> 32));
         }
         out += __popc(bal);
-        __syncwarp(gmask);
     }
+    __syncwarp(gmask);
     n = out;
     return (uint64_t)gmax_u32<G>(kmax, gmask) << 32;
 }
@@ -1189,10 +1189,13 @@ __global__ void __launch_bounds__(256, kWide ? 4 : 0) k_knn_group(KnnArgs a0) {
             float tau0 = r2max;
 #pragma unroll
             for (int h = 0; h < QW; ++h) {
+                // one query per warp: every lane already holds its predecessor's values
                 const int src = h * G;
-                const float sx = __shfl_sync(kFull, pqx, src), sy = __shfl_sync(kFull, pqy, src);
-                const float sz = __shfl_sync(kFull, pqz, src), sr = __shfl_sync(kFull, pr, src);
-                const bool sv = __shfl_sync(kFull, pvalid, src);
+                const float sx = QW == 1 ? pqx : __shfl_sync(kFull, pqx, src);
+                const float sy = QW == 1 ? pqy : __shfl_sync(kFull, pqy, src);
+                const float sz = QW == 1 ? pqz : __shfl_sync(kFull, pqz, src);
+                const float sr = QW == 1 ? pr : __shfl_sync(kFull, pr, src);
+                const bool sv = QW == 1 ? pvalid : __shfl_sync(kFull, pvalid, src);
                 if (sv) {
                     const float dq = __fsqrt_rn(d2_rn(qx, qy, qz, sx, sy, sz));
                     const float b = __fmul_rn(__fadd_rn(sr, dq), 1.000244140625f);
