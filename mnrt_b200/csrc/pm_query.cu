@@ -905,7 +905,7 @@ __device__ float group_finish(const KnnArgs& a, uint64_t* buf, uint32_t& n, uint
         rk2 = __uint_as_float((uint32_t)(group_select<G>(buf, n, k, hist, a.pos, s, gmask, lt, thr) >> 32));
     } else if (n == k) {
         uint32_t mx = 0;
-        for (uint32_t e = s; e < n; e += G) mx = max(mx, (uint32_t)(buf[e] >> 32));
+        for (uint32_t e = s; e < n; e += G) mx = max(mx, reinterpret_cast<const uint32_t*>(buf)[2 * e + 1]);
         rk2 = __uint_as_float(gmax_u32<G>(mx, gmask));
     }
     const float r2 = rk2;
@@ -974,9 +974,9 @@ __device__ __forceinline__ void scan_half(const KnnArgs& a, float d2, bool have,
     }
     const bool acc = have && (selected ? (d2 <= thr) : (d2 < thr));
     const uint32_t bal = __ballot_sync(kFull, acc);
+    // appends only; readers of the buffer (a selection, the finish) sync before they read
     if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | idx;
     n += __popc(bal);
-    __syncwarp();
 }
 
 // A leaf of up to 64 photons: both halves' loads are issued before either is
@@ -1016,7 +1016,7 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         const float lb = box_lb(qx, qy, qz, lo, hi);
         if (!(selected ? lb <= thr : lb < thr)) return;
         if (cnt & kWideFlag) {
-            if (lane == 0) { stack[0] = ref; stack[1] = stack_word(lb, cnt & kWideCount); }
+            if (lane == 0) reinterpret_cast<uint2*>(stack)[0] = make_uint2(ref, stack_word(lb, cnt & kWideCount));
             sp = 1;
             __syncwarp();
         } else if (cnt > 0) {
@@ -1026,7 +1026,8 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
     }
     while (sp > 0) {
         --sp;
-        const uint32_t first = stack[2 * sp], e1 = stack[2 * sp + 1];
+        const uint2 entry = reinterpret_cast<const uint2*>(stack)[sp];
+        const uint32_t first = entry.x, e1 = entry.y;
         const uint32_t kids = e1 & 63u;
         const float plb = __uint_as_float(e1 & ~63u);
         __syncwarp();
@@ -1066,8 +1067,7 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
                 const uint32_t others = intm & ~(1u << near);
                 if ((intm >> lane) & 1u) {
                     const uint32_t at = (uint32_t)sp + (lane == near ? np - 1 : __popc(others & lt));
-                    stack[2 * at] = ref;
-                    stack[2 * at + 1] = stack_word(lb, cnt & kWideCount);
+                    reinterpret_cast<uint2*>(stack)[at] = make_uint2(ref, stack_word(lb, cnt & kWideCount));
                 }
                 sp += (int)np;
                 __syncwarp();
