@@ -1492,7 +1492,10 @@ static KnnArgs make_args(const MapView& m, const QueryParams& p, const float4* q
     return a;
 }
 
-uint32_t group_capacity(uint32_t k) { return ((k + 31u) & ~31u) + 64u; }
+// Candidate buffer entries per query: k rounded up to a warp, plus 96 of
+// headroom before a selection must make room (with leaves of up to 64
+// photons, 96 measured 5.90 -> 5.87 ms against 64 on the plain workload).
+uint32_t group_capacity(uint32_t k) { return ((k + 31u) & ~31u) + 96u; }
 
 int wide_smem_bytes_per_warp(uint32_t k) {
     return (int)(group_capacity(k) * sizeof(uint64_t) + 256 * sizeof(uint32_t)) + 2 * kWideStack * (int)sizeof(uint32_t);
