@@ -17,10 +17,12 @@
 //
 // Scatter without float atomics, deterministic by construction:
 //   1. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
-//                   -> per-query record (g * norm, G, r^2, position, normal),
-//                   and one (photon tree position, pair id) key-value per
-//                   neighbour slot; empty slots get the sentinel key n
-//   2. stable LSD radix sort by photon (pair ids of one photon stay in
+//                   -> per-query record (g * norm, G, the filter's
+//                   reciprocal, position, normal), and one key-value per
+//                   neighbour slot: photon tree position, query << 1 | (the
+//                   photon is the query's k-th); empty slots get the
+//                   sentinel key n
+//   2. stable LSD radix sort by photon (the values of one photon stay in
 //      query order)
 //   3. k_bwd_bounds segment [start, end) of every photon in the sorted array
 //   4. k_bwd_reduce thread per photon: walks its segment in order and sums
@@ -43,18 +45,31 @@ __device__ __forceinline__ double norm_of(int filter, double r2, double cone_k) 
     return 1.0 / (kPiD * r2);
 }
 
-// w, dw/dd2 and dw/dr2 of the filters (FP64).
-__device__ __forceinline__ void weight_terms(int filter, double d2, double r2, double cone_k, double& w, double& dw_dd2,
-                                             double& dw_dr2) {
+// The filter's reciprocal of one query (one FP64 division per query, none
+// per neighbour pair): 1 / (k_c r) for the cone, 1 / r^2 for Epanechnikov,
+// 1 for the box (a positive marker of a query that carries gradient).
+__device__ __forceinline__ double filter_rinv(int filter, double r2, double cone_k) {
+    if (filter == 1) return 1.0 / (cone_k * sqrt(r2));
+    if (filter == 2) return 1.0 / r2;
+    return 1.0;
+}
+
+// w and dw/dd2 of the filters (FP64) from the query's reciprocal rinv:
+//   cone:         w = 1 - d rinv,     dw/dd2 = -rinv / (2 d)  (d = d^2 / sqrt(d^2) by one rsqrt)
+//   Epanechnikov: w = 1 - d^2 rinv,   dw/dd2 = -rinv
+// and dw/dr2 (the per-query pass only; inv_r2 = 1 / r^2):
+//   cone: d rinv inv_r2 / 2,   Epanechnikov: d^2 rinv^2.
+__device__ __forceinline__ void weight_terms(int filter, double d2, double rinv, double inv_r2, double& w,
+                                             double& dw_dd2, double& dw_dr2) {
     if (filter == 1) {   // cone: w = 1 - d / (k_c r)
-        const double d = sqrt(d2), r = sqrt(r2);
-        w = 1.0 - d / (cone_k * r);
-        dw_dd2 = d > 0.0 ? -1.0 / (2.0 * d * cone_k * r) : 0.0;
-        dw_dr2 = d / (2.0 * cone_k * r2 * r);
+        const double rs = d2 > 0.0 ? rsqrt(d2) : 0.0, d = d2 * rs;
+        w = 1.0 - d * rinv;
+        dw_dd2 = -0.5 * rinv * rs;
+        dw_dr2 = 0.5 * d * rinv * inv_r2;
     } else if (filter == 2) {   // Epanechnikov: w = 1 - d^2 / r^2
-        w = 1.0 - d2 / r2;
-        dw_dd2 = -1.0 / r2;
-        dw_dr2 = d2 / (r2 * r2);
+        w = 1.0 - d2 * rinv;
+        dw_dd2 = -rinv;
+        dw_dr2 = d2 * rinv * rinv;
     } else {   // box
         w = 1.0;
         dw_dd2 = 0.0;
@@ -77,7 +92,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 // set: neighbouring warps then gather neighbouring photons, which L1 and L2
 // serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records and pairs stay at the
 // caller's index, so the results do not depend on the order.  The warp also
-// writes the query's k (photon tree position, pair id) keys and values for
+// writes the query's k (photon tree position, query | k-th flag) keys and values for
 // the sort by photon (empty slots and queries without gradient get the
 // sentinel key n, which sorts after every photon): the neighbour rows and
 // the inverse permutation are read once, here.
@@ -108,6 +123,7 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     const bool active = cnt > 0 && cnt >= a.min_found && r2 > 0.0 && isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
     double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
     const uint64_t pair0 = (uint64_t)ql * k;
+    const double rinv = filter_rinv(a.filter, r2, (double)a.cone_k), inv_r2 = 1.0 / r2;
     for (uint32_t j = lane; j < k; j += 32) {
         uint32_t key = a.n;
         if (active && j < cnt) {
@@ -116,20 +132,20 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
             const float4 pp = a.pos[p], pw = a.pow[p];
             if (front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
                 double w, dwd, dwr;
-                weight_terms(a.filter, dist2_d(pp, qp), r2, (double)a.cone_k, w, dwd, dwr);
+                weight_terms(a.filter, dist2_d(pp, qp), rinv, inv_r2, w, dwd, dwr);
                 S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
                 T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
             }
         }
         a.keys[pair0 + j] = key;
-        a.vals[pair0 + j] = (uint32_t)(pair0 + j);
+        a.vals[pair0 + j] = (ql << 1) | (j == k - 1 ? 1u : 0u);   // the query, and whether p is its k-th
     }
     S0 = warp_sum_d(S0); S1 = warp_sum_d(S1); S2 = warp_sum_d(S2);
     T0 = warp_sum_d(T0); T1 = warp_sum_d(T1); T2 = warp_sum_d(T2);
     if (lane != 0) return;
     BwdQuery rec;
     rec.gx = rec.gy = rec.gz = rec.G = 0.0;
-    rec.r2 = active ? r2 : 0.0;
+    rec.rinv = active ? rinv : 0.0;
     rec.qx = qp.x; rec.qy = qp.y; rec.qz = qp.z;
     rec.nx = qn.x; rec.ny = qn.y; rec.nz = qn.z;
     if (active) {
@@ -175,26 +191,24 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
     if (b < e) {
         const float4 pp = a.pos[p], pw = a.pow[p];
         const uint32_t dir = __float_as_uint(pw.w);
-        const uint32_t k = a.k;
         for (uint32_t i = b; i < e; ++i) {
-            const uint32_t v = sorted_vals[i];
-            const uint32_t ql = v / k, j = v % k;
-            const BwdQuery rec = a.qrec[ql];
-            const double r2 = rec.r2;
-            if (!(r2 > 0.0)) continue;
+            const uint32_t v = sorted_vals[i];   // query << 1 | (the photon is the query's k-th)
+            const BwdQuery rec = a.qrec[v >> 1];
+            const double rinv = rec.rinv;
+            if (!(rinv > 0.0)) continue;
             const double dx = (double)pp.x - (double)rec.qx, dy = (double)pp.y - (double)rec.qy,
                          dz = (double)pp.z - (double)rec.qz;
             const double d2 = dx * dx + dy * dy + dz * dz;
             double coef = 0.0;
             if (front_rn(rec.nx, rec.ny, rec.nz, dir)) {
                 double w, dwd, dwr;
-                weight_terms(a.filter, d2, r2, (double)a.cone_k, w, dwd, dwr);
+                weight_terms(a.filter, d2, rinv, 0.0, w, dwd, dwr);   // dw/dr2 is the per-query pass's
                 g0 += w * rec.gx;
                 g1 += w * rec.gy;
                 g2 += w * rec.gz;
                 coef = (rec.gx * pw.x + rec.gy * pw.y + rec.gz * pw.z) * dwd;
             }
-            if (j == k - 1) coef += rec.G;   // the k-th neighbour sets r^2 of q
+            if (v & 1u) coef += rec.G;   // the k-th neighbour sets r^2 of q
             x0 += 2.0 * coef * dx;
             x1 += 2.0 * coef * dy;
             x2 += 2.0 * coef * dz;

@@ -307,7 +307,8 @@ int scale_rgb(float4* pw, uint32_t n, float scale, cudaStream_t st);
 struct __align__(16) BwdQuery {
     double gx, gy, gz;        // dL/dE * norm per channel
     double G;                 // the k-th neighbour's r^2 path (0 unless k were found)
-    double r2;                // r^2 of the filter (0 = the query carries no gradient)
+    double rinv;              // the filter's reciprocal: 1 / (k_c r) cone, 1 / r^2 Epanechnikov, 1 box;
+                              // 0 = the query carries no gradient
     float qx, qy, qz;         // position
     float nx, ny, nz;         // normal
 };
