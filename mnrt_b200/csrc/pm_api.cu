@@ -1329,7 +1329,7 @@ pm_status batch_build_device(pm_batch* b, const float* d_pos4, const float* d_po
     uint64_t* keys[2] = {bb.keys[0], bb.keys[1]};
     uint32_t* vals[2] = {bb.vals[0], bb.vals[1]};
     const SortGather g{pos, pw, format, P<float4>(m->pos), P<float4>(m->pow), P<uint32_t>(m->inv)};
-    const int cur = n > 1 ? radix_sort_pairs(keys, vals, n, 48 + map_id_bits(maps), bb.scratch, st, &nl, &g) : 0;
+    const int cur = n > 1 ? radix_sort_pairs(keys, vals, n, kMortonBits + map_id_bits(maps), bb.scratch, st, &nl, &g) : 0;
     nl += build_from_sorted(pos, pw, n, format, m->leaf_size, keys[cur], vals[cur], P<float4>(m->pos),
                             P<float4>(m->pow), P<uint32_t>(m->inv), P<Node>(m->nodes), P<MapHeader>(m->hdr), bb, st,
                             n > 1);

@@ -4,7 +4,7 @@
 // PhotonMap::GatherFor); the batch form has no counterpart there.  Photons of
 // all maps sit in one array (map i owns [ph_off_i, ph_off_i + n_i)), and so do
 // the queries.  The build sorts every photon once by the 64-bit key
-//   (map id << 48) | 48-bit Morton code in the map's own cubic cell,
+//   (map id << 39) | 39-bit Morton code in the map's own cubic cell,
 // so one radix tree holds every map: the map id bits split first, and the
 // node whose range is exactly a map's photons roots that map's subtree
 // (k_batch_roots).  The query sorts all queries by (map id << 30) | 30-bit
@@ -116,7 +116,7 @@ __global__ void k_batch_geom(const uint32_t* __restrict__ acc, uint32_t m, Batch
 
 // Query keys: map id above bit 30, Hilbert index in the map's cell (the
 // processing order only; 30 + map-id bits sort in fewer passes than the
-// photons' 48-bit codes).
+// photons' 39-bit codes).
 __global__ void k_batch_query_keys(const float4* __restrict__ pts, const uint32_t* __restrict__ off, uint32_t m,
                                    uint32_t n, const BatchGeom* __restrict__ geom, uint64_t* __restrict__ keys,
                                    uint32_t* __restrict__ vals) {
@@ -129,7 +129,7 @@ __global__ void k_batch_query_keys(const float4* __restrict__ pts, const uint32_
     vals[i] = i;
 }
 
-// Photon keys: map id in bits 48..63, Morton code in the map's cell.
+// Photon keys: map id above bit kMortonBits, Morton code in the map's cell.
 __global__ void k_batch_keys(const float4* __restrict__ pts, const uint32_t* __restrict__ off, uint32_t m, uint32_t n,
                              const BatchGeom* __restrict__ geom, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -137,7 +137,7 @@ __global__ void k_batch_keys(const float4* __restrict__ pts, const uint32_t* __r
     const uint32_t map = map_of(off, m, i);
     const BatchGeom& g = geom[map];
     const float4 p = pts[i];
-    keys[i] = ((uint64_t)map << 48) | morton48(p.x, p.y, p.z, g.lo, g.mscale);
+    keys[i] = ((uint64_t)map << kMortonBits) | morton39(p.x, p.y, p.z, g.lo, g.mscale);
     vals[i] = i;
 }
 

@@ -8,7 +8,7 @@
 //
 //   1. k_bounds       photon bounds + largest flux channel (one pass, last
 //                     block finalises the header)
-//   2. k_morton       48-bit Morton code per photon in the cubic root cell
+//   2. k_morton       39-bit Morton code per photon in the cubic root cell
 //   3. radix sort     (code, caller index): caller index breaks ties, so the
 //                     order -- and the whole tree -- is deterministic
 //                     (the reference picks sides of split-plane ties at
@@ -139,7 +139,7 @@ __global__ void k_morton(const float4* __restrict__ pos, uint32_t n, const MapHe
     if (i >= n) return;
     const float scale = morton_scale(hdr);
     const float4 p = pos[i];
-    keys[i] = morton48(p.x, p.y, p.z, hdr->lo, scale);
+    keys[i] = morton39(p.x, p.y, p.z, hdr->lo, scale);
     vals[i] = i;
 }
 
@@ -449,7 +449,7 @@ int build_map(const float4* in_pos, const float4* in_pow, uint32_t n, int format
         ++nl;
         // the last pass moves the photons into tree order (n >= 2; one photon is not sorted)
         const SortGather g{in_pos, in_pow, format, out_pos, out_pow, inv};
-        cur = radix_sort_pairs(keys, vals, n, 48, bb.scratch, st, &nl, n > 1 ? &g : nullptr);
+        cur = radix_sort_pairs(keys, vals, n, kMortonBits, bb.scratch, st, &nl, n > 1 ? &g : nullptr);
     }
     if (sort_done) cudaEventRecord(sort_done, st);
     nl += build_from_sorted(in_pos, in_pow, n, format, leaf_size, keys[cur], vals[cur], out_pos, out_pow, inv, nodes,

@@ -329,11 +329,12 @@ def test_autotune_keeps_results_exact(cuda, oracle_mod):
     check_against_oracle(oracle_mod, ph, q, res, 64, 0.05, "cone")
 
 
-def _morton48(p, lo, scale):
-    """Host restatement of the engine's 48-bit Morton code (16 bits per axis)."""
+def _morton39(p, lo, scale):
+    """Host restatement of the engine's 39-bit Morton code: the top 13 bits of
+    each axis' 16-bit quantisation, interleaved with x most significant."""
     q = np.clip((p[:, :3].astype(np.float32) - lo.astype(np.float32)).astype(np.float32) * np.float32(scale),
                 0.0, 65535.0).astype(np.float32)
-    q = np.nan_to_num(q).astype(np.uint64)
+    q = np.nan_to_num(q).astype(np.uint64) >> np.uint64(3)
 
     def spread(v):
         v = v & np.uint64(0xFFFF)
@@ -365,7 +366,7 @@ def test_radix_sort_and_scan_through_tree_order(cuda, n):
     ext = np.float32(max(hi - lo))
     scale = np.float32(65536.0) / ext if ext > 0 else np.float32(0)
     idx = tpos[:, 3].view(np.uint32)
-    codes = _morton48(ph.pos[idx], lo, scale)
+    codes = _morton39(ph.pos[idx], lo, scale)
     dc = np.diff(codes.astype(np.int64))
     di = np.diff(idx.astype(np.int64))
     assert ((dc > 0) | ((dc == 0) & (di > 0))).all(), "tree order is not (code, index) order"
