@@ -962,6 +962,14 @@ constexpr int kWideStack = 192;   // entries of 2 words: first child slot, stack
 // every query visits them first.
 constexpr int kTopBytes = 32 * (int)sizeof(ChildSlot);
 
+// The search's threshold test is strict until a selection has run and
+// inclusive after (x < thr, then x <= thr).  For the non-negative bounds and
+// distances compared, x <= thr is x < the next float above thr, so one
+// exclusive bound gives both as a single comparison.
+__device__ __forceinline__ float excl_bound(float thr, bool selected) {
+    return (selected && thr < INFINITY) ? __uint_as_float(__float_as_uint(thr) + 1u) : thr;
+}
+
 // One 32-photon half of a leaf: this lane's photon at tree position idx,
 // at squared distance d2 from the query, when `have`.
 __device__ __forceinline__ void scan_half(const KnnArgs& a, float d2, bool have, uint32_t idx, uint32_t k, uint32_t C,
@@ -972,7 +980,7 @@ __device__ __forceinline__ void scan_half(const KnnArgs& a, float d2, bool have,
         selected = true;
         thr = __uint_as_float((uint32_t)(T >> 32));
     }
-    const bool acc = have && (selected ? (d2 <= thr) : (d2 < thr));
+    const bool acc = have && d2 < excl_bound(thr, selected);
     const uint32_t bal = __ballot_sync(kFull, acc);
     // appends only; readers of the buffer (a selection, the finish) sync before they read
     if (acc) buf[n + __popc(bal & lt)] = ((uint64_t)__float_as_uint(d2) << 32) | idx;
@@ -1014,7 +1022,7 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         load_root(a.root, lo, hi, ref, cnt);
         if (ref == kInvalid) return;
         const float lb = box_lb(qx, qy, qz, lo, hi);
-        if (!(selected ? lb <= thr : lb < thr)) return;
+        if (!(lb < excl_bound(thr, selected))) return;
         if (cnt & kWideFlag) {
             if (lane == 0) reinterpret_cast<uint2*>(stack)[0] = make_uint2(ref, stack_word(lb, cnt & kWideCount));
             sp = 1;
@@ -1031,7 +1039,8 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         const uint32_t kids = e1 & 63u;
         const float plb = __uint_as_float(e1 & ~63u);
         __syncwarp();
-        if (!(selected ? plb <= thr : plb < thr)) continue;
+        const float thx = excl_bound(thr, selected);   // the node's children are tested against the same bound
+        if (!(plb < thx)) continue;
         float lo[3], hi[3];
         uint32_t ref = kInvalid, cnt = 0;
         if (lane < kids) {
@@ -1048,7 +1057,7 @@ __device__ __forceinline__ void wide_traverse(const KnnArgs& a, float qx, float 
         bool pass = false;
         if (ref != kInvalid) {
             lb = box_lb(qx, qy, qz, lo, hi);
-            pass = selected ? lb <= thr : lb < thr;
+            pass = lb < thx;
         }
         const bool is_wide = (cnt & kWideFlag) != 0;
         const uint32_t intm = __ballot_sync(kFull, pass && is_wide);
