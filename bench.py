@@ -759,7 +759,17 @@ def run_batch(args) -> dict | None:
     if mine:
         batch = PhotonMapBatch()
         out = batch.outputs(descs, qoff, dev)
-        bt = batch.autotune(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
+        if args.leaf or args.wpb or args.rounds or args.layout >= 0:   # a fixed setting (profiling runs)
+            wide = args.layout == 2 if args.layout >= 0 else True
+            batch.set_tuning(leaf_size=args.leaf or 32, warps_per_block=args.wpb or 4,
+                             rounds_per_chunk=args.rounds or 8, wide=wide)
+            bt = {"leaf_size": args.leaf or 32, "warps_per_block": args.wpb or 4,
+                  "rounds_per_chunk": args.rounds or 8, "wide_tree": wide, "chosen_by": "command line"}
+        else:
+            t = batch.autotune(d_pos, d_pw, poff, descs, d_qp, d_qn, qoff, out)
+            bt = {"leaf_size": t.leaf_size, "warps_per_block": t.warps_per_block,
+                  "rounds_per_chunk": t.rounds_per_chunk, "wide_tree": t.kbuf_layout == 2,
+                  "chosen_by": "pm_batch_autotune (rank 0)"}
 
         def eager():
             batch.build(d_pos, d_pw, poff)
@@ -791,9 +801,7 @@ def run_batch(args) -> dict | None:
         "sequential_queries_per_s": Q_all / (seq_ms / 1000.0), "batched_eager_queries_per_s": Q_all / (eager_ms / 1000.0),
         "speedup_graph_over_sequential": seq_ms / graph_ms, "device_errors": int(errors),
         "clocks": clock_runs[-1] if clock_runs else None,
-        "batch_tuning": None if bt is None else {
-            "leaf_size": bt.leaf_size, "warps_per_block": bt.warps_per_block, "rounds_per_chunk": bt.rounds_per_chunk,
-            "wide_tree": bt.kbuf_layout == 2, "chosen_by": "pm_batch_autotune (rank 0)"},
+        "batch_tuning": bt,
     }
 
 

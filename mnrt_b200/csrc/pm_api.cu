@@ -52,7 +52,7 @@ struct pm_map {
     DevBuf stats;           // query counters (profiling level 2)
     // backward (pm_query_backward): pair sort, per-query records, segments,
     // FP64 running sums, and the forward outputs when the kNN is recomputed
-    DevBuf bkeys0, bkeys1, bvals0, bvals1, bscratch, qrec, seg_start, seg_end, acc;
+    DevBuf bvals, bscratch, qrec, seg_start, seg_end, acc;
     DevBuf rnbr, rcnt, rr2, rrad;
     DevBuf gnrm, gest;        // pm_gather_for: flipped normals, estimates
     // PM_MODE_ZHOU_COMPAT: node radius estimates of the current tree, kept
@@ -331,7 +331,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
                      &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wcnt, &m->wfirst,
                      &m->wchild, &m->wroot, &m->wscan, &m->rootmark, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
-                     &m->qscratch, &m->counter, &m->fixq, &m->qsorted, &m->stats, &m->bkeys0, &m->bkeys1, &m->bvals0, &m->bvals1,
+                     &m->qscratch, &m->counter, &m->fixq, &m->qsorted, &m->stats, &m->bvals,
                      &m->bscratch, &m->qrec, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
                      &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
@@ -649,11 +649,8 @@ static pm_status ensure_bwd_capacity(pm_map* m, uint32_t chunk_q, uint32_t k, bo
 #define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
     const uint64_t pc = pairs ? pairs : 1;
     const size_t qc = chunk_q ? chunk_q : 1;
-    ENSURE(bkeys0, pc * sizeof(uint32_t));
-    ENSURE(bkeys1, pc * sizeof(uint32_t));
-    ENSURE(bvals0, pc * sizeof(uint32_t));
-    ENSURE(bvals1, pc * sizeof(uint32_t));
-    ENSURE(bscratch, bwd_sort_scratch_words(pc) * sizeof(uint32_t));
+    ENSURE(bvals, pc * sizeof(uint32_t));
+    ENSURE(bscratch, bwd_scratch_words(n) * sizeof(uint32_t));
     ENSURE(qrec, qc * sizeof(BwdQuery));
     ENSURE(seg_start, (size_t)n * sizeof(uint32_t));
     ENSURE(seg_end, (size_t)n * sizeof(uint32_t));
@@ -691,7 +688,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     if (m->n == 0) return PM_OK;   // no photons: nothing to differentiate
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t k = desc->k;
-    const uint64_t kMaxPairs = 1ull << 27;   // pairs sorted at once (about 2 GB of sort buffers)
+    const uint64_t kMaxPairs = 1ull << 27;   // neighbour pairs per chunk (512 MB of pair slots)
     uint32_t chunk = (uint32_t)(kMaxPairs / k);
     if (m->bwd_chunk) chunk = m->bwd_chunk < chunk ? m->bwd_chunk : chunk;
     if (nq > 0 && chunk > nq) chunk = nq;
@@ -714,11 +711,10 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     a.cone_k = desc->filter == PM_FILTER_CONE ? desc->cone_k : 1.0f;
     a.min_found = desc->min_found;
     a.qrec = P<BwdQuery>(m->qrec);
-    a.keys = nullptr; a.vals = nullptr;
+    a.vals = nullptr; a.cursor = nullptr; a.pair_cap = 0;
     a.nbr = nullptr; a.count_in = nullptr; a.order = nullptr;
     BwdBuffers b;
-    b.keys[0] = P<uint32_t>(m->bkeys0); b.keys[1] = P<uint32_t>(m->bkeys1);
-    b.vals[0] = P<uint32_t>(m->bvals0); b.vals[1] = P<uint32_t>(m->bvals1);
+    b.vals = P<uint32_t>(m->bvals);
     b.scratch = P<uint32_t>(m->bscratch);
     b.seg_start = P<uint32_t>(m->seg_start); b.seg_end = P<uint32_t>(m->seg_end);
     b.acc = P<double>(m->acc);

@@ -16,16 +16,19 @@
 // leaving N(q)) are measure-zero kinks and contribute nothing.
 //
 // Scatter without float atomics, deterministic by construction:
-//   1. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
+//   1. k_bwd_count  warp per query: counts every photon's pairs (the
+//                   neighbour slots of queries that carry gradient)
+//   2. exclusive scan of the counts: every photon's segment [start, end)
+//   3. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
 //                   -> per-query record (g * norm, G, the filter's
-//                   reciprocal, position, normal), and one key-value per
-//                   neighbour slot: photon tree position, query << 1 | (the
-//                   photon is the query's k-th); empty slots get the
-//                   sentinel key n
-//   2. stable LSD radix sort by photon (the values of one photon stay in
-//      query order)
-//   3. k_bwd_bounds segment [start, end) of every photon in the sorted array
-//   4. k_bwd_reduce thread per photon: walks its segment in order and sums
+//                   reciprocal, position, normal), and every pair's value
+//                   (query << 1 | the photon is the query's k-th) put into
+//                   its photon's segment at an atomic cursor
+//   4. k_bwd_segsort warp per photon: sorts its segment's values (bitonic
+//                   network in registers up to 256 values), which restores
+//                   the query order the cursor lost: the segment then holds
+//                   exactly what a stable sort of the pairs by photon gives
+//   5. k_bwd_reduce thread per photon: walks its segment in order and sums
 //                   the FP64 contributions; the running sum carries across
 //                   query chunks, so chunked and single-pass runs give the
 //                   same bits
@@ -88,14 +91,60 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+// The head of one query, shared by the counting pass and the per-query pass
+// so that both take the same pairs: the neighbours found (the count output,
+// else the valid prefix of the row), r^2 (d^2 of the k-th when k were found,
+// else R^2) and whether the query carries gradient.
+struct BwdHead {
+    float4 qp;
+    double r2;
+    uint32_t cnt;
+    bool active;
+};
+
+__device__ __forceinline__ BwdHead bwd_head(const BwdArgs& a, uint32_t ql, uint32_t q, uint32_t lane) {
+    const uint32_t k = a.k;
+    const uint32_t* row = a.nbr + (size_t)ql * k;
+    BwdHead h;
+    if (a.count_in) {
+        h.cnt = a.count_in[ql];
+    } else {
+        uint32_t c = 0;
+        for (uint32_t j = lane; j < k; j += 32) c += row[j] != kInvalid ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        h.cnt = c;
+    }
+    if (h.cnt > k) h.cnt = k;
+    h.qp = a.qpos[q];
+    h.r2 = (double)a.r_max * (double)a.r_max;
+    if (h.cnt == k) h.r2 = dist2_d(a.pos[a.inv[row[k - 1]]], h.qp);
+    h.active = h.cnt > 0 && h.cnt >= a.min_found && h.r2 > 0.0 && isfinite(h.qp.x) && isfinite(h.qp.y) &&
+               isfinite(h.qp.z);
+    return h;
+}
+
+// Warp per query: one count per pair on its photon's cursor (the cursors are
+// cleared before; the scan then turns the counts into segment starts).
+__global__ void __launch_bounds__(256) k_bwd_count(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
+    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp_global >= nq_chunk) return;
+    const uint32_t ql = a.order ? a.order[warp_global] : warp_global;
+    const BwdHead h = bwd_head(a, ql, q0 + ql, lane);
+    if (!h.active) return;
+    const uint32_t* row = a.nbr + (size_t)ql * a.k;
+    for (uint32_t j = lane; j < h.cnt; j += 32) atomicAdd(&a.cursor[a.inv[row[j]]], 1u);
+}
+
 // One warp per query of the chunk, taken in Hilbert order when a.order is
 // set: neighbouring warps then gather neighbouring photons, which L1 and L2
-// serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records and pairs stay at the
-// caller's index, so the results do not depend on the order.  The warp also
-// writes the query's k (photon tree position, query | k-th flag) keys and values for
-// the sort by photon (empty slots and queries without gradient get the
-// sentinel key n, which sorts after every photon): the neighbour rows and
-// the inverse permutation are read once, here.
+// serve (1M queries, k = 64: 1.48 -> 1.26 ms).  Records stay at the caller's
+// index and every pair's value names the caller's index, so the results do
+// not depend on the order.  The warp puts each pair's value into its
+// photon's segment at the photon's cursor (the segment start after the scan);
+// the cursor ends at the segment's end.  The slot is taken before the FP64
+// math, so the atomic's latency overlaps it.
 __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -103,42 +152,26 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     const uint32_t ql = a.order ? a.order[warp_global] : warp_global, q = q0 + ql;
     const uint32_t k = a.k;
     const uint32_t* row = a.nbr + (size_t)ql * k;
-    // neighbours found: the count output, else the valid prefix of the row
-    uint32_t cnt;
-    if (a.count_in) {
-        cnt = a.count_in[ql];
-    } else {
-        uint32_t c = 0;
-        for (uint32_t j = lane; j < k; j += 32) c += row[j] != kInvalid ? 1u : 0u;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        cnt = c;
-    }
-    if (cnt > k) cnt = k;
-    const float4 qp = a.qpos[q];
+    const BwdHead h = bwd_head(a, ql, q, lane);
+    const float4 qp = h.qp;
     const float4 qn = a.qnrm[q];
-    const double R2 = (double)a.r_max * (double)a.r_max;
-    double r2 = R2;
-    if (cnt == k) r2 = dist2_d(a.pos[a.inv[row[k - 1]]], qp);
-    const bool active = cnt > 0 && cnt >= a.min_found && r2 > 0.0 && isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
+    const double r2 = h.r2;
+    const bool active = h.active;
+    const uint32_t cnt = h.cnt;
     double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
-    const uint64_t pair0 = (uint64_t)ql * k;
     const double rinv = filter_rinv(a.filter, r2, (double)a.cone_k), inv_r2 = 1.0 / r2;
-    for (uint32_t j = lane; j < k; j += 32) {
-        uint32_t key = a.n;
-        if (active && j < cnt) {
-            const uint32_t p = a.inv[row[j]];
-            key = p;
-            const float4 pp = a.pos[p], pw = a.pow[p];
-            if (front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
-                double w, dwd, dwr;
-                weight_terms(a.filter, dist2_d(pp, qp), rinv, inv_r2, w, dwd, dwr);
-                S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
-                T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
-            }
+    const uint32_t jend = active ? cnt : 0u;
+    for (uint32_t j = lane; j < jend; j += 32) {
+        const uint32_t p = a.inv[row[j]];
+        const uint32_t slot = atomicAdd(&a.cursor[p], 1u);
+        const float4 pp = a.pos[p], pw = a.pow[p];
+        if (front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
+            double w, dwd, dwr;
+            weight_terms(a.filter, dist2_d(pp, qp), rinv, inv_r2, w, dwd, dwr);
+            S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
+            T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
         }
-        a.keys[pair0 + j] = key;
-        a.vals[pair0 + j] = (ql << 1) | (j == k - 1 ? 1u : 0u);   // the query, and whether p is its k-th
+        if (slot < a.pair_cap) a.vals[slot] = (ql << 1) | (j == k - 1 ? 1u : 0u);   // the query, and whether p is its k-th
     }
     S0 = warp_sum_d(S0); S1 = warp_sum_d(S1); S2 = warp_sum_d(S2);
     T0 = warp_sum_d(T0); T1 = warp_sum_d(T1); T2 = warp_sum_d(T2);
@@ -163,16 +196,97 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     a.qrec[ql] = rec;
 }
 
-// Segment bounds of every photon in the sorted keys (start = end = 0 when
-// the photon has no pair; both arrays are cleared before).
-__global__ void k_bwd_bounds(const uint32_t* __restrict__ keys, uint64_t m, uint32_t n, uint32_t* __restrict__ start,
-                             uint32_t* __restrict__ end) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    const uint32_t key = keys[i];
-    if (key >= n) return;
-    if (i == 0 || keys[i - 1] != key) start[key] = (uint32_t)i;
-    if (i + 1 == m || keys[i + 1] != key) end[key] = (uint32_t)(i + 1);
+// Ascending bitonic network over the 32 R slots of a warp, slot lane R + r in
+// v[r] (the all-ascending form: the first step of every merge compares a slot
+// with its mirror in the block, i ^ (kk - 1), the others i with i ^ j).
+template <int R>
+__device__ __forceinline__ void warp_bitonic(uint32_t (&v)[R], uint32_t lane) {
+#pragma unroll
+    for (int kk = 2; kk <= 32 * R; kk <<= 1) {
+#pragma unroll
+        for (int j = kk / 2; j > 0; j >>= 1) {
+            const bool flip = j == kk / 2;
+            if ((flip ? kk - 1 : j) < R) {   // partner in the same lane
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int o = flip ? (r ^ (kk - 1)) : (r ^ j);
+                    if (o > r) {
+                        const uint32_t lo = min(v[r], v[o]), hi = max(v[r], v[o]);
+                        v[r] = lo;
+                        v[o] = hi;
+                    }
+                }
+            } else {   // partner in lane ^ lm; the lower slot keeps the minimum
+                const int lm = flip ? kk / R - 1 : j / R;
+                const bool lower = (lane & (uint32_t)(flip ? kk / (2 * R) : j / R)) == 0;
+                uint32_t w[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) w[r] = __shfl_xor_sync(0xffffffffu, v[flip ? R - 1 - r : r], lm);
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[r] = lower ? min(v[r], w[r]) : max(v[r], w[r]);
+            }
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void sort_segment_regs(uint32_t* seg, uint32_t m, uint32_t lane) {
+    uint32_t v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t i = lane * R + r;
+        v[r] = i < m ? seg[i] : 0xffffffffu;   // padding sorts last
+    }
+    warp_bitonic<R>(v, lane);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t i = lane * R + r;
+        if (i < m) seg[i] = v[r];
+    }
+}
+
+// Segments above 256 values: the same network in place over the next power
+// of two, the slots at and above m read as +infinity (a pair whose upper
+// slot is past m is already in order); L2 loads and stores, a warp barrier
+// between steps.
+__device__ __forceinline__ void sort_segment_global(uint32_t* seg, uint32_t m, uint32_t lane) {
+    uint32_t P = 1;
+    while (P < m) P <<= 1;
+    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
+        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = lane; t < (P >> 1); t += 32) {
+                const uint32_t i = (t / j) * 2 * j + (t % j);   // bit j of i clear
+                const uint32_t o = j == (kk >> 1) ? (i ^ (kk - 1)) : (i + j);
+                if (o < m) {
+                    const uint32_t x = __ldcg(seg + i), y = __ldcg(seg + o);
+                    if (x > y) {
+                        __stcg(seg + i, y);
+                        __stcg(seg + o, x);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Warp per photon: sorts the values of its segment (distinct: a photon is
+// in a query's list at most once), so the segment lists its queries in
+// caller order.
+__global__ void __launch_bounds__(256, 8) k_bwd_segsort(const uint32_t* __restrict__ start,
+                                                        const uint32_t* __restrict__ end, uint32_t n,
+                                                        uint64_t cap, uint32_t* __restrict__ vals) {
+    const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (p >= n) return;
+    const uint32_t e = (uint32_t)min((uint64_t)end[p], cap), b = min(start[p], e), m = e - b;
+    if (m < 2) return;
+    uint32_t* seg = vals + b;
+    if (m <= 32) sort_segment_regs<1>(seg, m, lane);
+    else if (m <= 64) sort_segment_regs<2>(seg, m, lane);
+    else if (m <= 128) sort_segment_regs<4>(seg, m, lane);
+    else if (m <= 256) sort_segment_regs<8>(seg, m, lane);
+    else sort_segment_global(seg, m, lane);
 }
 
 // One thread per photon (tree position).  acc holds 6 doubles per photon
@@ -187,7 +301,7 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
         const double* s = acc + (size_t)p * 6;
         g0 = s[0]; g1 = s[1]; g2 = s[2]; x0 = s[3]; x1 = s[4]; x2 = s[5];
     }
-    const uint32_t b = start[p], e = end[p];
+    const uint32_t e = (uint32_t)min((uint64_t)end[p], a.pair_cap), b = start[p];   // the cap: pair slots held
     if (b < e) {
         const float4 pp = a.pos[p], pw = a.pow[p];
         const uint32_t dir = __float_as_uint(pw.w);
@@ -224,39 +338,38 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
     }
 }
 
-int key_bits_for(uint32_t n) {
-    int b = 1;
-    while (b < 32 && (1ull << b) <= (uint64_t)n) ++b;   // sentinel n must fit
-    return b;
-}
-
 }  // namespace
 
-size_t bwd_sort_scratch_words(uint64_t pairs) { return sort_scratch_words((uint32_t)pairs) + 64; }
+size_t bwd_scratch_words(uint32_t n) { return scan_scratch_words(n) + 1; }
 
 int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
                    float4* grad_pow, float4* grad_pos, cudaStream_t st) {
     int nl = 0;
-    const uint64_t pairs = (uint64_t)nq_chunk * a.k;
     BwdArgs x = a;
-    x.keys = b.keys[0];
-    x.vals = b.vals[0];
+    x.vals = b.vals;
+    x.cursor = b.seg_end;
+    x.pair_cap = (uint64_t)nq_chunk * a.k;
+    const uint32_t warps_per_block = 8;
+    const uint32_t qblocks = (nq_chunk + warps_per_block - 1) / warps_per_block;
+    cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
     if (nq_chunk > 0) {
-        const uint32_t warps_per_block = 8;
-        k_bwd_prep<<<(nq_chunk + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
+        k_bwd_count<<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
         ++nl;
     }
-    uint32_t* keys[2] = {b.keys[0], b.keys[1]};
-    uint32_t* vals[2] = {b.vals[0], b.vals[1]};
-    const int cur = radix_sort_pairs32(keys, vals, (uint32_t)pairs, key_bits_for(a.n), b.scratch, st, &nl);
-    cudaMemsetAsync(b.seg_start, 0, (size_t)a.n * sizeof(uint32_t), st);
-    cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
-    if (pairs > 0) {
-        k_bwd_bounds<<<(uint32_t)((pairs + 255) / 256), 256, 0, st>>>(keys[cur], pairs, a.n, b.seg_start, b.seg_end);
+    // counts -> segment starts; the cursors start there and end at the ends
+    nl += exclusive_scan(b.seg_end, b.seg_end, a.n, b.scratch, nullptr, st);
+    cudaMemcpyAsync(b.seg_start, b.seg_end, (size_t)a.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    if (nq_chunk > 0) {
+        k_bwd_prep<<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
         ++nl;
     }
     if (a.n > 0) {
-        k_bwd_reduce<<<(a.n + 127) / 128, 128, 0, st>>>(x, q0, vals[cur], b.seg_start, b.seg_end, first ? 1 : 0,
+        if (nq_chunk > 0) {
+            k_bwd_segsort<<<(a.n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
+                b.seg_start, b.seg_end, a.n, x.pair_cap, b.vals);
+            ++nl;
+        }
+        k_bwd_reduce<<<(a.n + 127) / 128, 128, 0, st>>>(x, q0, b.vals, b.seg_start, b.seg_end, first ? 1 : 0,
                                                         last ? 1 : 0, b.acc, grad_pow, grad_pos);
         ++nl;
     }

@@ -329,19 +329,19 @@ struct BwdArgs {
     float cone_k;
     uint32_t min_found;
     BwdQuery* qrec;           // per chunk query: the record the per-photon pass reads
-    uint32_t* keys;           // pair keys / values (set by backward_chunk)
-    uint32_t* vals;
+    uint32_t* vals;           // pair values grouped by photon (set by backward_chunk)
+    uint32_t* cursor;         // per photon: pair count, then the next free slot of its segment
+    uint64_t pair_cap;        // slots in vals
     const uint32_t* order;    // the chunk's queries in Hilbert order (chunk-local ids), or nullptr
 };
 struct BwdBuffers {
-    uint32_t* keys[2];
-    uint32_t* vals[2];
-    uint32_t* scratch;
+    uint32_t* vals;           // one slot per neighbour pair of a chunk
+    uint32_t* scratch;        // the scan of the per-photon counts
     uint32_t* seg_start;
     uint32_t* seg_end;
     double* acc;              // 6 doubles per photon, carried between chunks
 };
-size_t bwd_sort_scratch_words(uint64_t pairs);
+size_t bwd_scratch_words(uint32_t n);
 int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
                    float4* grad_pow, float4* grad_pos, cudaStream_t st);
 
