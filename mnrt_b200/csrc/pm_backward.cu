@@ -17,7 +17,9 @@
 //
 // Scatter without float atomics, deterministic by construction:
 //   1. k_bwd_count  warp per query: counts every photon's pairs (the
-//                   neighbour slots of queries that carry gradient)
+//                   listed neighbours of queries with cnt >= max(1,
+//                   min_found); the per-photon pass skips the pairs of
+//                   queries that carry no gradient)
 //   2. exclusive scan of the counts: every photon's segment [start, end)
 //   3. k_bwd_prep   warp per query: FP64 S, T sums over the neighbour list
 //                   -> per-query record (g * norm, G, the filter's
@@ -102,20 +104,33 @@ struct BwdHead {
     bool active;
 };
 
+// Neighbours found by query ql: the count output, else the valid prefix of
+// its row (warp-wide).
+__device__ __forceinline__ uint32_t bwd_found(const BwdArgs& a, uint32_t ql, uint32_t lane) {
+    const uint32_t k = a.k;
+    uint32_t c = 0;
+    if (a.count_in) {
+        c = a.count_in[ql];
+    } else {
+        const uint32_t* row = a.nbr + (size_t)ql * k;
+        for (uint32_t j = lane; j < k; j += 32) c += row[j] != kInvalid ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    return c < k ? c : k;
+}
+
+// The pairs that go into the photons' segments: every listed neighbour of a
+// query with cnt >= max(1, min_found).  A superset of the pairs that carry
+// gradient (the per-photon pass skips those of queries whose record has no
+// filter reciprocal), decided without the query's position or r^2.
+__device__ __forceinline__ bool bwd_placed(const BwdArgs& a, uint32_t cnt) { return cnt > 0 && cnt >= a.min_found; }
+
 __device__ __forceinline__ BwdHead bwd_head(const BwdArgs& a, uint32_t ql, uint32_t q, uint32_t lane) {
     const uint32_t k = a.k;
     const uint32_t* row = a.nbr + (size_t)ql * k;
     BwdHead h;
-    if (a.count_in) {
-        h.cnt = a.count_in[ql];
-    } else {
-        uint32_t c = 0;
-        for (uint32_t j = lane; j < k; j += 32) c += row[j] != kInvalid ? 1u : 0u;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        h.cnt = c;
-    }
-    if (h.cnt > k) h.cnt = k;
+    h.cnt = bwd_found(a, ql, lane);
     h.qp = a.qpos[q];
     h.r2 = (double)a.r_max * (double)a.r_max;
     if (h.cnt == k) h.r2 = dist2_d(a.pos[a.inv[row[k - 1]]], h.qp);
@@ -124,17 +139,19 @@ __device__ __forceinline__ BwdHead bwd_head(const BwdArgs& a, uint32_t ql, uint3
     return h;
 }
 
-// Warp per query: one count per pair on its photon's cursor (the cursors are
-// cleared before; the scan then turns the counts into segment starts).
+// Warp per query, in caller order: one count per placed pair on its
+// photon's cursor (the cursors are cleared before; the scan then turns the
+// counts into segment starts).  Two dependent loads per pair (row, inverse
+// permutation) and no per-query gathers: the pass is latency-bound.
 __global__ void __launch_bounds__(256) k_bwd_count(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
-    const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    (void)q0;
+    const uint32_t ql = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
-    if (warp_global >= nq_chunk) return;
-    const uint32_t ql = a.order ? a.order[warp_global] : warp_global;
-    const BwdHead h = bwd_head(a, ql, q0 + ql, lane);
-    if (!h.active) return;
+    if (ql >= nq_chunk) return;
+    const uint32_t cnt = bwd_found(a, ql, lane);
+    if (!bwd_placed(a, cnt)) return;
     const uint32_t* row = a.nbr + (size_t)ql * a.k;
-    for (uint32_t j = lane; j < h.cnt; j += 32) atomicAdd(&a.cursor[a.inv[row[j]]], 1u);
+    for (uint32_t j = lane; j < cnt; j += 32) atomicAdd(&a.cursor[a.inv[row[j]]], 1u);
 }
 
 // One warp per query of the chunk, taken in Hilbert order when a.order is
@@ -160,12 +177,12 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     const uint32_t cnt = h.cnt;
     double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
     const double rinv = filter_rinv(a.filter, r2, (double)a.cone_k), inv_r2 = 1.0 / r2;
-    const uint32_t jend = active ? cnt : 0u;
+    const uint32_t jend = bwd_placed(a, cnt) ? cnt : 0u;
     for (uint32_t j = lane; j < jend; j += 32) {
         const uint32_t p = a.inv[row[j]];
         const uint32_t slot = atomicAdd(&a.cursor[p], 1u);
         const float4 pp = a.pos[p], pw = a.pow[p];
-        if (front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
+        if (active && front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
             double w, dwd, dwr;
             weight_terms(a.filter, dist2_d(pp, qp), rinv, inv_r2, w, dwd, dwr);
             S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
@@ -305,9 +322,19 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
     if (b < e) {
         const float4 pp = a.pos[p], pw = a.pow[p];
         const uint32_t dir = __float_as_uint(pw.w);
+        // software pipeline: the next entry's record and the value after it
+        // load while this entry's math runs (the sums keep their order)
+        uint32_t vnext = sorted_vals[b];   // query << 1 | (the photon is the query's k-th)
+        BwdQuery rnext = a.qrec[vnext >> 1];
+        uint32_t vafter = b + 1 < e ? sorted_vals[b + 1] : 0u;
         for (uint32_t i = b; i < e; ++i) {
-            const uint32_t v = sorted_vals[i];   // query << 1 | (the photon is the query's k-th)
-            const BwdQuery rec = a.qrec[v >> 1];
+            const uint32_t v = vnext;
+            const BwdQuery rec = rnext;
+            if (i + 1 < e) {
+                vnext = vafter;
+                rnext = a.qrec[vafter >> 1];
+                vafter = i + 2 < e ? sorted_vals[i + 2] : 0u;
+            }
             const double rinv = rec.rinv;
             if (!(rinv > 0.0)) continue;
             const double dx = (double)pp.x - (double)rec.qx, dy = (double)pp.y - (double)rec.qy,
