@@ -254,10 +254,10 @@ PM_API pm_status pm_query_noalloc(pm_map* map, const pm_query_desc* desc, const 
  *          the same desc); d_nbr == NULL recomputes the kNN in chunks.
  *   d_r2:  not read (r^2 is re-derived in FP64 from the k-th neighbour).
  * Position gradients flow through the filter weights and through r^2, which
- * the k-th neighbour sets.  Contributions are evaluated in FP64 and scattered
- * by a sort by photon plus an ordered segmented sum (no float atomics): the
- * result is bitwise reproducible, and identical with or without reuse and
- * for any chunking. */
+ * the k-th neighbour sets.  Contributions are evaluated in FP64 and summed
+ * per photon in query order (pairs grouped by photon, each photon's segment
+ * sorted; no float atomics): the result is bitwise reproducible, and
+ * identical with or without reuse and for any chunking. */
 PM_API pm_status pm_query_backward(pm_map* map, const pm_query_desc* desc, const float* d_qpos4,
                             const float* d_qnrm4, uint32_t nq, const float* d_grad_rad4, const uint32_t* d_nbr,
                             const float* d_r2, const uint32_t* d_count, float* d_grad_pow4, float* d_grad_pos4,

@@ -267,8 +267,8 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const Key* __res
 }
 
 // Up to this many tiles (4M keys) a pass scans the digit rows with one
-// launch of 256 blocks; above it a block walks its long row serially (the
-// adjoint's 67M-pair sort measured 0.27 ms slower with row scans), and the
+// launch of 256 blocks; above it a block walks its long row serially (a
+// 3-pass sort of 67M pairs measured 0.27 ms slower with row scans), and the
 // generic scan of the whole digit-major array (three launches, every SM
 // busy) takes over.
 constexpr uint32_t kRowScanMaxTiles = 2048;
