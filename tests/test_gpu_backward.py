@@ -119,6 +119,29 @@ def test_backward_min_found_and_edges(cuda, oracle_mod):
     assert rel_err(res["gpos"][:, :3], hx, 1e-6).max() <= RTOL_HOST
 
 
+@pytest.mark.parametrize("n", [2000, 10000])
+def test_backward_long_segments(cuda, oracle_mod, n):
+    """Photons in hundreds of neighbour lists (few photons, many queries, a
+    wide radius): the adjoint sorts each photon's segment of pairs with a
+    256-slot register network when it holds 129-256 values and in place
+    through L2 above that; both must give the host gradient, and chunking
+    must not change a bit."""
+    k, r = 64, 0.5
+    ph, q, t, idx, cnt = setup_problem(oracle_mod, n, 30000, k, r, "epanechnikov", seed=97)
+    seg = np.bincount(idx[idx != np.uint32(0xFFFFFFFF)].astype(np.int64), minlength=n)
+    assert (seg > 256).any()
+    if n == 10000:
+        assert ((seg > 128) & (seg <= 256)).any()
+    res = engine_grads(cuda, ph, q, t, k, r, "epanechnikov")
+    assert np.array_equal(res["nbr"], idx) and np.array_equal(res["count"], cnt)
+    hp, hx = oracle_mod.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, res["g"][:, :3].astype(np.float64),
+                                      "epanechnikov")
+    assert rel_err(res["gpow"][:, :3], hp, 1e-6).max() <= RTOL_HOST
+    assert rel_err(res["gpos"][:, :3], hx, 1e-6).max() <= RTOL_HOST
+    chunked = engine_grads(cuda, ph, q, t, k, r, "epanechnikov", chunk=7001)
+    assert np.array_equal(res["gpow"], chunked["gpow"]) and np.array_equal(res["gpos"], chunked["gpos"])
+
+
 def test_autograd_wrapper(cuda, oracle_mod):
     from mnrt_b200.autograd import RadianceEstimate
     k, r = 16, 0.06
