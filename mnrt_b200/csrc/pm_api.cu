@@ -52,7 +52,7 @@ struct pm_map {
     DevBuf stats;           // query counters (profiling level 2)
     // backward (pm_query_backward): pair sort, per-query records, segments,
     // FP64 running sums, and the forward outputs when the kNN is recomputed
-    DevBuf bvals, bscratch, qrec, seg_start, seg_end, acc;
+    DevBuf bvals, bvals1, bkeys0, bkeys1, bscratch, blong, qrec, seg_start, seg_end, acc;
     DevBuf rnbr, rcnt, rr2, rrad;
     DevBuf gnrm, gest;        // pm_gather_for: flipped normals, estimates
     // PM_MODE_ZHOU_COMPAT: node radius estimates of the current tree, kept
@@ -331,7 +331,7 @@ pm_status pm_destroy(pm_map* m) {
                      &m->scratch, &m->kfirst, &m->klast, &m->ksplit, &m->kkeep, &m->krank, &m->parent,
                      &m->arrive, &m->nleaf, &m->partials, &m->wflag, &m->wcnt, &m->wfirst,
                      &m->wchild, &m->wroot, &m->wscan, &m->rootmark, &m->qkeys0, &m->qkeys1, &m->qvals0, &m->qvals1,
-                     &m->qscratch, &m->counter, &m->fixq, &m->qsorted, &m->stats, &m->bvals,
+                     &m->qscratch, &m->counter, &m->fixq, &m->qsorted, &m->stats, &m->bvals, &m->bvals1, &m->bkeys0, &m->bkeys1, &m->blong,
                      &m->bscratch, &m->qrec, &m->seg_start, &m->seg_end, &m->acc, &m->rnbr,
                      &m->rcnt, &m->rr2, &m->rrad, &m->gnrm, &m->gest, &m->compat_est, &m->mpos, &m->mpow, &m->mflags,
                      &m->mrank, &m->mscan, &m->ic_pslot, &m->ic_level, &m->ic_range, &m->ic_center,
@@ -639,18 +639,28 @@ static pm_status ensure_bwd_capacity(pm_map* m, uint32_t chunk_q, uint32_t k, bo
                                      cudaStream_t st) {
     const uint64_t pairs = (uint64_t)chunk_q * k;
     const uint32_t n = m->n ? m->n : 1;
+    const uint64_t pc = pairs ? pairs : 1;
+    // the sort path's buffers when the largest chunk takes it
+    const bool sort_path = bwd_sort_path(pairs, n);
+    const size_t scratch_bytes = bwd_scratch_words(n, pc, sort_path) * sizeof(uint32_t);
     const bool grow = pairs > m->cap_pairs || chunk_q > m->cap_bq || n > m->cap_bn || (chunked && !m->acc.ptr) ||
                       (chunked && m->acc.bytes < (size_t)n * 6 * sizeof(double)) ||
+                      m->bscratch.bytes < scratch_bytes || (sort_path && m->bkeys1.bytes < pc * sizeof(uint32_t)) ||
                       (recompute && (chunk_q > m->cap_rq || !m->rnbr.ptr || m->rnbr.bytes < pairs * 4));
     if (!grow) return PM_OK;
     if (capturing(st))
         return fail(m, PM_ERR_STATE, "backward storage must grow during stream capture; run one backward first");
     pm_status s;
 #define ENSURE(buf, bytes) if ((s = buf_ensure(m, m->buf, (bytes), #buf)) != PM_OK) return s
-    const uint64_t pc = pairs ? pairs : 1;
     const size_t qc = chunk_q ? chunk_q : 1;
     ENSURE(bvals, pc * sizeof(uint32_t));
-    ENSURE(bscratch, bwd_scratch_words(n) * sizeof(uint32_t));
+    if (sort_path) {
+        ENSURE(bvals1, pc * sizeof(uint32_t));
+        ENSURE(bkeys0, pc * sizeof(uint32_t));
+        ENSURE(bkeys1, pc * sizeof(uint32_t));
+    }
+    ENSURE(bscratch, scratch_bytes);
+    ENSURE(blong, ((size_t)n + 1) * sizeof(uint32_t));
     ENSURE(qrec, qc * sizeof(BwdQuery));
     ENSURE(seg_start, (size_t)n * sizeof(uint32_t));
     ENSURE(seg_end, (size_t)n * sizeof(uint32_t));
@@ -688,7 +698,7 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     if (m->n == 0) return PM_OK;   // no photons: nothing to differentiate
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const uint32_t k = desc->k;
-    const uint64_t kMaxPairs = 1ull << 27;   // neighbour pairs per chunk (512 MB of pair slots)
+    const uint64_t kMaxPairs = 1ull << 27;   // neighbour pairs per chunk (512 MB of pair slots; 2 GB on the sort path)
     uint32_t chunk = (uint32_t)(kMaxPairs / k);
     if (m->bwd_chunk) chunk = m->bwd_chunk < chunk ? m->bwd_chunk : chunk;
     if (nq > 0 && chunk > nq) chunk = nq;
@@ -714,9 +724,11 @@ pm_status pm_query_backward(pm_map* m, const pm_query_desc* desc, const float* d
     a.vals = nullptr; a.cursor = nullptr; a.pair_cap = 0;
     a.nbr = nullptr; a.count_in = nullptr; a.order = nullptr;
     BwdBuffers b;
-    b.vals = P<uint32_t>(m->bvals);
+    b.vals[0] = P<uint32_t>(m->bvals); b.vals[1] = P<uint32_t>(m->bvals1);
+    b.keys[0] = P<uint32_t>(m->bkeys0); b.keys[1] = P<uint32_t>(m->bkeys1);
     b.scratch = P<uint32_t>(m->bscratch);
     b.seg_start = P<uint32_t>(m->seg_start); b.seg_end = P<uint32_t>(m->seg_end);
+    b.long_count = P<uint32_t>(m->blong); b.long_list = b.long_count + 1;
     b.acc = P<double>(m->acc);
     int nl = 0;
     for (uint32_t c = 0; c < nchunks; ++c) {

@@ -27,7 +27,8 @@
 //                   (query << 1 | the photon is the query's k-th) put into
 //                   its photon's segment at an atomic cursor
 //   4. k_bwd_segsort warp per photon: sorts its segment's values (bitonic
-//                   network in registers up to 256 values), which restores
+//                   network in registers up to 256 values; longer segments
+//                   by a block each, k_bwd_segsort_long), which restores
 //                   the query order the cursor lost: the segment then holds
 //                   exactly what a stable sort of the pairs by photon gives
 //   5. k_bwd_reduce thread per photon: walks its segment in order and sums
@@ -162,6 +163,10 @@ __global__ void __launch_bounds__(256) k_bwd_count(BwdArgs a, uint32_t q0, uint3
 // photon's segment at the photon's cursor (the segment start after the scan);
 // the cursor ends at the segment's end.  The slot is taken before the FP64
 // math, so the atomic's latency overlaps it.
+// kPlace false (the sort path, for chunks of high fan-in): every neighbour
+// slot writes its photon key (the sentinel n for a slot without a pair, which
+// sorts after every photon) and value at the caller's pair index instead.
+template <bool kPlace>
 __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32_t nq_chunk) {
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
@@ -178,9 +183,16 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
     double S0 = 0, S1 = 0, S2 = 0, T0 = 0, T1 = 0, T2 = 0;
     const double rinv = filter_rinv(a.filter, r2, (double)a.cone_k), inv_r2 = 1.0 / r2;
     const uint32_t jend = bwd_placed(a, cnt) ? cnt : 0u;
-    for (uint32_t j = lane; j < jend; j += 32) {
+    const uint64_t pair0 = (uint64_t)ql * k;
+    for (uint32_t j = lane; j < (kPlace ? jend : k); j += 32) {
+        const uint32_t val = (ql << 1) | (j == k - 1 ? 1u : 0u);   // the query, and whether p is its k-th
+        if (!kPlace && j >= jend) {
+            a.keys[pair0 + j] = a.n;
+            a.vals[pair0 + j] = val;
+            continue;
+        }
         const uint32_t p = a.inv[row[j]];
-        const uint32_t slot = atomicAdd(&a.cursor[p], 1u);
+        const uint32_t slot = kPlace ? atomicAdd(&a.cursor[p], 1u) : 0u;
         const float4 pp = a.pos[p], pw = a.pow[p];
         if (active && front_rn(qn.x, qn.y, qn.z, __float_as_uint(pw.w))) {
             double w, dwd, dwr;
@@ -188,7 +200,12 @@ __global__ void __launch_bounds__(256) k_bwd_prep(BwdArgs a, uint32_t q0, uint32
             S0 += w * pw.x; S1 += w * pw.y; S2 += w * pw.z;
             T0 += dwr * pw.x; T1 += dwr * pw.y; T2 += dwr * pw.z;
         }
-        if (slot < a.pair_cap) a.vals[slot] = (ql << 1) | (j == k - 1 ? 1u : 0u);   // the query, and whether p is its k-th
+        if (kPlace) {
+            if (slot < a.pair_cap) a.vals[slot] = val;
+        } else {
+            a.keys[pair0 + j] = p;
+            a.vals[pair0 + j] = val;
+        }
     }
     S0 = warp_sum_d(S0); S1 = warp_sum_d(S1); S2 = warp_sum_d(S2);
     T0 = warp_sum_d(T0); T1 = warp_sum_d(T1); T2 = warp_sum_d(T2);
@@ -262,37 +279,51 @@ __device__ __forceinline__ void sort_segment_regs(uint32_t* seg, uint32_t m, uin
     }
 }
 
-// Segments above 256 values: the same network in place over the next power
-// of two, the slots at and above m read as +infinity (a pair whose upper
-// slot is past m is already in order); L2 loads and stores, a warp barrier
-// between steps.
-__device__ __forceinline__ void sort_segment_global(uint32_t* seg, uint32_t m, uint32_t lane) {
-    uint32_t P = 1;
-    while (P < m) P <<= 1;
-    for (uint32_t kk = 2; kk <= P; kk <<= 1) {
-        for (uint32_t j = kk >> 1; j > 0; j >>= 1) {
-            for (uint32_t t = lane; t < (P >> 1); t += 32) {
-                const uint32_t i = (t / j) * 2 * j + (t % j);   // bit j of i clear
+constexpr uint32_t kSegRegMax = 256;       // values a warp sorts in registers
+constexpr uint32_t kSegSmemMax = 8192;     // values a block sorts in shared memory
+constexpr int kSegLongThreads = 512;
+
+// The all-ascending network over P (a power of two >= m) slots by a block:
+// pairs (i, partner) with bit j of i clear, the slots at and above m read as
+// +infinity (a pair whose upper slot is past m is already in order).  kShared:
+// s is the block's shared copy; else s is the segment, sorted in place
+// through L2.
+template <bool kShared>
+__device__ __forceinline__ void block_bitonic(uint32_t* s, uint32_t m, uint32_t P) {
+    for (uint32_t lk = 1; (1u << lk) <= P; ++lk) {
+        const uint32_t kk = 1u << lk;
+        for (int lj = (int)lk - 1; lj >= 0; --lj) {
+            const uint32_t j = 1u << lj;
+            for (uint32_t t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+                const uint32_t i = ((t >> lj) << (lj + 1)) | (t & (j - 1));   // bit j of i clear
                 const uint32_t o = j == (kk >> 1) ? (i ^ (kk - 1)) : (i + j);
                 if (o < m) {
-                    const uint32_t x = __ldcg(seg + i), y = __ldcg(seg + o);
+                    const uint32_t x = kShared ? s[i] : __ldcg(s + i), y = kShared ? s[o] : __ldcg(s + o);
                     if (x > y) {
-                        __stcg(seg + i, y);
-                        __stcg(seg + o, x);
+                        if (kShared) {
+                            s[i] = y;
+                            s[o] = x;
+                        } else {
+                            __stcg(s + i, y);
+                            __stcg(s + o, x);
+                        }
                     }
                 }
             }
-            __syncwarp();
+            __syncthreads();
         }
     }
 }
 
 // Warp per photon: sorts the values of its segment (distinct: a photon is
 // in a query's list at most once), so the segment lists its queries in
-// caller order.
+// caller order.  Segments above kSegRegMax values are listed for
+// k_bwd_segsort_long.
 __global__ void __launch_bounds__(256, 8) k_bwd_segsort(const uint32_t* __restrict__ start,
                                                         const uint32_t* __restrict__ end, uint32_t n,
-                                                        uint64_t cap, uint32_t* __restrict__ vals) {
+                                                        uint64_t cap, uint32_t* __restrict__ vals,
+                                                        uint32_t* __restrict__ long_list,
+                                                        uint32_t* __restrict__ long_count) {
     const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (p >= n) return;
@@ -302,8 +333,54 @@ __global__ void __launch_bounds__(256, 8) k_bwd_segsort(const uint32_t* __restri
     if (m <= 32) sort_segment_regs<1>(seg, m, lane);
     else if (m <= 64) sort_segment_regs<2>(seg, m, lane);
     else if (m <= 128) sort_segment_regs<4>(seg, m, lane);
-    else if (m <= 256) sort_segment_regs<8>(seg, m, lane);
-    else sort_segment_global(seg, m, lane);
+    else if (m <= kSegRegMax) sort_segment_regs<8>(seg, m, lane);
+    else if (lane == 0) long_list[atomicAdd(long_count, 1u)] = p;   // at most n photons: the list holds n
+}
+
+// Block per listed segment (above kSegRegMax values): in shared memory up to
+// kSegSmemMax values, in place through L2 beyond.  The grid loops over the
+// list, whose length only the device knows.
+__global__ void __launch_bounds__(kSegLongThreads) k_bwd_segsort_long(const uint32_t* __restrict__ long_list,
+                                                                      const uint32_t* __restrict__ long_count,
+                                                                      const uint32_t* __restrict__ start,
+                                                                      const uint32_t* __restrict__ end, uint64_t cap,
+                                                                      uint32_t* __restrict__ vals) {
+    __shared__ uint32_t s[kSegSmemMax];
+    const uint32_t count = *long_count;
+    for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+        const uint32_t p = long_list[li];
+        const uint32_t e = (uint32_t)min((uint64_t)end[p], cap), b = min(start[p], e), m = e - b;
+        uint32_t* seg = vals + b;
+        uint32_t P = 1;
+        while (P < m) P <<= 1;
+        if (m <= kSegSmemMax) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s[i] = seg[i];
+            __syncthreads();
+            block_bitonic<true>(s, m, P);
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) seg[i] = s[i];
+        } else {
+            block_bitonic<false>(seg, m, P);
+        }
+        __syncthreads();   // s is reused by the block's next segment
+    }
+}
+
+// Sort path: segment bounds of every photon in the sorted keys (start = end
+// = 0 when the photon has no pair; both arrays are cleared before).
+__global__ void k_bwd_bounds(const uint32_t* __restrict__ keys, uint64_t m, uint32_t n, uint32_t* __restrict__ start,
+                             uint32_t* __restrict__ end) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t key = keys[i];
+    if (key >= n) return;
+    if (i == 0 || keys[i - 1] != key) start[key] = (uint32_t)i;
+    if (i + 1 == m || keys[i + 1] != key) end[key] = (uint32_t)(i + 1);
+}
+
+int key_bits_for(uint32_t n) {
+    int b = 1;
+    while (b < 32 && (1ull << b) <= (uint64_t)n) ++b;   // sentinel n must fit
+    return b;
 }
 
 // One thread per photon (tree position).  acc holds 6 doubles per photon
@@ -367,36 +444,61 @@ __global__ void k_bwd_reduce(BwdArgs a, uint32_t q0, const uint32_t* __restrict_
 
 }  // namespace
 
-size_t bwd_scratch_words(uint32_t n) { return scan_scratch_words(n) + 1; }
+size_t bwd_scratch_words(uint32_t n, uint64_t pairs, bool sort_path) {
+    const size_t scan = scan_scratch_words(n) + 1;
+    const size_t sort = sort_path ? sort_scratch_words((uint32_t)pairs) + 64 : 0;
+    return scan > sort ? scan : sort;
+}
 
 int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
                    float4* grad_pow, float4* grad_pos, cudaStream_t st) {
     int nl = 0;
     BwdArgs x = a;
-    x.vals = b.vals;
-    x.cursor = b.seg_end;
-    x.pair_cap = (uint64_t)nq_chunk * a.k;
+    const uint64_t pairs = (uint64_t)nq_chunk * a.k;
+    x.pair_cap = pairs;
     const uint32_t warps_per_block = 8;
     const uint32_t qblocks = (nq_chunk + warps_per_block - 1) / warps_per_block;
-    cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
-    if (nq_chunk > 0) {
-        k_bwd_count<<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
+    const uint32_t* sorted_vals = b.vals[0];
+    if (nq_chunk > 0 && bwd_sort_path(pairs, a.n)) {
+        // high fan-in: a stable radix sort of the (photon, value) pairs, whose
+        // cost does not depend on how many pairs one photon holds
+        x.keys = b.keys[0];
+        x.vals = b.vals[0];
+        x.cursor = nullptr;
+        k_bwd_prep<false><<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
         ++nl;
-    }
-    // counts -> segment starts; the cursors start there and end at the ends
-    nl += exclusive_scan(b.seg_end, b.seg_end, a.n, b.scratch, nullptr, st);
-    cudaMemcpyAsync(b.seg_start, b.seg_end, (size_t)a.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
-    if (nq_chunk > 0) {
-        k_bwd_prep<<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
+        uint32_t* keys[2] = {b.keys[0], b.keys[1]};
+        uint32_t* vals[2] = {b.vals[0], b.vals[1]};
+        const int cur = radix_sort_pairs32(keys, vals, (uint32_t)pairs, key_bits_for(a.n), b.scratch, st, &nl);
+        cudaMemsetAsync(b.seg_start, 0, (size_t)a.n * sizeof(uint32_t), st);
+        cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
+        k_bwd_bounds<<<(uint32_t)((pairs + 255) / 256), 256, 0, st>>>(keys[cur], pairs, a.n, b.seg_start, b.seg_end);
         ++nl;
-    }
-    if (a.n > 0) {
+        sorted_vals = vals[cur];
+    } else {
+        x.keys = nullptr;
+        x.vals = b.vals[0];
+        x.cursor = b.seg_end;
+        cudaMemsetAsync(b.seg_end, 0, (size_t)a.n * sizeof(uint32_t), st);
         if (nq_chunk > 0) {
-            k_bwd_segsort<<<(a.n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
-                b.seg_start, b.seg_end, a.n, x.pair_cap, b.vals);
+            k_bwd_count<<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
             ++nl;
         }
-        k_bwd_reduce<<<(a.n + 127) / 128, 128, 0, st>>>(x, q0, b.vals, b.seg_start, b.seg_end, first ? 1 : 0,
+        // counts -> segment starts; the cursors start there and end at the ends
+        nl += exclusive_scan(b.seg_end, b.seg_end, a.n, b.scratch, nullptr, st);
+        cudaMemcpyAsync(b.seg_start, b.seg_end, (size_t)a.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+        if (nq_chunk > 0) {
+            k_bwd_prep<true><<<qblocks, 32 * warps_per_block, 0, st>>>(x, q0, nq_chunk);
+            cudaMemsetAsync(b.long_count, 0, sizeof(uint32_t), st);
+            k_bwd_segsort<<<(a.n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
+                b.seg_start, b.seg_end, a.n, x.pair_cap, b.vals[0], b.long_list, b.long_count);
+            k_bwd_segsort_long<<<a.n < 1024u ? a.n : 1024u, kSegLongThreads, 0, st>>>(
+                b.long_list, b.long_count, b.seg_start, b.seg_end, x.pair_cap, b.vals[0]);
+            nl += 3;
+        }
+    }
+    if (a.n > 0) {
+        k_bwd_reduce<<<(a.n + 127) / 128, 128, 0, st>>>(x, q0, sorted_vals, b.seg_start, b.seg_end, first ? 1 : 0,
                                                         last ? 1 : 0, b.acc, grad_pow, grad_pos);
         ++nl;
     }

@@ -329,19 +329,27 @@ struct BwdArgs {
     float cone_k;
     uint32_t min_found;
     BwdQuery* qrec;           // per chunk query: the record the per-photon pass reads
-    uint32_t* vals;           // pair values grouped by photon (set by backward_chunk)
+    uint32_t* keys;           // sort path: one photon key per neighbour slot (set by backward_chunk)
+    uint32_t* vals;           // pair values: grouped by photon (placement), or per slot (sort)
     uint32_t* cursor;         // per photon: pair count, then the next free slot of its segment
     uint64_t pair_cap;        // slots in vals
     const uint32_t* order;    // the chunk's queries in Hilbert order (chunk-local ids), or nullptr
 };
 struct BwdBuffers {
-    uint32_t* vals;           // one slot per neighbour pair of a chunk
-    uint32_t* scratch;        // the scan of the per-photon counts
+    uint32_t* vals[2];        // one slot per neighbour pair of a chunk ([1]: sort path only)
+    uint32_t* keys[2];        // sort path only
+    uint32_t* scratch;        // the scan of the per-photon counts, or the sort's
     uint32_t* seg_start;
     uint32_t* seg_end;
+    uint32_t* long_list;      // photons whose segments a block sorts (n entries)
+    uint32_t* long_count;
     double* acc;              // 6 doubles per photon, carried between chunks
 };
-size_t bwd_scratch_words(uint32_t n);
+// Mean pairs per photon above which a chunk groups its pairs by a stable
+// radix sort instead of counts, atomic placement and segment sorts.
+constexpr uint64_t kBwdPlaceMaxFanIn = 256;
+inline bool bwd_sort_path(uint64_t pairs, uint32_t n) { return pairs > kBwdPlaceMaxFanIn * (uint64_t)n; }
+size_t bwd_scratch_words(uint32_t n, uint64_t pairs, bool sort_path);
 int backward_chunk(const BwdArgs& a, uint32_t q0, uint32_t nq_chunk, bool first, bool last, const BwdBuffers& b,
                    float4* grad_pow, float4* grad_pos, cudaStream_t st);
 

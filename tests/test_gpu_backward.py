@@ -142,6 +142,28 @@ def test_backward_long_segments(cuda, oracle_mod, n):
     assert np.array_equal(res["gpow"], chunked["gpow"]) and np.array_equal(res["gpos"], chunked["gpos"])
 
 
+def test_backward_skewed_segments(cuda, oracle_mod):
+    """Twelve photons near every query, the rest far away: a mean of 12
+    pairs per photon (the placement path) with twelve segments of 20,000
+    pairs, which a block sorts in place through L2."""
+    k, r = 8, 2.0
+    ph = gen.photons(20000, seed=99, caustic_frac=0.2)
+    ph.pos[12:, :3] += 50.0
+    q = gen.queries(30000, seed=100)
+    idx, _d2, cnt, _r2 = oracle_mod.KdTree(ph.pos).knn(q.pos, k, r)
+    seg = np.bincount(idx[idx != np.uint32(0xFFFFFFFF)].astype(np.int64), minlength=ph.n)
+    assert (seg > 8192).sum() == 12 and seg.sum() <= 256 * ph.n
+    t = oracle_mod.radiance_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, "cone") * 0.9
+    res = engine_grads(cuda, ph, q, t, k, r, "cone")
+    assert np.array_equal(res["nbr"], idx) and np.array_equal(res["count"], cnt)
+    hp, hx = oracle_mod.backward_fp64(ph.pos, ph.pow, q.pos, q.nrm, idx, cnt, k, r, res["g"][:, :3].astype(np.float64),
+                                      "cone")
+    assert rel_err(res["gpow"][:, :3], hp, 1e-6).max() <= RTOL_HOST
+    assert rel_err(res["gpos"][:, :3], hx, 1e-6).max() <= RTOL_HOST
+    chunked = engine_grads(cuda, ph, q, t, k, r, "cone", chunk=9999)
+    assert np.array_equal(res["gpow"], chunked["gpow"]) and np.array_equal(res["gpos"], chunked["gpos"])
+
+
 def test_autograd_wrapper(cuda, oracle_mod):
     from mnrt_b200.autograd import RadianceEstimate
     k, r = 16, 0.06
