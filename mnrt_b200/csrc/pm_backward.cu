@@ -35,6 +35,13 @@
 //                   the FP64 contributions; the running sum carries across
 //                   query chunks, so chunked and single-pass runs give the
 //                   same bits
+// A chunk with more than kBwdPlaceMaxFanIn pairs per photon on average
+// replaces steps 1-4 by the sort path: k_bwd_prep<false> writes one (photon,
+// value) pair per neighbour slot, a stable LSD radix sort orders them by
+// photon and k_bwd_bounds finds the segments.  There the cursors of the
+// photons that neighbouring warps share contend and the segments grow long,
+// while the sort's cost does not depend on how the pairs spread; both paths
+// give the same segments, so the same bits.
 // Contributions are evaluated in FP64 from the FP32 inputs (the neighbour set
 // and the front test follow the FP32 forward contract).
 #include "pm_internal.h"
